@@ -1,0 +1,443 @@
+// api.cu -- context lifecycle, composite operators and the plain-pointer C ABI
+// declared in include/fabipb_b200.h.
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "context.cuh"
+#include "quad.cuh"
+
+namespace fb {
+
+static thread_local char g_err[1024] = "";
+
+void set_error(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+const char *get_error() { return g_err[0] ? g_err : "no error recorded"; }
+
+bool init_quad_tables() {
+  // Gauss-Legendre on [0,1], the published 15-decimal values the reference
+  // tabulates in src/numQuad.c:221-294.
+  static const double T[11][10] = {
+      {0},
+      {0.500000000000000},
+      {0.211324865405187, 0.788675134594813},
+      {0.112701665379258, 0.500000000000000, 0.887298334620742},
+      {0.069431844202974, 0.330009478207572, 0.669990521792428, 0.930568155797026},
+      {0.046910077030668, 0.230765344947158, 0.500000000000000, 0.769234655052841, 0.953089922969332},
+      {0.033765242898424, 0.169395306766868, 0.380690406958402, 0.619309593041598, 0.830604693233132,
+       0.966234757101576},
+      {0.025446043828621, 0.129234407200303, 0.297077424311301, 0.500000000000000, 0.702922575688699,
+       0.870765592799697, 0.974553956171379},
+      {0.019855071751232, 0.101666761293187, 0.237233795041836, 0.408282678752175, 0.591717321247825,
+       0.762766204958164, 0.898333238706813, 0.980144928248768},
+      {0.015919880246187, 0.081984446336682, 0.193314283649705, 0.337873288298095, 0.500000000000000,
+       0.662126711701904, 0.806685716350295, 0.918015553663318, 0.984080119753813},
+      {0.013046735741414, 0.067468316655508, 0.160295215850488, 0.283302302935376, 0.425562830509184,
+       0.574437169490816, 0.716697697064624, 0.839704784149512, 0.932531683344492, 0.986953264258586}};
+  static const double W[11][10] = {
+      {0},
+      {1.000000000000000},
+      {0.500000000000000, 0.500000000000000},
+      {0.277777777777778, 0.444444444444444, 0.277777777777778},
+      {0.173927422568727, 0.326072577431273, 0.326072577431273, 0.173927422568727},
+      {0.118463442528095, 0.239314335249683, 0.284444444444444, 0.239314335249683, 0.118463442528095},
+      {0.085662246189585, 0.180380786524070, 0.233956967286346, 0.233956967286346, 0.180380786524069,
+       0.085662246189585},
+      {0.064742483084435, 0.139852695744638, 0.190915025252560, 0.208979591836735, 0.190915025252559,
+       0.139852695744638, 0.064742483084435},
+      {0.050614268145188, 0.111190517226687, 0.156853322938944, 0.181341891689181, 0.181341891689181,
+       0.156853322938944, 0.111190517226687, 0.050614268145188},
+      {0.040637194180787, 0.090324080347429, 0.130305348201467, 0.156173538520002, 0.165119677500630,
+       0.156173538520002, 0.130305348201468, 0.090324080347429, 0.040637194180787},
+      {0.033335672154344, 0.074725674575290, 0.109543181257991, 0.134633359654998, 0.147762112357376,
+       0.147762112357376, 0.134633359654998, 0.109543181257991, 0.074725674575290, 0.033335672154344}};
+  FB_CUDA(cudaMemcpyToSymbol(c_tLeg, T, sizeof(T)));
+  FB_CUDA(cudaMemcpyToSymbol(c_wLeg, W, sizeof(W)));
+  return true;
+}
+
+Context::~Context() {
+  free_charges(*this);
+  free_precond(*this);
+  arena.release();
+  if (ownStream && stream) cudaStreamDestroy(stream);
+}
+
+bool setup_geometry(Context &c, const double *vtx, const double *nrm, const double *area) {
+  const int n = c.n;
+  if (!build_panel_tree(c.pt, n, vtx, c.prm.depth, c.prm.height, c.prm.sep_ratio, c.prm.order,
+                        c.prm.order_mom))
+    return false;
+  const PanelTree &pt = c.pt;
+  c.h_vtx.resize(9 * (size_t)n);
+  c.h_nrm.resize(3 * (size_t)n);
+  c.h_area.resize(n);
+  for (int i = 0; i < n; i++) {
+    int o = pt.order[i];
+    memcpy(&c.h_vtx[9 * (size_t)i], &vtx[9 * (size_t)o], 9 * sizeof(double));
+    memcpy(&c.h_nrm[3 * (size_t)i], &nrm[3 * (size_t)o], 3 * sizeof(double));
+    c.h_area[i] = area[o];
+  }
+  std::vector<int> leafOf(n);
+  std::vector<double> leafCtr(3 * (size_t)pt.nLeaves);
+  for (int L = 0; L < pt.nLeaves; L++) {
+    for (int k = 0; k < pt.leafCount[L]; k++) leafOf[pt.leafStart[L] + k] = L;
+    for (int k = 0; k < 3; k++) leafCtr[3 * (size_t)L + k] = pt.t.x[3 * (size_t)pt.leafCube[L] + k];
+  }
+  cudaStream_t s = c.stream;
+  if (!c.arena.upload(&c.d_vtx, c.h_vtx, s) || !c.arena.upload(&c.d_nrm, c.h_nrm, s) ||
+      !c.arena.upload(&c.d_area, c.h_area, s) || !c.arena.upload(&c.d_leafStart, pt.leafStart, s) ||
+      !c.arena.upload(&c.d_leafCount, pt.leafCount, s) || !c.arena.upload(&c.d_leafOfPanel, leafOf, s) ||
+      !c.arena.upload(&c.d_nearOff, pt.nearOff, s) || !c.arena.upload(&c.d_nearSrc, pt.nearSrc, s) ||
+      !c.arena.upload(&c.d_leafCtr, leafCtr, s))
+    return false;
+  if (!c.arena.alloc_n(&c.d_x, 2 * (size_t)n) || !c.arena.alloc_n(&c.d_y, 2 * (size_t)n) ||
+      !c.arena.alloc_n(&c.d_w, 2 * (size_t)n))
+    return false;
+  return true;
+}
+
+// pot = beta*pot + alpha*K_part*sgm
+bool op_apply(Context &c, int part, double alpha, const double *sgm, double beta, double *pot) {
+  if (part & FABIPB_B200_FAR) {
+    if (!launch_far_upward(c, sgm)) return false;
+    if (!launch_l2p(c, alpha, beta, pot, nullptr, 0.0, 0.0)) return false;
+  } else if (beta != 1.0) {
+    // scale pot by beta through L2P with alpha = 0 would still read lec;
+    // a plain scale is cheaper
+    if (beta == 0.0) {
+      FB_CUDA(cudaMemsetAsync(pot, 0, 2 * (size_t)c.n * sizeof(double), c.stream));
+    } else {
+      extern bool scale_vec(Context &, double *, double, long long);
+      if (!scale_vec(c, pot, beta, 2LL * c.n)) return false;
+    }
+  }
+  if (part & FABIPB_B200_NEAR) {
+    if (!launch_near(c, sgm, alpha, pot)) return false;
+  }
+  return true;
+}
+
+// y = alpha*(D - K)x + beta*y, D = diag(s1*A, s2*A) (MtVmain)
+bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y) {
+  double s1 = (1.0 + c.epsilon) / 2.0 * alpha;
+  double s2 = (1.0 + 1.0 / c.epsilon) / 2.0 * alpha;
+  if (!launch_far_upward(c, x)) return false;
+  if (!launch_l2p(c, -alpha, beta, y, x, s1, s2)) return false;
+  if (!launch_near(c, x, -alpha, y)) return false;
+  return true;
+}
+
+__global__ void scale_kernel(double *v, double a, long long n) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] *= a;
+}
+
+bool scale_vec(Context &c, double *v, double a, long long n) {
+  scale_kernel<<<ceil_div(n, 256), 256, 0, c.stream>>>(v, a, n);
+  FB_CUDA(cudaGetLastError());
+  return true;
+}
+
+}  // namespace fb
+
+using namespace fb;
+
+static bool valid_ctx(void *ctx) {
+  if (ctx == nullptr) {
+    set_error("null context");
+    return false;
+  }
+  return true;
+}
+
+// Run `fn` on device vectors; for host pointers copy in/out around it.
+template <typename F>
+static int with_vectors(Context *c, const double *in, double *inout, bool readOut, int on_device, F fn) {
+  cudaSetDevice(c->device);
+  const size_t bytes = 2 * (size_t)c->n * sizeof(double);
+  if (on_device) {
+    if (!fn(in, inout)) return 0;
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+      set_error("kernel failure: %s", cudaGetErrorString(cudaGetLastError()));
+      return 0;
+    }
+    return 1;
+  }
+  if (in && cudaMemcpyAsync(c->d_x, in, bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess) {
+    set_error("host-to-device copy failed");
+    return 0;
+  }
+  if (readOut && cudaMemcpyAsync(c->d_y, inout, bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess) {
+    set_error("host-to-device copy failed");
+    return 0;
+  }
+  if (!fn(in ? c->d_x : nullptr, c->d_y)) return 0;
+  if (cudaMemcpyAsync(inout, c->d_y, bytes, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess) {
+    set_error("device-to-host copy failed");
+    return 0;
+  }
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    set_error("kernel failure: %s", cudaGetErrorString(cudaGetLastError()));
+    return 0;
+  }
+  return 1;
+}
+
+extern "C" {
+
+void fabipb_b200_default_params(fabipb_b200_params *p) {
+  p->order = 3;
+  p->order_mom = 0;
+  p->depth = 5;
+  p->height = 2;
+  p->quad_order = 1;
+  p->sep_ratio = 0.8;
+  p->kappa = 0.1257;
+  p->eps1 = 1.0;
+  p->eps2 = 80.0;
+  p->rhs_theta = 0.8;
+  p->energy_theta = 0.8;
+  p->charge_order = 0;
+  p->precision = FABIPB_B200_MIXED;
+  p->device = 0;
+}
+
+const char *fabipb_b200_last_error(void) { return get_error(); }
+
+int fabipb_b200_create(const fabipb_b200_params *p, int n, const double *vtx, const double *normal,
+                       const double *area, void **out) {
+  if (out) *out = nullptr;
+  if (p == nullptr || vtx == nullptr || normal == nullptr || area == nullptr || out == nullptr || n <= 0) {
+    set_error("fabipb_b200_create: invalid arguments");
+    return 0;
+  }
+  auto t0 = std::chrono::steady_clock::now();
+  Context *c = new Context();
+  c->prm = *p;
+  c->n = n;
+  c->epsilon = p->eps2 / p->eps1;
+  c->mixed = (p->precision == FABIPB_B200_MIXED);
+  c->device = p->device;
+  bool ok = true;
+  if (cudaSetDevice(p->device) != cudaSuccess) {
+    set_error("cudaSetDevice(%d) failed", p->device);
+    ok = false;
+  }
+  if (ok && cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    set_error("cudaStreamCreate failed");
+    ok = false;
+  }
+  c->ownStream = ok;
+  ok = ok && init_quad_tables();
+  ok = ok && setup_geometry(*c, vtx, normal, area);
+  ok = ok && setup_near(*c);
+  ok = ok && setup_fmm(*c);
+  if (ok && cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    set_error("setup kernels failed: %s", cudaGetErrorString(cudaGetLastError()));
+    ok = false;
+  }
+  if (!ok) {
+    std::string keep = get_error();
+    delete c;
+    set_error("%s", keep.c_str());
+    return 0;
+  }
+  c->setupSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  *out = c;
+  return 1;
+}
+
+void fabipb_b200_destroy(void *ctx) {
+  if (ctx == nullptr) return;
+  Context *c = (Context *)ctx;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  delete c;
+}
+
+int fabipb_b200_set_stream(void *ctx, void *stream) {
+  if (!valid_ctx(ctx)) return 0;
+  Context *c = (Context *)ctx;
+  if (c->ownStream && c->stream) {
+    cudaStreamSynchronize(c->stream);
+    cudaStreamDestroy(c->stream);
+  }
+  c->ownStream = false;
+  c->stream = (cudaStream_t)stream;
+  return 1;
+}
+
+int fabipb_b200_info_get(void *ctx, fabipb_b200_info *o) {
+  if (!valid_ctx(ctx) || o == nullptr) return 0;
+  Context *c = (Context *)ctx;
+  o->panels = c->n;
+  o->leaves = c->pt.nLeaves;
+  o->near_pairs = (int)c->pt.nearSrc.size();
+  o->m2l_pairs = (int)c->pt.m2lSrc.size();
+  o->cubes = c->pt.nFmm;
+  o->max_order = c->P;
+  o->leaf_order = c->leafOrder;
+  o->max_leaf = c->maxLeaf;
+  o->near_panel_pairs = c->nearPanelPairs;
+  o->special_pairs = c->nSpecial;
+  o->setup_seconds = c->setupSeconds;
+  o->device_bytes = (double)c->arena.bytes;
+  return 1;
+}
+
+int fabipb_b200_panel_order(void *ctx, int *order) {
+  if (!valid_ctx(ctx) || order == nullptr) return 0;
+  Context *c = (Context *)ctx;
+  memcpy(order, c->pt.order.data(), (size_t)c->n * sizeof(int));
+  return 1;
+}
+
+int fabipb_b200_leaf_layout(void *ctx, int *start, int *count) {
+  if (!valid_ctx(ctx)) return 0;
+  Context *c = (Context *)ctx;
+  memcpy(start, c->pt.leafStart.data(), c->pt.leafStart.size() * sizeof(int));
+  memcpy(count, c->pt.leafCount.data(), c->pt.leafCount.size() * sizeof(int));
+  return 1;
+}
+
+int fabipb_b200_near_pairs(void *ctx, int *src, int *dst) {
+  if (!valid_ctx(ctx)) return 0;
+  Context *c = (Context *)ctx;
+  memcpy(src, c->pt.nearSrc.data(), c->pt.nearSrc.size() * sizeof(int));
+  memcpy(dst, c->pt.nearDst.data(), c->pt.nearDst.size() * sizeof(int));
+  return 1;
+}
+
+int fabipb_b200_m2l_pairs(void *ctx, int *src, int *dst) {
+  if (!valid_ctx(ctx)) return 0;
+  Context *c = (Context *)ctx;
+  memcpy(src, c->pt.m2lPairSrc.data(), c->pt.m2lPairSrc.size() * sizeof(int));
+  memcpy(dst, c->pt.m2lPairDst.data(), c->pt.m2lPairDst.size() * sizeof(int));
+  return 1;
+}
+
+int fabipb_b200_cube_data(void *ctx, int *level, double *ctr4) {
+  if (!valid_ctx(ctx)) return 0;
+  Context *c = (Context *)ctx;
+  for (int f = 0; f < c->pt.nFmm; f++) {
+    int cc = c->pt.fmmCube[f];
+    level[f] = c->pt.t.level[cc];
+    for (int k = 0; k < 3; k++) ctr4[4 * f + k] = c->pt.t.x[3 * (size_t)cc + k];
+    ctr4[4 * f + 3] = c->pt.t.rad[cc];
+  }
+  return 1;
+}
+
+int fabipb_b200_apply(void *ctx, int part, double alpha, const double *sgm, double beta, double *pot,
+                      int on_device) {
+  if (!valid_ctx(ctx) || sgm == nullptr || pot == nullptr) return 0;
+  Context *c = (Context *)ctx;
+  if (part < 1 || part > 3) {
+    set_error("fabipb_b200_apply: part must be NEAR, FAR or ALL");
+    return 0;
+  }
+  return with_vectors(c, sgm, pot, beta != 0.0, on_device, [&](const double *x, double *y) {
+    return op_apply(*c, part, alpha, x, beta, y);
+  });
+}
+
+int fabipb_b200_matvec(void *ctx, double alpha, const double *x, double beta, double *y, int on_device) {
+  if (!valid_ctx(ctx) || x == nullptr || y == nullptr) return 0;
+  Context *c = (Context *)ctx;
+  return with_vectors(c, x, y, beta != 0.0, on_device, [&](const double *xd, double *yd) {
+    return op_matvec(*c, alpha, xd, beta, yd);
+  });
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int fabipb_b200_set_charges(void *ctx, int m, const double *pos, const double *q) {
+  if (!valid_ctx(ctx) || m <= 0 || pos == nullptr || q == nullptr) {
+    set_error("fabipb_b200_set_charges: invalid arguments");
+    return 0;
+  }
+  Context *c = (Context *)ctx;
+  cudaSetDevice(c->device);
+  if (!setup_charges(*c, m, pos, q)) return 0;
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    set_error("charge setup failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return 0;
+  }
+  return 1;
+}
+
+int fabipb_b200_rhs(void *ctx, int use_tree, double *rhs, int on_device) {
+  if (!valid_ctx(ctx) || rhs == nullptr) return 0;
+  Context *c = (Context *)ctx;
+  return with_vectors(c, nullptr, rhs, false, on_device, [&](const double *, double *y) {
+    return launch_rhs(*c, use_tree, y);
+  });
+}
+
+int fabipb_b200_energy(void *ctx, const double *sgm, double *raw, int on_device) {
+  if (!valid_ctx(ctx) || sgm == nullptr || raw == nullptr) return 0;
+  Context *c = (Context *)ctx;
+  cudaSetDevice(c->device);
+  const double *d = sgm;
+  if (!on_device) {
+    if (cudaMemcpyAsync(c->d_x, sgm, 2 * (size_t)c->n * sizeof(double), cudaMemcpyHostToDevice, c->stream) !=
+        cudaSuccess) {
+      set_error("host-to-device copy failed");
+      return 0;
+    }
+    d = c->d_x;
+  }
+  if (!launch_energy(*c, d, raw)) return 0;
+  return 1;
+}
+
+int fabipb_b200_precond_setup(void *ctx, int mode) {
+  if (!valid_ctx(ctx)) return 0;
+  Context *c = (Context *)ctx;
+  cudaSetDevice(c->device);
+  if (!precond_setup(*c, mode)) return 0;
+  if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    set_error("preconditioner setup failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return 0;
+  }
+  return 1;
+}
+
+int fabipb_b200_precond_apply(void *ctx, const double *b, double *x, int on_device) {
+  if (!valid_ctx(ctx) || b == nullptr || x == nullptr) return 0;
+  Context *c = (Context *)ctx;
+  return with_vectors(c, b, x, false, on_device, [&](const double *bd, double *xd) {
+    return precond_apply(*c, bd, xd);
+  });
+}
+
+int fabipb_b200_solve(void *ctx, const double *b, double *x, int restart, int maxit, double tol, int *iters,
+                      double *resid, int *info, int on_device) {
+  if (!valid_ctx(ctx) || b == nullptr || x == nullptr || restart < 1 || maxit < 1) {
+    set_error("fabipb_b200_solve: invalid arguments");
+    return 0;
+  }
+  Context *c = (Context *)ctx;
+  int it = 0, inf = 0;
+  double res = 0.0;
+  int ok = with_vectors(c, b, x, true, on_device, [&](const double *bd, double *xd) {
+    return gmres_solve(*c, bd, xd, restart, maxit, tol, &it, &res, &inf);
+  });
+  if (iters) *iters = it;
+  if (resid) *resid = res;
+  if (info) *info = inf;
+  return ok;
+}
+
+}  // extern "C"

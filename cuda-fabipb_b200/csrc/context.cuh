@@ -1,0 +1,108 @@
+// context.cuh -- the device-resident state of one surface mesh.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/fabipb_b200.h"
+#include "common.cuh"
+#include "tree.hpp"
+
+namespace fb {
+
+struct ChargeTreeDev;
+struct PrecondDev;
+struct GraphCache;
+
+struct Context {
+  fabipb_b200_params prm{};
+  double epsilon = 80.0;  // eps2 / eps1
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool ownStream = false;
+  DevArena arena;
+
+  // ---- panels (tree order) and tree ----------------------------------
+  PanelTree pt;
+  int n = 0;
+  std::vector<double> h_vtx, h_nrm, h_area;  // tree order (host copy)
+  double *d_vtx = nullptr, *d_nrm = nullptr, *d_area = nullptr;
+  int *d_leafStart = nullptr, *d_leafCount = nullptr, *d_leafOfPanel = nullptr;
+  int *d_nearOff = nullptr, *d_nearSrc = nullptr;
+  double *d_leafCtr = nullptr;             // 3 per leaf: enclosing-box centre
+  int nWork = 0;                           // near-field warp tasks
+  int2 *d_work = nullptr;                  // (leaf, 32-target group)
+  long long nearPanelPairs = 0;
+  int maxLeaf = 0;
+
+  // ---- near field -------------------------------------------------------
+  bool mixed = false;                      // FP32 P2P when true
+  void *d_tgtP = nullptr, *d_tgtN = nullptr;   // T4: {rel pos, area}, {normal, 0}
+  void *d_srcA = nullptr, *d_srcB = nullptr;   // T4: {rel pos, A*s_dpdn}, {normal, A*s_pot}
+  long long nSpecial = 0;
+  int *d_spOff = nullptr, *d_spSrc = nullptr;  // CSR by destination panel
+  double4 *d_spK = nullptr;                    // exact minus one-point coefficient
+
+  // ---- FMM ----------------------------------------------------------
+  int P = 0, NM = 0;                       // max order, nmom(max order)
+  int leafOrder = 0, NMleaf = 0;
+  double *d_Q0 = nullptr, *d_Q1 = nullptr; // [NMleaf][n]: moments, noments
+  double *d_cubeCtr = nullptr;             // 3 per FMM cube
+  int *d_m2lOff = nullptr, *d_m2lSrc = nullptr;
+  int *d_fmmParent = nullptr;              // parent FMM index (or -1)
+  int *d_leafFmm = nullptr;                // leaf -> FMM index
+  double *d_mom = nullptr;                 // [2][nFmm][NM]  pot, dpdn
+  double *d_lec = nullptr;                 // [4][nFmm][NM]
+  std::vector<int> h_m2lDst;               // destination cubes with a list
+  int *d_m2lDst = nullptr;
+  int *d_lstOff = nullptr, *d_lst = nullptr;   // (beta, alpha+beta, |beta|) per alpha
+  int *d_mOff = nullptr, *d_mLst = nullptr;    // (alpha-k, k) per alpha
+  int *d_kidFirst = nullptr, *d_kidCount = nullptr;  // FMM indices of the children
+  int *d_ordM2L = nullptr;                     // per FMM cube
+
+  // ---- scratch vectors for host-pointer calls ------------------------
+  double *d_x = nullptr, *d_y = nullptr, *d_w = nullptr;
+
+  // ---- charges, RHS, energy -------------------------------------------
+  int nChar = 0;
+  std::vector<double> h_pos, h_chr;
+  ChargeTreeDev *ct = nullptr;
+
+  // ---- preconditioner and GMRES ---------------------------------------
+  PrecondDev *pc = nullptr;
+  GraphCache *graphs = nullptr;
+
+  double setupSeconds = 0.0;
+  ~Context();
+};
+
+// setup pieces (each returns false with the error recorded)
+bool setup_geometry(Context &c, const double *vtx, const double *nrm, const double *area);
+bool setup_near(Context &c);
+bool setup_fmm(Context &c);
+bool setup_charges(Context &c, int m, const double *pos, const double *q);
+
+// device operators on device vectors (stream-ordered, no synchronisation)
+// near:  out += coef * K_near * sgm
+bool launch_near(Context &c, const double *sgm, double coef, double *out);
+// upward pass + interaction + downward pass: leaves local expansions in d_lec
+bool launch_far_upward(Context &c, const double *sgm);
+// L2P: out = beta*out + alpha*far + diag*(area .* x) (diag part optional)
+bool launch_l2p(Context &c, double alpha, double beta, double *out, const double *diagX,
+                double s1, double s2);
+bool launch_m2l_only(Context &c);
+bool launch_rhs(Context &c, int useTree, double *rhs);
+bool launch_energy(Context &c, const double *sgm, double *raw_host);
+bool precond_setup(Context &c, int mode);
+bool precond_apply(Context &c, const double *b, double *x);
+bool gmres_solve(Context &c, const double *b, double *x, int restart, int maxit, double tol,
+                 int *iters, double *resid, int *info);
+void free_charges(Context &c);
+void free_precond(Context &c);
+
+// composite operators (device vectors)
+bool op_apply(Context &c, int part, double alpha, const double *sgm, double beta, double *pot);
+bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y);
+
+}  // namespace fb

@@ -1,0 +1,7 @@
+// fabipb_b200.cu -- the library is compiled as one translation unit so the
+// constant-memory tables (quadrature rules, multi-index tables) are shared by
+// every kernel without relocatable device code.
+#include "near.cu"
+#include "fmm.cu"
+#include "stubs_tmp.cu"
+#include "api.cu"

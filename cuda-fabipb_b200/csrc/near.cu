@@ -1,0 +1,372 @@
+// near.cu -- Galerkin near field on the device.
+//
+// The near field couples every panel X of a leaf with every panel Y of each
+// leaf in its near list (src/fmm.c:554-593).  With the one-point rule (-q=1,
+// the reference default) a disjoint pair is K = Ax*Ay*KER4(mX - mY)
+// (src/numQuad.c:586-618 at q=1, src/gpu/gpu_nearfield_cuda.inc:1127-1137);
+// pairs that share a vertex, an edge, or are the same panel use the Sauter
+// rules instead (src/numQuad.c:401-571).
+//
+// B200 design:
+//   * nothing per pair is stored: each warp owns 32 target panels of one
+//     leaf, keeps them in registers, and streams the source panels of every
+//     near leaf through a per-warp shared-memory tile, so the P2P work is pure
+//     FP32 (or FP64) ALU + two MUFU ops per pair;
+//   * positions are stored relative to their own leaf centre, and a target
+//     is moved into each source leaf's frame once per leaf pair, which keeps
+//     FP32 differences of close panels accurate to ~1e-7 relative;
+//   * the coincident pair is masked (r = 0 gives 0), and every pair with a
+//     shared vertex carries an FP64 correction "exact Sauter value minus the
+//     one-point value" in a CSR table built once on the device, applied in
+//     FP64 in the same kernel.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <unordered_map>
+
+#include "context.cuh"
+#include "quad.cuh"
+
+namespace fb {
+
+template <typename T>
+struct Vec4;
+template <>
+struct Vec4<float> {
+  typedef float4 t;
+};
+template <>
+struct Vec4<double> {
+  typedef double4 t;
+};
+
+__device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
+// e^{-kappa r}: float uses the MUFU ex2 path with kexp = -kappa*log2(e)
+__device__ __forceinline__ float expneg_t(float kexp, float r) { return exp2f(kexp * r); }
+__device__ __forceinline__ double expneg_t(double kexp, double r) { return exp(kexp * r); }
+
+template <typename T>
+__global__ void near_targets_kernel(int n, const double *__restrict__ vtx, const double *__restrict__ nrm,
+                                    const double *__restrict__ area, const int *__restrict__ leafOfPanel,
+                                    const double *__restrict__ leafCtr, typename Vec4<T>::t *tgtP,
+                                    typename Vec4<T>::t *tgtN) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double *v = vtx + 9 * (size_t)i;
+  const double *c = leafCtr + 3 * (size_t)leafOfPanel[i];
+  double m[3];
+  for (int k = 0; k < 3; k++) {
+    double a2 = v[3 + k] - v[k], a0 = v[6 + k] - v[3 + k];
+    m[k] = v[k] + 0.5 * (a2 + 0.5 * a0);
+  }
+  typename Vec4<T>::t p, q;
+  p.x = (T)(m[0] - c[0]); p.y = (T)(m[1] - c[1]); p.z = (T)(m[2] - c[2]); p.w = (T)area[i];
+  q.x = (T)nrm[3 * (size_t)i]; q.y = (T)nrm[3 * (size_t)i + 1]; q.z = (T)nrm[3 * (size_t)i + 2]; q.w = (T)0;
+  tgtP[i] = p;
+  tgtN[i] = q;
+}
+
+template <typename T>
+__global__ void near_pack_kernel(int n, const typename Vec4<T>::t *__restrict__ tgtP,
+                                 const typename Vec4<T>::t *__restrict__ tgtN, const double *__restrict__ area,
+                                 const double *__restrict__ sgm, typename Vec4<T>::t *srcA,
+                                 typename Vec4<T>::t *srcB) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  typename Vec4<T>::t a = tgtP[i], b = tgtN[i];
+  double A = area[i];
+  a.w = (T)(A * sgm[n + i]);  // weight of the dpdn density
+  b.w = (T)(A * sgm[i]);      // weight of the potential density
+  srcA[i] = a;
+  srcB[i] = b;
+}
+
+constexpr int kNearWarps = 4;
+
+template <typename T>
+__global__ void __launch_bounds__(kNearWarps * 32)
+near_apply_kernel(int nWork, const int2 *__restrict__ work, const int *__restrict__ leafStart,
+                  const int *__restrict__ leafCount, const int *__restrict__ nearOff,
+                  const int *__restrict__ nearSrc, const double *__restrict__ leafCtr,
+                  const typename Vec4<T>::t *__restrict__ tgtP, const typename Vec4<T>::t *__restrict__ tgtN,
+                  const typename Vec4<T>::t *__restrict__ srcA, const typename Vec4<T>::t *__restrict__ srcB,
+                  const int *__restrict__ spOff, const int *__restrict__ spSrc,
+                  const double4 *__restrict__ spK, const double *__restrict__ sgm,
+                  const double *__restrict__ area, int n, T kappa, T kexp, T eps, T ieps, T kap2,
+                  double coef, double *out) {
+  typedef typename Vec4<T>::t V;
+  __shared__ V sA[kNearWarps][32];
+  __shared__ V sB[kNearWarps][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int task = blockIdx.x * kNearWarps + warp;
+  if (task >= nWork) return;  // warp-uniform
+  const int2 wk = work[task];
+  const int L = wk.x;
+  const int base = leafStart[L], cnt = leafCount[L];
+  const int ti = 32 * wk.y + lane;
+  const bool valid = ti < cnt;
+  const int X = base + (valid ? ti : 0);
+  const V tp = tgtP[X], tn = tgtN[X];
+  const double cx = leafCtr[3 * L], cy = leafCtr[3 * L + 1], cz = leafCtr[3 * L + 2];
+  T acc0 = (T)0, acc1 = (T)0;
+  const int p1 = nearOff[L + 1];
+  for (int p = nearOff[L]; p < p1; p++) {
+    const int S = nearSrc[p];
+    const int sb = leafStart[S], sc = leafCount[S];
+    const T tx = tp.x + (T)(cx - leafCtr[3 * S]);
+    const T ty = tp.y + (T)(cy - leafCtr[3 * S + 1]);
+    const T tz = tp.z + (T)(cz - leafCtr[3 * S + 2]);
+    for (int j0 = 0; j0 < sc; j0 += 32) {
+      const int m = min(32, sc - j0);
+      if (lane < m) {
+        sA[warp][lane] = srcA[sb + j0 + lane];
+        sB[warp][lane] = srcB[sb + j0 + lane];
+      }
+      __syncwarp();
+#pragma unroll 4
+      for (int jj = 0; jj < m; jj++) {
+        const V a = sA[warp][jj];
+        const V b = sB[warp][jj];
+        const T dx = tx - a.x, dy = ty - a.y, dz = tz - a.z;
+        const T r2 = dx * dx + dy * dy + dz * dz;
+        const T g = r2 > (T)0 ? rsqrt_t(r2) : (T)0;   // 1/r, 0 for the coincident pair
+        const T r = r2 * g;
+        const T e = expneg_t(kexp, r);
+        const T c = (kappa * r + (T)1) * e;           // (kappa r + 1) e^{-kappa r}
+        const T g2 = g * g;
+        const T h = g2 * g;
+        const T ipX = tn.x * dx + tn.y * dy + tn.z * dz;
+        const T ipY = b.x * dx + b.y * dy + b.z * dz;
+        const T ip0 = tn.x * b.x + tn.y * b.y + tn.z * b.z;
+        const T t1 = ipY * h;                          // dG0/dn_y * 4 pi
+        const T t2 = ipX * h;                          // dG0/dn_x * 4 pi
+        const T y0 = g - g * e;                        // G0 - Gk
+        const T y1 = t1 * (eps * c - (T)1);            // eps dGk/dn_y - dG0/dn_y
+        const T y2 = t2 * (c * ieps - (T)1);           // dGk/dn_x / eps - dG0/dn_x
+        const T dd = (ip0 * g - (T)3 * t1 * ipX) * g2; // d2 G0 / dn_x dn_y
+        const T y3 = dd * (c - (T)1) - kap2 * e * ipX * t1;
+        acc0 += y0 * a.w + y1 * b.w;
+        acc1 += y2 * a.w + y3 * b.w;
+      }
+      __syncwarp();
+    }
+  }
+  if (!valid) return;
+  double e0 = 0.0, e1 = 0.0;
+  const int s1 = spOff[X + 1];
+  for (int e = spOff[X]; e < s1; e++) {
+    const int Y = spSrc[e];
+    const double4 d = spK[e];
+    const double sp = sgm[Y], sd = sgm[n + Y];
+    e0 += d.x * sd + d.y * sp;
+    e1 += d.z * sd + d.w * sp;
+  }
+  const double AX = area[X] * kFourPiI;
+  out[X] += coef * (AX * (double)acc0 + e0);
+  out[X + n] += coef * (AX * (double)acc1 + e1);
+}
+
+// FP64 correction for every special pair: exact panelIA0 minus the
+// one-point value the P2P loop computes for the same pair.
+__global__ void special_coeff_kernel(long long nSp, const int *__restrict__ spDst, const int *__restrict__ spSrc,
+                                     const double *__restrict__ vtx, const double *__restrict__ nrm,
+                                     const double *__restrict__ area, int q, double kappa, double eps,
+                                     double4 *spK, int *caseOut) {
+  long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nSp) return;
+  int Xi = spDst[e], Yi = spSrc[e];
+  PanelD X, Y;
+  const double *vx = vtx + 9 * (size_t)Xi, *vy = vtx + 9 * (size_t)Yi;
+  for (int k = 0; k < 3; k++) {
+    for (int c = 0; c < 3; c++) { X.v[k][c] = vx[3 * k + c]; Y.v[k][c] = vy[3 * k + c]; }
+  }
+  for (int c = 0; c < 3; c++) {
+    X.a[0][c] = X.v[2][c] - X.v[1][c]; X.a[1][c] = X.v[0][c] - X.v[2][c]; X.a[2][c] = X.v[1][c] - X.v[0][c];
+    Y.a[0][c] = Y.v[2][c] - Y.v[1][c]; Y.a[1][c] = Y.v[0][c] - Y.v[2][c]; Y.a[2][c] = Y.v[1][c] - Y.v[0][c];
+    X.n[c] = nrm[3 * (size_t)Xi + c];
+    Y.n[c] = nrm[3 * (size_t)Yi + c];
+  }
+  X.area = area[Xi];
+  Y.area = area[Yi];
+  double K[4], M[4] = {0, 0, 0, 0};
+  int cs = 0;
+  panel_ia0_d(q, kappa, eps, X, Y, Xi == Yi, K, &cs);
+  if (Xi != Yi) {
+    double r[3];
+    for (int c = 0; c < 3; c++) {
+      double mx = X.v[0][c] + 0.5 * (X.a[2][c] + 0.5 * X.a[0][c]);
+      double my = Y.v[0][c] + 0.5 * (Y.a[2][c] + 0.5 * Y.a[0][c]);
+      r[c] = mx - my;
+    }
+    if (r[0] != 0.0 || r[1] != 0.0 || r[2] != 0.0) {
+      double y[4];
+      ker4_d(kappa, eps, r, X.n, Y.n, y);
+      for (int i = 0; i < 4; i++) M[i] = X.area * Y.area * y[i];
+    }
+  }
+  spK[e] = make_double4(K[0] - M[0], K[1] - M[1], K[2] - M[2], K[3] - M[3]);
+  if (caseOut) caseOut[e] = cs;
+}
+
+namespace {
+
+struct VKey {
+  uint64_t a, b, c;
+  bool operator==(const VKey &o) const { return a == o.a && b == o.b && c == o.c; }
+};
+struct VKeyHash {
+  size_t operator()(const VKey &k) const {
+    uint64_t h = k.a * 0x9E3779B97F4A7C15ULL;
+    h ^= k.b + 0x7F4A7C159E3779B9ULL + (h << 6) + (h >> 2);
+    h ^= k.c + 0x94D049BB133111EBULL + (h << 6) + (h >> 2);
+    return (size_t)h;
+  }
+};
+inline uint64_t dbits(double v) {
+  if (v == 0.0) v = 0.0;  // -0.0 and 0.0 compare equal in nrCommonVtx
+  uint64_t u;
+  memcpy(&u, &v, 8);
+  return u;
+}
+
+}  // namespace
+
+bool setup_near(Context &c) {
+  const PanelTree &pt = c.pt;
+  const int n = c.n;
+  cudaStream_t s = c.stream;
+  if (c.prm.quad_order != 1) {
+    set_error("the device near field implements the one-point panel rule (-q=1); got -q=%d",
+              c.prm.quad_order);
+    return false;
+  }
+  // warp tasks: (leaf, group of 32 targets)
+  std::vector<int2> work;
+  c.maxLeaf = 0;
+  c.nearPanelPairs = 0;
+  for (int L = 0; L < pt.nLeaves; L++) {
+    int cnt = pt.leafCount[L];
+    c.maxLeaf = std::max(c.maxLeaf, cnt);
+    for (int g = 0; g * 32 < cnt; g++) work.push_back(make_int2(L, g));
+    long long srcs = 0;
+    for (int p = pt.nearOff[L]; p < pt.nearOff[L + 1]; p++) srcs += pt.leafCount[pt.nearSrc[p]];
+    c.nearPanelPairs += srcs * cnt;
+  }
+  c.nWork = (int)work.size();
+  if (!c.arena.upload(&c.d_work, work, s)) return false;
+
+  // special pairs: panels sharing a vertex (exact coordinates), restricted to
+  // near leaf pairs, plus the panel itself
+  std::unordered_map<VKey, int, VKeyHash> vid;
+  vid.reserve((size_t)n * 2);
+  std::vector<int> pv(3 * (size_t)n);
+  for (int i = 0; i < n; i++)
+    for (int k = 0; k < 3; k++) {
+      const double *x = &c.h_vtx[9 * (size_t)i + 3 * k];
+      VKey key{dbits(x[0]), dbits(x[1]), dbits(x[2])};
+      auto it = vid.find(key);
+      int id;
+      if (it == vid.end()) {
+        id = (int)vid.size();
+        vid.emplace(key, id);
+      } else {
+        id = it->second;
+      }
+      pv[3 * (size_t)i + k] = id;
+    }
+  const int nv = (int)vid.size();
+  std::vector<int> vOff(nv + 1, 0), vPan(3 * (size_t)n);
+  for (int i = 0; i < 3 * n; i++) vOff[pv[i] + 1]++;
+  for (int v = 0; v < nv; v++) vOff[v + 1] += vOff[v];
+  {
+    std::vector<int> cur(vOff.begin(), vOff.end() - 1);
+    for (int i = 0; i < 3 * n; i++) vPan[cur[pv[i]]++] = i / 3;
+  }
+  std::vector<int> leafOf(n);
+  for (int L = 0; L < pt.nLeaves; L++)
+    for (int k = 0; k < pt.leafCount[L]; k++) leafOf[pt.leafStart[L] + k] = L;
+  std::vector<std::vector<int>> nearSorted(pt.nLeaves);
+  for (int L = 0; L < pt.nLeaves; L++) {
+    nearSorted[L].assign(pt.nearSrc.begin() + pt.nearOff[L], pt.nearSrc.begin() + pt.nearOff[L + 1]);
+    std::sort(nearSorted[L].begin(), nearSorted[L].end());
+  }
+  std::vector<int> spOff(n + 1, 0), spDst, spSrc;
+  spDst.reserve(16 * (size_t)n);
+  spSrc.reserve(16 * (size_t)n);
+  std::vector<int> cand;
+  for (int X = 0; X < n; X++) {
+    cand.clear();
+    cand.push_back(X);
+    for (int k = 0; k < 3; k++) {
+      int v = pv[3 * (size_t)X + k];
+      for (int e = vOff[v]; e < vOff[v + 1]; e++) cand.push_back(vPan[e]);
+    }
+    std::sort(cand.begin(), cand.end());
+    cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+    const std::vector<int> &ns = nearSorted[leafOf[X]];
+    for (int Y : cand) {
+      if (std::binary_search(ns.begin(), ns.end(), leafOf[Y])) {
+        spDst.push_back(X);
+        spSrc.push_back(Y);
+      }
+    }
+    spOff[X + 1] = (int)spSrc.size();
+  }
+  c.nSpecial = (long long)spSrc.size();
+  int *d_spDst = nullptr;
+  if (!c.arena.upload(&c.d_spOff, spOff, s)) return false;
+  if (!c.arena.upload(&c.d_spSrc, spSrc, s)) return false;
+  if (!c.arena.upload(&d_spDst, spDst, s)) return false;
+  if (!c.arena.alloc_n(&c.d_spK, (size_t)std::max<long long>(c.nSpecial, 1))) return false;
+  if (c.nSpecial > 0) {
+    special_coeff_kernel<<<ceil_div(c.nSpecial, 128), 128, 0, s>>>(
+        c.nSpecial, d_spDst, c.d_spSrc, c.d_vtx, c.d_nrm, c.d_area, c.prm.quad_order, c.prm.kappa,
+        c.epsilon, c.d_spK, nullptr);
+    FB_CUDA(cudaGetLastError());
+  }
+
+  // static target geometry relative to the leaf centres
+  size_t vb = c.mixed ? sizeof(float4) : sizeof(double4);
+  if (!c.arena.alloc(&c.d_tgtP, vb * n) || !c.arena.alloc(&c.d_tgtN, vb * n) ||
+      !c.arena.alloc(&c.d_srcA, vb * n) || !c.arena.alloc(&c.d_srcB, vb * n))
+    return false;
+  if (c.mixed) {
+    near_targets_kernel<float><<<ceil_div(n, 256), 256, 0, s>>>(
+        n, c.d_vtx, c.d_nrm, c.d_area, c.d_leafOfPanel, c.d_leafCtr, (float4 *)c.d_tgtP, (float4 *)c.d_tgtN);
+  } else {
+    near_targets_kernel<double><<<ceil_div(n, 256), 256, 0, s>>>(
+        n, c.d_vtx, c.d_nrm, c.d_area, c.d_leafOfPanel, c.d_leafCtr, (double4 *)c.d_tgtP, (double4 *)c.d_tgtN);
+  }
+  FB_CUDA(cudaGetLastError());
+  return true;
+}
+
+bool launch_near(Context &c, const double *sgm, double coef, double *out) {
+  const int n = c.n;
+  cudaStream_t s = c.stream;
+  const double kap = c.prm.kappa, eps = c.epsilon;
+  unsigned grid = ceil_div(c.nWork, kNearWarps);
+  if (c.mixed) {
+    near_pack_kernel<float><<<ceil_div(n, 256), 256, 0, s>>>(n, (const float4 *)c.d_tgtP, (const float4 *)c.d_tgtN,
+                                                             c.d_area, sgm, (float4 *)c.d_srcA, (float4 *)c.d_srcB);
+    near_apply_kernel<float><<<grid, kNearWarps * 32, 0, s>>>(
+        c.nWork, c.d_work, c.d_leafStart, c.d_leafCount, c.d_nearOff, c.d_nearSrc, c.d_leafCtr,
+        (const float4 *)c.d_tgtP, (const float4 *)c.d_tgtN, (const float4 *)c.d_srcA, (const float4 *)c.d_srcB,
+        c.d_spOff, c.d_spSrc, c.d_spK, sgm, c.d_area, n, (float)kap, (float)(-kap * 1.4426950408889634),
+        (float)eps, (float)(1.0 / eps), (float)(kap * kap), coef, out);
+  } else {
+    near_pack_kernel<double><<<ceil_div(n, 256), 256, 0, s>>>(n, (const double4 *)c.d_tgtP,
+                                                              (const double4 *)c.d_tgtN, c.d_area, sgm,
+                                                              (double4 *)c.d_srcA, (double4 *)c.d_srcB);
+    near_apply_kernel<double><<<grid, kNearWarps * 32, 0, s>>>(
+        c.nWork, c.d_work, c.d_leafStart, c.d_leafCount, c.d_nearOff, c.d_nearSrc, c.d_leafCtr,
+        (const double4 *)c.d_tgtP, (const double4 *)c.d_tgtN, (const double4 *)c.d_srcA,
+        (const double4 *)c.d_srcB, c.d_spOff, c.d_spSrc, c.d_spK, sgm, c.d_area, n, kap, -kap, eps, 1.0 / eps,
+        kap * kap, coef, out);
+  }
+  FB_CUDA(cudaGetLastError());
+  return true;
+}
+
+}  // namespace fb

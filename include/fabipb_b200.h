@@ -1,0 +1,108 @@
+/*
+ * fabipb_b200.h -- plain-pointer C ABI of the B200 FABIPB hot path.
+ *
+ * One context holds a molecular-surface mesh resident on one GPU: the octree
+ * (built exactly as the reference's gkInit, src/gkSetup.c:446-508), the leaf
+ * moment matrices, the near-field special-pair table and the FMM expansion
+ * storage.  Every operator the reference's GMRES matvec uses is then a few
+ * kernel launches on vectors that stay in HBM.
+ *
+ * Conventions (those of the reference):
+ *   - panels are given in mesh-face (input) order: vtx[9*i + 3*k + d] is
+ *     coordinate d of vertex k, normal[3*i + d], area[i];
+ *   - unknown vectors have length 2N in tree (pnlLst) order: entries [0,N)
+ *     are the potential part, [N,2N) the normal-derivative part.  The
+ *     permutation is returned by fabipb_b200_panel_order();
+ *   - every function returns 1 on success and 0 on failure, with a message
+ *     in fabipb_b200_last_error() (src/gpu_backend_cuda.cu:320-326 uses the
+ *     same 1/0 convention).  There is no CPU fallback anywhere: a failure is
+ *     reported, never silently recomputed on the host;
+ *   - `on_device` = 1 means the vector pointers are CUDA device pointers on
+ *     the context's device; 0 means host pointers (copied in and out inside
+ *     the call, the path the reference's plugin ABI takes).
+ */
+#ifndef FABIPB_B200_H
+#define FABIPB_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* arithmetic of the near field and the FMM passes */
+#define FABIPB_B200_FP64 0   /* everything in double */
+#define FABIPB_B200_MIXED 1  /* near-field P2P in float, singular pairs and
+                                the far field in double */
+
+/* which part of the boundary operator K an apply covers */
+#define FABIPB_B200_NEAR 1
+#define FABIPB_B200_FAR 2
+#define FABIPB_B200_ALL 3
+
+typedef struct fabipb_b200_params {
+  int order;          /* -p : >0 fixed Taylor order, <=0 variable (gkSetup.c:42) */
+  int order_mom;      /* -pm (default 0) */
+  int depth;          /* -t : octree depth */
+  int height;         /* -H : coarsest FMM level */
+  int quad_order;     /* -q : panel quadrature order (the device path needs 1) */
+  double sep_ratio;   /* -S : MAC separation ratio */
+  double kappa;       /* -k : Debye-Hueckel screening */
+  double eps1, eps2;  /* -eps1 -eps2 */
+  double rhs_theta;   /* charge-tree acceptance for the RHS (default 0.8) */
+  double energy_theta;/* charge-tree acceptance for the energy (default 0.8) */
+  int charge_order;   /* charge-tree Taylor order: >0 flat, 0 follow the FMM */
+  int precision;      /* FABIPB_B200_FP64 or FABIPB_B200_MIXED */
+  int device;         /* CUDA device ordinal */
+} fabipb_b200_params;
+
+typedef struct fabipb_b200_info {
+  int panels, leaves, near_pairs, m2l_pairs, cubes, max_order, leaf_order;
+  int max_leaf;
+  long long near_panel_pairs;  /* panel pairs the near field visits per apply */
+  long long special_pairs;     /* of those, pairs with a shared vertex/edge or self */
+  double setup_seconds;
+  double device_bytes;         /* device memory held by the context */
+} fabipb_b200_info;
+
+void fabipb_b200_default_params(fabipb_b200_params *p);
+
+int fabipb_b200_create(const fabipb_b200_params *p, int n_panels, const double *vtx,
+                       const double *normal, const double *area, void **ctx);
+int fabipb_b200_set_charges(void *ctx, int n_charges, const double *pos, const double *q);
+void fabipb_b200_destroy(void *ctx);
+int fabipb_b200_set_stream(void *ctx, void *cuda_stream);
+const char *fabipb_b200_last_error(void);
+
+/* tree queries, for parity checks against the reference layouts */
+int fabipb_b200_info_get(void *ctx, fabipb_b200_info *out);
+int fabipb_b200_panel_order(void *ctx, int *order);      /* tree index -> input index (N) */
+int fabipb_b200_leaf_layout(void *ctx, int *start, int *count);
+int fabipb_b200_near_pairs(void *ctx, int *src, int *dst);   /* fmm.c:234-268 order */
+int fabipb_b200_m2l_pairs(void *ctx, int *src, int *dst);    /* fmm.c:326-373 order */
+int fabipb_b200_cube_data(void *ctx, int *level, double *ctr4);
+
+/* pot = beta*pot + alpha*K_part*sgm  (applyFMM, src/fmm.c:710, and its
+   near/far halves) */
+int fabipb_b200_apply(void *ctx, int part, double alpha, const double *sgm, double beta,
+                      double *pot, int on_device);
+/* y = alpha*(D - K)x + beta*y  (MtVmain, src/fabipb.c:1237) */
+int fabipb_b200_matvec(void *ctx, double alpha, const double *x, double beta, double *y,
+                       int on_device);
+/* right-hand side, 2N in tree order (setupRHS, src/fabipb.c:744):
+   use_tree = 0 direct panel-charge sum, 1 charge-tree walk */
+int fabipb_b200_rhs(void *ctx, int use_tree, double *rhs, int on_device);
+/* raw solvation energy sum (before 2*pi*332.0716), panel-charge-tree walk
+   (applyPanelChargeTreeEnergy, src/treecode.c:927) */
+int fabipb_b200_energy(void *ctx, const double *sgm, double *raw, int on_device);
+/* preconditioner (src/precond_fmm.c): mode 2 block LU, 3 diagonal, -1 none */
+int fabipb_b200_precond_setup(void *ctx, int mode);
+int fabipb_b200_precond_apply(void *ctx, const double *b, double *x, int on_device);
+/* restarted left-preconditioned GMRES on the device (src/gmres.c:153);
+   x holds the initial guess on entry.  Returns info like the reference in
+   *info (0 converged, 1 iteration limit, 2 breakdown). */
+int fabipb_b200_solve(void *ctx, const double *b, double *x, int restart, int maxit,
+                      double tol, int *iters, double *resid, int *info, int on_device);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

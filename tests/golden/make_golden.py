@@ -1,0 +1,119 @@
+"""Generate the golden fixtures under tests/golden/ from the reference itself.
+
+    python tests/golden/make_golden.py
+
+Needs the reference CPU solver compiled from its own sources
+(``make -C oracle ref``, which reads the read-only reference mount).  For each
+small seeded case it writes ``<case>.npz`` holding what the reference
+computes on that mesh:
+
+* tree layout: panel order (mesh-face index per tree slot), leaf start/count,
+  near and M2L pair lists, FMM cube levels/centres/radii, panel areas;
+* one near-field apply and one full matvec (MtVmain) of a seeded density;
+* the direct and the charge-tree right-hand side (setupRHS);
+* the panel-tree energy of the seeded density;
+* the full CLI solve: solvation energy, GMRES iterations, final residual.
+
+The meshes themselves are regenerated by ``fabipb_b200.meshgen`` from the
+seeds recorded in ``cases.json``; a SHA-256 of the generated files is stored so
+a test can tell a generator change from a solver change.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "cuda-fabipb_b200"))
+sys.path.insert(0, ROOT)
+
+from fabipb_b200 import meshgen  # noqa: E402
+
+# name -> (generator, generator kwargs, reference options)
+CASES = {
+    "sphere320": ("sphere", dict(nsub=2, radius=20.0, n_charges=50, seed=3),
+                  dict(p=3, t=2, S=0.8, a=10, o=1e-4, eps1=1.0, eps2=80.0)),
+    "sphere1280": ("sphere", dict(nsub=3, radius=20.0, n_charges=100, seed=4),
+                   dict(p=3, t=3, S=0.8, a=10, o=1e-4, eps1=1.0, eps2=80.0)),
+    "star2048": ("star", dict(freq=16, radius=25.0, n_charges=300, seed=5),
+                 dict(p=4, t=3, S=0.7, a=10, o=1e-5, eps1=2.0, eps2=80.0)),
+    "shell1152": ("shell", dict(freq=12, r_in=20.0, r_out=26.0, n_charges=200, seed=6),
+                  dict(p=5, t=3, S=0.6, a=10, o=1e-6, eps1=2.0, eps2=80.0)),
+}
+
+
+def generate_mesh(name, directory):
+    kind, kw, _ = CASES[name]
+    base = os.path.join(directory, name)
+    fn = {"sphere": meshgen.sphere_case, "star": meshgen.star_case, "shell": meshgen.shell_case}[kind]
+    fn(base, **kw)
+    return base
+
+
+def mesh_digest(base):
+    h = hashlib.sha256()
+    for ext in (".vert", ".face", ".pqr"):
+        with open(base + ext, "rb") as fp:
+            h.update(fp.read())
+    return h.hexdigest()
+
+
+def ref_opts(opts, with_solver=False):
+    out = ["-p=%d" % opts["p"], "-t=%d" % opts["t"], "-S=%g" % opts["S"], "-eps1=%g" % opts["eps1"],
+           "-eps2=%g" % opts["eps2"]]
+    if with_solver:
+        out += ["-a=%d" % opts["a"], "-o=%g" % opts["o"]]
+    return out
+
+
+def seeded_sigma(n, seed=0):
+    return np.random.default_rng(seed).standard_normal(2 * n)
+
+
+def main():
+    from oracle import oracle as O
+    if not O.ref_available():
+        raise SystemExit("build the reference first: make -C oracle ref")
+    meta = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for name, (_, _, opts) in CASES.items():
+            base = generate_mesh(name, tmp)
+            pre = os.path.join(tmp, name + "_out")
+            o = ref_opts(opts)
+            O.run_ref_harness("tree", base, pre, o)
+            hdr = O.read_bin(pre, "hdr", np.int32)
+            n = int(hdr[0])
+            data = {"hdr": hdr}
+            for key, dt in (("order", np.int32), ("leafStart", np.int32), ("leafCount", np.int32),
+                            ("nearSrc", np.int32), ("nearDst", np.int32), ("m2lSrc", np.int32),
+                            ("m2lDst", np.int32), ("cubeLevel", np.int32), ("cubeCtr", np.float64),
+                            ("area", np.float64)):
+                data[key] = O.read_bin(pre, key, dt)
+            sg = seeded_sigma(n)
+            O.run_ref_harness("near", base, pre, o, sigma=sg)
+            data["near"] = O.read_bin(pre, "pot", np.float64)
+            O.run_ref_harness("matvec", base, pre, o, sigma=sg)
+            data["matvec"] = O.read_bin(pre, "pot", np.float64)
+            O.run_ref_harness("rhs", base, pre, o)
+            data["rhs"] = O.read_bin(pre, "rhs", np.float64)
+            O.run_ref_harness("rhs", base, pre, o, extra_env={"FABIPB_FORCE_TREE_RHS": "1"})
+            data["rhs_tree"] = O.read_bin(pre, "rhs", np.float64)
+            O.run_ref_harness("energy", base, pre, o, sigma=sg)
+            data["energy_raw"] = O.read_bin(pre, "energy", np.float64)
+            e, it, res, _ = O.run_ref_solve(base, ref_opts(opts, True), threads=4)
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), **data)
+            meta[name] = {"panels": n, "opts": opts, "digest": mesh_digest(base),
+                          "solve": {"energy": e, "iterations": it, "residual": res}}
+            print(name, n, "energy", e, "its", it, "resid", res)
+    with open(os.path.join(HERE, "cases.json"), "w") as fp:
+        json.dump(meta, fp, indent=1, sort_keys=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,96 @@
+"""GPU parity: the CUDA library against the FP64 restatement oracle and the
+reference goldens, through the C ABI (include/fabipb_b200.h).
+
+Tolerances:
+  * tree layouts: identical integers and bit-identical box centres;
+  * FP64 mode operators: relative L2 <= 1e-12 against the oracle;
+  * mixed (FP32 near-field P2P) mode: relative L2 <= 5e-6 for the near field
+    and the matvec.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import case_params, load_golden, rel_l2
+from fabipb_b200 import lib, meshio
+import make_golden
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+CASES = list(make_golden.CASES)
+
+
+def surface(case_dir, meta, name, precision):
+    pan, ch = meshio.load_case(os.path.join(case_dir, name))
+    prm = lib.params(precision=precision, **case_params(meta[name]["opts"]))
+    return lib.Surface(pan, prm), pan, ch
+
+
+@pytest.fixture(scope="module")
+def oracles(case_dir, golden_meta):
+    out = {}
+    for name in CASES:
+        pan, ch = meshio.load_case(os.path.join(case_dir, name))
+        out[name] = O.Oracle(pan, O.make_params(**case_params(golden_meta[name]["opts"])), ch)
+    return out
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_tree_matches_reference(name, case_dir, golden_meta):
+    g = load_golden(name)
+    s, pan, _ = surface(case_dir, golden_meta, name, lib.FP64)
+    info = s.info()
+    assert (info["panels"], info["leaves"], info["near_pairs"], info["m2l_pairs"], info["cubes"]) == \
+        tuple(int(v) for v in g["hdr"][:5])
+    assert np.array_equal(pan.face_index[s.panel_order()], g["order"])
+    st, ct = s.leaf_layout()
+    assert np.array_equal(st, g["leafStart"]) and np.array_equal(ct, g["leafCount"])
+    ns, nd = s.near_pairs()
+    assert np.array_equal(ns, g["nearSrc"]) and np.array_equal(nd, g["nearDst"])
+    ms, md = s.m2l_pairs()
+    assert np.array_equal(ms, g["m2lSrc"]) and np.array_equal(md, g["m2lDst"])
+    lev, ctr = s.cube_data()
+    assert np.array_equal(lev, g["cubeLevel"]) and np.array_equal(ctr.reshape(-1), g["cubeCtr"])
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("precision,tol", [(lib.FP64, 1e-12), (lib.MIXED, 5e-6)])
+def test_near_field(name, precision, tol, case_dir, golden_meta):
+    g = load_golden(name)
+    s, _, _ = surface(case_dir, golden_meta, name, precision)
+    sg = make_golden.seeded_sigma(s.n)
+    got = s.apply(sg, part=lib.NEAR)
+    assert rel_l2(got, g["near"]) < tol
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_far_field_fp64(name, case_dir, golden_meta, oracles):
+    s, _, _ = surface(case_dir, golden_meta, name, lib.FP64)
+    sg = make_golden.seeded_sigma(s.n, 3)
+    got = s.apply(sg, part=lib.FAR, alpha=0.5)
+    ref = oracles[name].far_apply(sg, 0.5, 0.0)
+    assert rel_l2(got, ref) < 1e-12
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("precision,tol", [(lib.FP64, 1e-12), (lib.MIXED, 5e-6)])
+def test_matvec(name, precision, tol, case_dir, golden_meta):
+    g = load_golden(name)
+    s, _, _ = surface(case_dir, golden_meta, name, precision)
+    sg = make_golden.seeded_sigma(s.n)
+    got = s.matvec(sg)
+    assert rel_l2(got, g["matvec"]) < tol
+
+
+def test_apply_alpha_beta_semantics(case_dir, golden_meta, oracles):
+    name = "star2048"
+    s, _, _ = surface(case_dir, golden_meta, name, lib.FP64)
+    rng = np.random.default_rng(5)
+    sg, y0 = rng.standard_normal(2 * s.n), rng.standard_normal(2 * s.n)
+    got = s.matvec(sg, alpha=-1.0, beta=1.0, y=y0)
+    ref = oracles[name].matvec(sg, -1.0, 1.0, y0)
+    assert rel_l2(got, ref) < 1e-12
+    got = s.apply(sg, part=lib.ALL, alpha=0.3, beta=-2.0, pot=y0)
+    ref = oracles[name].fmm_apply(sg, 0.3, -2.0, y0)
+    assert rel_l2(got, ref) < 1e-12
