@@ -1,0 +1,350 @@
+"""Benchmark of the FABIPB GMRES matvec on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision mixed|fp64] [--case star204800|sphere20480]
+
+Workload (one "step" = one operator application y = (D - K)x, the GMRES
+matvec of src/fabipb.c:1237): the star-shaped globular surface of 204,800
+flat triangles (octahedral geodesic, frequency 160, radius 25 A perturbed by
+l=2..6 harmonics), Taylor order p=4, MAC ratio 0.7, octree depth 5 (mean
+leaf 46 panels), eps 2/80, kappa 0.1257, synthetic seeded inputs.
+
+Reported:
+  value      matvec/s with x, y resident in HBM (device time, CUDA events on
+             the library's stream), L2 flushed between steps outside the
+             timed intervals;
+  e2e        matvec/s through the C ABI with host buffers (H2D of x and D2H
+             of y inside the timed region, pinned host memory);
+  roofline   the near-field P2P kernel (the dominant kernel): algorithmic
+             FLOPs (60 per panel pair) per launch / its event-timed duration,
+             against the FP32 SIMT peak of the measured SM clock;
+  cpu_baseline  the reference CPU solver compiled from its own sources
+             (oracle/_ref), timed on a bounded sample of matvecs on this
+             host's cores.
+With --impl reference the line times that reference CPU matvec itself.
+N>1 GPUs run independent replicas (the path does not shard: replicas only);
+value is the sum over replicas, timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cuda-fabipb_b200"))
+sys.path.insert(0, ROOT)
+
+CASES = {
+    # name: (generator, kwargs, solver options)
+    "star204800": ("star", dict(freq=160, radius=25.0, n_charges=20000, seed=1),
+                   dict(order=4, depth=5, sep_ratio=0.7, eps1=2.0, eps2=80.0, tol=1e-5, restart=10)),
+    "sphere20480": ("sphere", dict(nsub=5, radius=20.0, n_charges=500, seed=0),
+                    dict(order=3, depth=3, sep_ratio=0.8, eps1=1.0, eps2=80.0, tol=1e-4, restart=10)),
+}
+METRIC = "matvec/s"
+FLOP_PER_PAIR = 60.0   # algorithmic count per near panel pair (KER4 + apply)
+
+
+def case_base(name):
+    d = os.path.join(tempfile.gettempdir(), "fabipb_b200_cases")
+    os.makedirs(d, exist_ok=True)
+    base = os.path.join(d, name)
+    if not all(os.path.exists(base + e) for e in (".vert", ".face", ".pqr")):
+        from fabipb_b200 import meshgen
+        kind, kw, _ = CASES[name]
+        tmp = base + ".tmp%d" % os.getpid()
+        {"sphere": meshgen.sphere_case, "star": meshgen.star_case, "shell": meshgen.shell_case}[kind](tmp, **kw)
+        for e in (".vert", ".face", ".pqr"):
+            os.replace(tmp + e, base + e)
+    return base
+
+
+def ref_opts(opts):
+    return ["-p=%d" % opts["order"], "-t=%d" % opts["depth"], "-S=%g" % opts["sep_ratio"],
+            "-eps1=%g" % opts["eps1"], "-eps2=%g" % opts["eps2"]]
+
+
+def cpu_reference_rate(base, opts, reps, warmup=1, budget=60.0):
+    """matvec/s of the reference CPU solver (oracle/_ref) or, if it is absent,
+    of the FP64 restatement oracle; returns (value, kind, cores, sample).
+    At most `reps` timed matvecs, fewer if the warm-up matvec shows they would
+    exceed `budget` seconds (at least one is always timed)."""
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    if not O.ref_available() and os.path.isdir("/root/reference/src"):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=False,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+    if O.ref_available():
+        pre = os.path.join(tempfile.gettempdir(), "fabipb_ref_time")
+        out = O.run_ref_harness("time", base, pre, ref_opts(opts), threads=cores, reps=reps,
+                                warmup=max(warmup, 1), budget=budget)
+        r = json.loads(out.strip().splitlines()[-1])
+        return (r["matvec_per_s"], "reference", cores,
+                "%d timed matvecs (MtVmain) of the full mesh after %d warm-up" % (r["reps"], max(warmup, 1)))
+    from fabipb_b200 import meshio
+    pan, _ = meshio.load_case(base)
+    orc = O.Oracle(pan, O.make_params(order=opts["order"], depth=opts["depth"], sep_ratio=opts["sep_ratio"],
+                                      eps1=opts["eps1"], eps2=opts["eps2"], threads=cores))
+    x = np.random.default_rng(0).standard_normal(2 * pan.n)
+    w0 = time.perf_counter()
+    for _ in range(max(warmup, 1)):
+        orc.matvec(x)
+    reps = max(1, min(reps, int(budget / max(time.perf_counter() - w0, 1e-9))))
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        orc.matvec(x)
+    dt = time.perf_counter() - t0
+    return reps / dt, "port", cores, "%d timed matvecs of the full mesh (FP64 restatement)" % reps
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during timing."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.path = os.path.join(tempfile.gettempdir(), "fabipb_clocks_%d.csv" % os.getpid())
+        self.proc = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.fp = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.fp, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fp.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as fp:
+            for line in fp:
+                p = [v.strip() for v in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    smax = float(p[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, p[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+        load = [v for v in sm if smax and v > 0.3 * smax] or sm
+        return {"sm_mhz": float(np.median(load)) if load else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
+        pg = dist
+    return rank, world, local, pg
+
+
+def run_reference(args):
+    rank, world, local, pg = dist_setup(args)
+    name = args.case
+    opts = CASES[name][2]
+    if rank != 0:
+        if pg:
+            pg.destroy_process_group()
+        return
+    base = case_base(name)
+    t0 = time.perf_counter()
+    # one process: setup once, `warmup` untimed matvecs, then `steps` timed ones
+    value, kind, cores, sample = cpu_reference_rate(base, opts, args.steps, 1, budget=args.ref_budget)
+    wall = time.perf_counter() - t0
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "matvec/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded star surface, 204,800 panels)",
+            "config": {"workload": name, "panels": 204800 if name == "star204800" else 20480,
+                       "order": opts["order"], "depth": opts["depth"], "sep_ratio": opts["sep_ratio"]},
+            "cpu_baseline": {"value": value, "unit": "matvec/s", "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "matvec/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": wall}
+    if pg:
+        pg.destroy_process_group()
+    print(json.dumps(line))
+
+
+def run_ours(args):
+    import torch
+    from fabipb_b200 import lib, meshio
+
+    rank, world, local, pg = dist_setup(args)
+    torch.cuda.set_device(local)
+    name = args.case
+    opts = CASES[name][2]
+    base = case_base(name)
+    pan, ch = meshio.load_case(base)
+    prec = lib.MIXED if args.precision == "mixed" else lib.FP64
+    prm = lib.params(order=opts["order"], depth=opts["depth"], sep_ratio=opts["sep_ratio"], eps1=opts["eps1"],
+                     eps2=opts["eps2"], precision=prec, device=local)
+    surf = lib.Surface(pan, prm, ch)
+    info = surf.info()
+    n2 = 2 * surf.n
+    stream = torch.cuda.current_stream()
+    surf.set_stream(stream.cuda_stream)
+    x = torch.from_numpy(np.random.default_rng(rank).standard_normal(n2)).cuda()
+    y = torch.zeros(n2, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        surf.matvec(x.data_ptr(), 1.0, 0.0, y.data_ptr(), on_device=1)
+
+    def near_only():
+        surf.apply(x.data_ptr(), part=lib.NEAR, alpha=1.0, beta=1.0, pot=y.data_ptr(), on_device=1)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    launches0 = surf.launch_count()
+    with ClockSampler(local) as clk:
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        for i in range(args.steps):
+            flush.zero_()
+            starts[i].record(stream)
+            step()
+            ends[i].record(stream)
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+        launches = surf.launch_count() - launches0
+        # the dominant kernel alone, same stream, for the roofline
+        nstarts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        nends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        for i in range(args.steps):
+            flush.zero_()
+            nstarts[i].record(stream)
+            near_only()
+            nends[i].record(stream)
+        torch.cuda.synchronize()
+        # e2e: host buffers through the C ABI (pinned), copies inside the region
+        xh = torch.from_numpy(np.random.default_rng(rank + 7).standard_normal(n2)).pin_memory()
+        yh = torch.zeros(n2, dtype=torch.float64).pin_memory()
+        xh_np, yh_np = xh.numpy(), yh.numpy()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            surf.matvec(xh_np, 1.0, 0.0, yh_np)
+        e2e_s = time.perf_counter() - t0
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    near_ms = [s.elapsed_time(e) for s, e in zip(nstarts, nends)]
+    total_s = sum(step_ms) / 1000.0
+    e2e_rate = args.steps / e2e_s
+    if pg:
+        t = torch.tensor([total_s, e2e_s], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_s, e2e_s = float(t[0]), float(t[1])
+        e2e_rate = args.steps / e2e_s
+    value = world * args.steps / total_s
+    if rank != 0:
+        if pg:
+            pg.destroy_process_group()
+        return
+    clocks = clk.summary()
+    near_s = float(np.mean(near_ms)) / 1000.0
+    pairs = float(info["near_panel_pairs"])
+    achieved = FLOP_PER_PAIR * pairs / near_s / 1e12
+    sm_mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    props = torch.cuda.get_device_properties(local)
+    n_sm = props.multi_processor_count
+    if prec == lib.MIXED:
+        peak = n_sm * 128 * 2 * sm_mhz * 1e6 / 1e12
+        peak_src = "FP32 SIMT FMA pipe: %d SMs x 128 lanes x 2 flop x %.0f MHz (median SM clock sampled)" % (n_sm, sm_mhz)
+    else:
+        peak = n_sm * 64 * 2 * sm_mhz * 1e6 / 1e12
+        peak_src = "FP64 SIMT FMA pipe: %d SMs x 64 lanes x 2 flop x %.0f MHz (median SM clock sampled)" % (n_sm, sm_mhz)
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "near_apply_%s_traffic.json" % args.precision)
+    if os.path.exists(prof):
+        with open(prof) as fp:
+            traffic = json.load(fp).get("dram_bytes_per_launch")
+    cpu = None
+    if not args.no_cpu_baseline:
+        v, kind, cores, sample = cpu_reference_rate(base, opts, args.cpu_reps, 1, budget=30.0)
+        cpu = {"value": v, "unit": "matvec/s", "cores": cores, "kind": kind, "sample": sample}
+    line = {
+        "metric": METRIC, "value": value, "unit": "matvec/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * total_s / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec == lib.MIXED else "f64",
+        "data": "synthetic (seeded star surface, 20,000 seeded charges)",
+        "config": {"workload": name, "panels": surf.n, "order": opts["order"], "depth": opts["depth"],
+                   "sep_ratio": opts["sep_ratio"], "eps1": opts["eps1"], "eps2": opts["eps2"],
+                   "precision": args.precision, "parallelism": "replicas" if world > 1 else "single",
+                   "leaves": info["leaves"], "near_panel_pairs": info["near_panel_pairs"],
+                   "m2l_pairs": info["m2l_pairs"], "special_pairs": info["special_pairs"],
+                   "l2": "256 MiB buffer written between steps, outside the timed intervals"},
+        "e2e": {"value": e2e_rate * world, "unit": "matvec/s", "h2d_bytes_per_step": n2 * 8,
+                "d2h_bytes_per_step": n2 * 8},
+        "roofline": {"kernel": "near_apply_kernel<%s>" % ("float" if prec == lib.MIXED else "double"),
+                     "bound": "fp32" if prec == lib.MIXED else "fp64", "achieved": achieved, "peak": peak,
+                     "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": peak_src, "flop_per_pair": FLOP_PER_PAIR,
+                     "pairs_per_launch": pairs, "launch_ms": near_s * 1000.0},
+        "cpu_baseline": cpu,
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "setup_s": info["setup_seconds"],
+    }
+    if pg:
+        pg.destroy_process_group()
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--case", default="star204800", choices=sorted(CASES))
+    ap.add_argument("--cpu-reps", type=int, default=2)
+    ap.add_argument("--ref-budget", type=float, default=90.0,
+                    help="seconds of timed reference matvecs at most (--impl reference)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -142,6 +142,7 @@ __global__ void scale_kernel(double *v, double a, long long n) {
 }
 
 bool scale_vec(Context &c, double *v, double a, long long n) {
+  c.launches += 1;
   scale_kernel<<<ceil_div(n, 256), 256, 0, c.stream>>>(v, a, n);
   FB_CUDA(cudaGetLastError());
   return true;
@@ -292,6 +293,11 @@ int fabipb_b200_info_get(void *ctx, fabipb_b200_info *o) {
   o->setup_seconds = c->setupSeconds;
   o->device_bytes = (double)c->arena.bytes;
   return 1;
+}
+
+long long fabipb_b200_launch_count(void *ctx) {
+  if (ctx == nullptr) return -1;
+  return ((Context *)ctx)->launches;
 }
 
 int fabipb_b200_panel_order(void *ctx, int *order) {

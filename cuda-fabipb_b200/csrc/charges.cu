@@ -1,0 +1,425 @@
+// charges.cu -- right-hand side and solvation energy on the device.
+//
+//   direct RHS      setupRHS direct loop, src/fabipb.c:788-798, with the
+//                   panel quadrature of panelRHS/kernelRHS,
+//                   src/numQuad.c:786-819, src/kernel.c:152-167
+//   charge octree   buildChargeTree, src/chargeTree.c:228-307 (same cell
+//                   tests as the panel tree, over the charge bounding cube)
+//   charge moments  computeChgMoments, src/chargeTree.c:314-416
+//   cluster order   rhsChargeExpansionOrder, src/chargeTree.c:117-129
+//   tree RHS walk   rhsTreeWalkLocal, src/treecode.c:283-450
+//   energy walk     energyTreeWalk/panelEnergyTree, src/treecode.c:581-695,
+//                   summed as in panelEnergyWorker, src/treecode.c:869-887
+//
+// Each walk is one thread per panel with an explicit stack that pops the
+// children in index order, i.e. the reference's depth-first recursion and
+// its summation order.  Accepted clusters evaluate the Cartesian derivative
+// tensor (fmm.cu derivs<>) to order p+1 and contract it with the cluster
+// moments; leaves sum their charges directly.  All in FP64; the energy is
+// reduced per block and then in block order, so it is deterministic.
+#include <algorithm>
+#include <cstring>
+
+#include "context.cuh"
+#include "quad.cuh"
+
+namespace fb {
+
+struct ChargeTreeDev {
+  bool built = false;
+  int nCubes = 0, depth = 0, height = 0, maxStack = 0;
+  DevArena arena;
+  double *d_pos = nullptr, *d_chr = nullptr;   // in charge-tree leaf order
+  double *d_ctr = nullptr, *d_rad = nullptr;
+  int *d_level = nullptr, *d_kidStart = nullptr, *d_kidCount = nullptr;
+  int *d_itemStart = nullptr, *d_itemCount = nullptr, *d_order = nullptr;
+  double *d_mom = nullptr;                     // nCubes x NM
+  double *d_partial = nullptr;                 // energy partial sums
+  int partialCap = 0;
+  double *d_posOrig = nullptr, *d_chrOrig = nullptr;  // input order (direct RHS)
+};
+
+void free_charges(Context &c) {
+  if (c.ct) {
+    c.ct->arena.release();
+    delete c.ct;
+    c.ct = nullptr;
+  }
+}
+
+bool setup_charges(Context &c, int m, const double *pos, const double *q) {
+  free_charges(c);
+  c.nChar = m;
+  c.h_pos.assign(pos, pos + 3 * (size_t)m);
+  c.h_chr.assign(q, q + m);
+  c.ct = new ChargeTreeDev();
+  if (!c.ct->arena.upload(&c.ct->d_posOrig, c.h_pos, c.stream) ||
+      !c.ct->arena.upload(&c.ct->d_chrOrig, c.h_chr, c.stream))
+    return false;
+  return true;
+}
+
+// charge-tree Taylor order of a level (chargeTree.c:117-129)
+static int charge_order(const Context &c, int level) {
+  int order;
+  if (c.prm.charge_order > 0) order = c.prm.charge_order;
+  else order = std::max(c.pt.ordMom[level], 4);
+  return std::min(order, c.P);
+}
+
+static bool build_charge_tree(Context &c) {
+  ChargeTreeDev &d = *c.ct;
+  if (d.built) return true;
+  const int m = c.nChar;
+  const double *pos = c.h_pos.data();
+  double cminx = pos[0], cmaxx = pos[0], cminy = pos[1], cmaxy = pos[1], cminz = pos[2], cmaxz = pos[2];
+  for (int j = 1; j < m; j++) {
+    double x = pos[3 * (size_t)j], y = pos[3 * (size_t)j + 1], z = pos[3 * (size_t)j + 2];
+    cminx = cminx > x ? x : cminx; cmaxx = x > cmaxx ? x : cmaxx;
+    cminy = cminy > y ? y : cminy; cmaxy = y > cmaxy ? y : cmaxy;
+    cminz = cminz > z ? z : cminz; cmaxz = z > cmaxz ? z : cmaxz;
+  }
+  double length = (cmaxx - cminx) > (cmaxy - cminy) ? (cmaxx - cminx) : (cmaxy - cminy);
+  length = (cmaxz - cminz) > length ? (cmaxz - cminz) : length;
+  if (length <= 0.0) length = 1.0;
+  Octree t;
+  std::vector<int> sorted;
+  if (!build_octree(t, m, pos, c.pt.t.depth, c.pt.t.height, cminx, cminy, cminz, length, sorted)) return false;
+  octree_boxes_points(t, pos, sorted);
+  d.nCubes = t.nCubes;
+  d.depth = t.depth;
+  d.height = t.height;
+  d.maxStack = 7 * t.depth + 2;
+  const int NM = c.NM;
+  std::vector<int> order(t.nCubes, 0);
+  for (int cc = 0; cc < t.nCubes; cc++) order[cc] = (t.level[cc] >= t.height) ? charge_order(c, t.level[cc]) : 0;
+  // moments (computeChgLeafMoments / transM2Mchr), host FP64
+  std::vector<double> mom((size_t)t.nCubes * NM, 0.0);
+  std::vector<int> mi;  // multi-indices for orders <= P
+  std::vector<int> idx3((c.P + 2) * (c.P + 2) * (c.P + 2), 0);
+  std::vector<double> ifact3;
+  {
+    double fact[32];
+    fact[0] = 1.0;
+    for (int k = 1; k < 32; k++) fact[k] = fact[k - 1] * k;
+    int D = c.P + 2, i = 0;
+    for (int n = 0; n <= c.P; n++)
+      for (int a = 0; a <= n; a++)
+        for (int b = 0; b <= n - a; b++, i++) {
+          int cc = n - a - b;
+          idx3[(a * D + b) * D + cc] = i;
+          mi.push_back(a); mi.push_back(b); mi.push_back(cc);
+          ifact3.push_back(1.0 / (fact[a] * fact[b] * fact[cc]));
+        }
+  }
+  const int D = c.P + 2;
+  auto conv_vect = [&](int ord, const double *tr, double *cv) {
+    double f1[32], f2[32], f3[32];
+    f1[0] = f2[0] = f3[0] = 1.0;
+    for (int i = 1; i <= ord; i++) {
+      f1[i] = f1[i - 1] * tr[0]; f2[i] = f2[i - 1] * tr[1]; f3[i] = f3[i - 1] * tr[2];
+    }
+    int nmo = nmom(ord);
+    for (int i = 0; i < nmo; i++) {
+      cv[i] = f1[mi[3 * i]] * f2[mi[3 * i + 1]] * f3[mi[3 * i + 2]];
+      cv[i] *= ifact3[i];
+    }
+  };
+  std::vector<double> cv(NM);
+  for (int cc = t.levStart[t.depth]; cc < t.levStart[t.depth + 1]; cc++) {
+    int ord = order[cc], nmo = nmom(ord);
+    for (int k = 0; k < t.itemCount[cc]; k++) {
+      int j = sorted[t.itemStart[cc] + k];
+      double tr[3] = {pos[3 * (size_t)j] - t.x[3 * (size_t)cc], pos[3 * (size_t)j + 1] - t.x[3 * (size_t)cc + 1],
+                      pos[3 * (size_t)j + 2] - t.x[3 * (size_t)cc + 2]};
+      conv_vect(ord, tr, cv.data());
+      for (int i = 0; i < nmo; i++) mom[(size_t)cc * NM + i] += c.h_chr[j] * cv[i];
+    }
+  }
+  for (int lev = t.depth - 1; lev >= t.height; lev--) {
+    for (int cc = t.levStart[lev]; cc < t.levStart[lev + 1]; cc++) {
+      int ordOut = order[cc];
+      for (int k = 0; k < t.kidCount[cc]; k++) {
+        int kid = t.kidStart[cc] + k, nIn = nmom(order[kid]);
+        double tr[3] = {t.x[3 * (size_t)kid] - t.x[3 * (size_t)cc], t.x[3 * (size_t)kid + 1] - t.x[3 * (size_t)cc + 1],
+                        t.x[3 * (size_t)kid + 2] - t.x[3 * (size_t)cc + 2]};
+        conv_vect(ordOut, tr, cv.data());
+        int nOut = nmom(ordOut);
+        for (int i = 0; i < nOut; i++) {
+          int i1 = mi[3 * i], i2 = mi[3 * i + 1], i3 = mi[3 * i + 2];
+          double tmp = 0.0;
+          for (int k1 = 0; k1 <= i1; k1++)
+            for (int k2 = 0; k2 <= i2; k2++)
+              for (int k3 = 0; k3 <= i3; k3++) {
+                int bi = idx3[(k1 * D + k2) * D + k3];
+                if (bi < nIn) tmp += cv[idx3[((i1 - k1) * D + (i2 - k2)) * D + (i3 - k3)]] * mom[(size_t)kid * NM + bi];
+              }
+          mom[(size_t)cc * NM + i] += tmp;
+        }
+      }
+    }
+  }
+  std::vector<double> spos(3 * (size_t)m), schr(m);
+  for (int i = 0; i < m; i++) {
+    for (int k = 0; k < 3; k++) spos[3 * (size_t)i + k] = pos[3 * (size_t)sorted[i] + k];
+    schr[i] = c.h_chr[sorted[i]];
+  }
+  cudaStream_t s = c.stream;
+  if (!d.arena.upload(&d.d_pos, spos, s) || !d.arena.upload(&d.d_chr, schr, s) ||
+      !d.arena.upload(&d.d_ctr, t.x, s) || !d.arena.upload(&d.d_rad, t.rad, s) ||
+      !d.arena.upload(&d.d_level, t.level, s) || !d.arena.upload(&d.d_kidStart, t.kidStart, s) ||
+      !d.arena.upload(&d.d_kidCount, t.kidCount, s) || !d.arena.upload(&d.d_itemStart, t.itemStart, s) ||
+      !d.arena.upload(&d.d_itemCount, t.itemCount, s) || !d.arena.upload(&d.d_order, order, s) ||
+      !d.arena.upload(&d.d_mom, mom, s))
+    return false;
+  FB_CUDA(cudaStreamSynchronize(s));  // host vectors above are about to go out of scope
+  d.built = true;
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// direct RHS: thread per panel, charges staged through shared memory
+// ---------------------------------------------------------------------------
+constexpr int kRhsTile = 256;
+
+__global__ void rhs_direct_kernel(int n, int m, int q, const double *__restrict__ vtx, const double *__restrict__ nrm,
+                                  const double *__restrict__ area, const double *__restrict__ pos,
+                                  const double *__restrict__ chr, double fac, double *rhs) {
+  __shared__ double4 sc[kRhsTile];
+  const int X = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = X < n;
+  const int Xs = valid ? X : 0;
+  const double *v0 = vtx + 9 * (size_t)Xs;
+  double ax2[3], ax0[3], nx[3];
+  for (int k = 0; k < 3; k++) {
+    ax2[k] = v0[3 + k] - v0[k];
+    ax0[k] = v0[6 + k] - v0[3 + k];
+    nx[k] = nrm[3 * (size_t)Xs + k];
+  }
+  const double A2 = 2.0 * area[Xs];
+  const double *t = c_tLeg[q], *w = c_wLeg[q];
+  double s0 = 0.0, s1 = 0.0;
+  for (int base = 0; base < m; base += kRhsTile) {
+    const int cnt = min(kRhsTile, m - base);
+    for (int j = threadIdx.x; j < cnt; j += blockDim.x)
+      sc[j] = make_double4(pos[3 * (size_t)(base + j)], pos[3 * (size_t)(base + j) + 1], pos[3 * (size_t)(base + j) + 2],
+                           chr[base + j]);
+    __syncthreads();
+    for (int j = 0; j < cnt; j++) {
+      const double4 cj = sc[j];
+      const double r0[3] = {v0[0] - cj.x, v0[1] - cj.y, v0[2] - cj.z};
+      double i0 = 0.0, i1 = 0.0;
+      for (int ix = 0; ix < q; ix++)
+        for (int jx = 0; jx < q; jx++) {
+          double r[3];
+          for (int k = 0; k < 3; k++) r[k] = r0[k] + t[ix] * (ax2[k] + t[jx] * ax0[k]);
+          const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+          const double ri = 1.0 / sqrt(r2);
+          const double r3i = ri / r2;
+          const double ip = nx[0] * r[0] + nx[1] * r[1] + nx[2] * r[2];
+          i0 += ri * t[ix] * w[ix] * w[jx];
+          i1 += (-ip * r3i) * t[ix] * w[ix] * w[jx];
+        }
+      s0 += cj.w * (i0 * A2);
+      s1 += cj.w * (i1 * A2);
+    }
+    __syncthreads();
+  }
+  if (valid) {
+    rhs[X] = s0 * fac;
+    rhs[n + X] = s1 * fac;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// charge-tree walks: mode 0 = RHS (Coulomb), mode 1 = energy (G0 - Gk)
+// ---------------------------------------------------------------------------
+template <int PM>
+__device__ void walk_point(int mode, const double *qp, const double *nx, double theta, int height, int depth,
+                           double kappa, double eps, int NM, const double *__restrict__ ctr,
+                           const double *__restrict__ rad, const int *__restrict__ level,
+                           const int *__restrict__ kidStart, const int *__restrict__ kidCount,
+                           const int *__restrict__ itemStart, const int *__restrict__ itemCount,
+                           const int *__restrict__ order, const double *__restrict__ mom,
+                           const double *__restrict__ pos, const double *__restrict__ chr, double *y) {
+  constexpr int ND = nmom_c(PM);
+  int stack[8 * 20 + 4];
+  int sp = 0;
+  stack[sp++] = 0;
+  double d0[ND], dk[ND];
+  while (sp > 0) {
+    const int c = stack[--sp];
+    double r[3] = {qp[0] - ctr[3 * c], qp[1] - ctr[3 * c + 1], qp[2] - ctr[3 * c + 2]};
+    const double dist = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    if (rad[c] < theta * dist && level[c] >= height) {
+      const int ord = order[c], nmo = nmom(ord);
+      derivs<PM>(ord + 1, r, kappa, mode == 0, d0, dk);
+      const double *mc = mom + (size_t)c * NM;
+      double y0 = 0.0, y1 = 0.0;
+      for (int i = 0; i < nmo; i++) {
+        const char4 a = c_mi[i];
+        const int e1 = IDX(a.x + 1, a.y, a.z), e2 = IDX(a.x, a.y + 1, a.z), e3 = IDX(a.x, a.y, a.z + 1);
+        const double sm = c_sgn3[i] * mc[i];
+        if (mode == 0) {
+          y0 += sm * d0[i];
+          y1 += sm * (nx[0] * d0[e1] + nx[1] * d0[e2] + nx[2] * d0[e3]);
+        } else {
+          y0 += sm * (d0[i] - dk[i]);
+          const double dn0 = nx[0] * d0[e1] + nx[1] * d0[e2] + nx[2] * d0[e3];
+          const double dnk = nx[0] * dk[e1] + nx[1] * dk[e2] + nx[2] * dk[e3];
+          y1 += sm * (eps * dnk - dn0);
+        }
+      }
+      if (mode == 0) {
+        y[0] += y0 / kFourPiI;
+        y[1] += y1 / kFourPiI;
+      } else {
+        y[0] += y0;
+        y[1] += y1;
+      }
+      continue;
+    }
+    if (level[c] == depth) {
+      const int s0 = itemStart[c], s1 = s0 + itemCount[c];
+      for (int j = s0; j < s1; j++) {
+        const double x[3] = {qp[0] - pos[3 * (size_t)j], qp[1] - pos[3 * (size_t)j + 1], qp[2] - pos[3 * (size_t)j + 2]};
+        const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+        const double ip = nx[0] * x[0] + nx[1] * x[1] + nx[2] * x[2];
+        if (mode == 0) {
+          const double ri = 1.0 / sqrt(r2), r3i = ri / r2;
+          y[0] += chr[j] * ri;
+          y[1] += chr[j] * (-ip * r3i);
+        } else {
+          const double rn = sqrt(r2), G0 = kFourPiI / rn, ek = exp(-kappa * rn);
+          const double Gk = ek * G0, coef = (kappa * rn + 1.0) * ek;
+          const double dG0dn = -ip * G0 / r2, dGkdn = coef * dG0dn;
+          y[0] += chr[j] * (G0 - Gk);
+          y[1] += chr[j] * (eps * dGkdn - dG0dn);
+        }
+      }
+      continue;
+    }
+    // children pop in index order
+    for (int k = kidCount[c] - 1; k >= 0; k--) stack[sp++] = kidStart[c] + k;
+  }
+}
+
+template <int PM>
+__global__ void tree_walk_kernel(int mode, int n, int q, const double *__restrict__ vtx, const double *__restrict__ nrm,
+                                 const double *__restrict__ area, double theta, int height, int depth, double kappa,
+                                 double eps, int NM, const double *__restrict__ ctr, const double *__restrict__ rad,
+                                 const int *__restrict__ level, const int *__restrict__ kidStart,
+                                 const int *__restrict__ kidCount, const int *__restrict__ itemStart,
+                                 const int *__restrict__ itemCount, const int *__restrict__ order,
+                                 const double *__restrict__ mom, const double *__restrict__ pos,
+                                 const double *__restrict__ chr, double fac, const double *__restrict__ sgm,
+                                 double *rhs, double *partial) {
+  __shared__ double red[256];
+  const int X = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0.0;
+  if (X < n) {
+    const double *v0 = vtx + 9 * (size_t)X;
+    double ax2[3], ax0[3], nx[3];
+    for (int k = 0; k < 3; k++) {
+      ax2[k] = v0[3 + k] - v0[k];
+      ax0[k] = v0[6 + k] - v0[3 + k];
+      nx[k] = nrm[3 * (size_t)X + k];
+    }
+    const double *t = c_tLeg[q], *w = c_wLeg[q];
+    double o0 = 0.0, o1 = 0.0;
+    for (int ix = 0; ix < q; ix++)
+      for (int jx = 0; jx < q; jx++) {
+        double qp[3], y[2] = {0.0, 0.0};
+        for (int k = 0; k < 3; k++) qp[k] = v0[k] + t[ix] * (ax2[k] + t[jx] * ax0[k]);
+        walk_point<PM>(mode, qp, nx, theta, height, depth, kappa, eps, NM, ctr, rad, level, kidStart, kidCount,
+                       itemStart, itemCount, order, mom, pos, chr, y);
+        o0 += y[0] * t[ix] * w[ix] * w[jx];
+        o1 += y[1] * t[ix] * w[ix] * w[jx];
+      }
+    o0 *= 2.0 * area[X];
+    o1 *= 2.0 * area[X];
+    if (mode == 0) {
+      rhs[X] = fac * o0;
+      rhs[n + X] = fac * o1;
+    } else {
+      e = o0 * sgm[X + n] + o1 * sgm[X];
+    }
+  }
+  if (mode == 1) {
+    red[threadIdx.x] = e;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) partial[blockIdx.x] = red[0];
+  }
+}
+
+__global__ void sum_partials_kernel(int k, const double *__restrict__ p, double *out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double s = 0.0;
+    for (int i = 0; i < k; i++) s += p[i];
+    *out = s;
+  }
+}
+
+template <int PM>
+static void launch_walk(Context &c, int mode, const double *sgm, double *rhs, double *partial) {
+  ChargeTreeDev &d = *c.ct;
+  const double theta = (mode == 0) ? c.prm.rhs_theta : c.prm.energy_theta;
+  tree_walk_kernel<PM><<<ceil_div(c.n, 256), 256, 0, c.stream>>>(
+      mode, c.n, c.prm.quad_order, c.d_vtx, c.d_nrm, c.d_area, theta, d.height, d.depth, c.prm.kappa, c.epsilon,
+      c.NM, d.d_ctr, d.d_rad, d.d_level, d.d_kidStart, d.d_kidCount, d.d_itemStart, d.d_itemCount, d.d_order,
+      d.d_mom, d.d_pos, d.d_chr, kFourPiI / c.prm.eps1, sgm, rhs, partial);
+}
+
+#define FB_DISPATCH_WALK(P, ...)                      \
+  switch (P) {                                        \
+    case 1: launch_walk<2>(__VA_ARGS__); break;       \
+    case 2: launch_walk<3>(__VA_ARGS__); break;       \
+    case 3: launch_walk<4>(__VA_ARGS__); break;       \
+    case 4: launch_walk<5>(__VA_ARGS__); break;       \
+    case 5: launch_walk<6>(__VA_ARGS__); break;       \
+    case 6: launch_walk<7>(__VA_ARGS__); break;       \
+    case 7: launch_walk<8>(__VA_ARGS__); break;       \
+    default: launch_walk<9>(__VA_ARGS__); break;      \
+  }
+
+bool launch_rhs(Context &c, int useTree, double *rhs) {
+  FB_CHECK(c.ct != nullptr && c.nChar > 0, "no charges set (fabipb_b200_set_charges)");
+  FB_CHECK(c.prm.quad_order >= 1 && c.prm.quad_order <= 10, "quadrature order %d outside 1..10", c.prm.quad_order);
+  c.launches += 1;
+  if (!useTree) {
+    rhs_direct_kernel<<<ceil_div(c.n, 128), 128, 0, c.stream>>>(c.n, c.nChar, c.prm.quad_order, c.d_vtx, c.d_nrm,
+                                                                c.d_area, c.ct->d_posOrig, c.ct->d_chrOrig,
+                                                                kFourPiI / c.prm.eps1, rhs);
+    FB_CUDA(cudaGetLastError());
+    return true;
+  }
+  if (!build_charge_tree(c)) return false;
+  FB_CHECK(c.ct->depth <= 20, "charge tree depth %d above the walk stack limit", c.ct->depth);
+  FB_DISPATCH_WALK(c.P, c, 0, nullptr, rhs, nullptr);
+  FB_CUDA(cudaGetLastError());
+  return true;
+}
+
+bool launch_energy(Context &c, const double *sgm, double *raw_host) {
+  FB_CHECK(c.ct != nullptr && c.nChar > 0, "no charges set (fabipb_b200_set_charges)");
+  if (!build_charge_tree(c)) return false;
+  ChargeTreeDev &d = *c.ct;
+  const int blocks = (int)ceil_div(c.n, 256);
+  if (d.partialCap < blocks + 1) {
+    if (!d.arena.alloc_n(&d.d_partial, (size_t)blocks + 1)) return false;
+    d.partialCap = blocks + 1;
+  }
+  FB_DISPATCH_WALK(c.P, c, 1, sgm, nullptr, d.d_partial);
+  c.launches += 2;
+  sum_partials_kernel<<<1, 32, 0, c.stream>>>(blocks, d.d_partial, d.d_partial + blocks);
+  FB_CUDA(cudaGetLastError());
+  FB_CUDA(cudaMemcpyAsync(raw_host, d.d_partial + blocks, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  FB_CUDA(cudaStreamSynchronize(c.stream));
+  return true;
+}
+
+}  // namespace fb

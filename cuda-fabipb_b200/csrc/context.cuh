@@ -74,6 +74,7 @@ struct Context {
   GraphCache *graphs = nullptr;
 
   double setupSeconds = 0.0;
+  long long launches = 0;                  // kernels launched by this context
   ~Context();
 };
 

@@ -3,5 +3,6 @@
 // every kernel without relocatable device code.
 #include "near.cu"
 #include "fmm.cu"
-#include "stubs_tmp.cu"
+#include "charges.cu"
+#include "solver.cu"
 #include "api.cu"

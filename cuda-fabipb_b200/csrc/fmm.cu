@@ -549,6 +549,7 @@ bool launch_far_upward(Context &c, const double *sgm) {
   const size_t plane = (size_t)pt.nFmm * c.NM;
   FB_CUDA(cudaMemsetAsync(c.d_mom, 0, 2 * plane * sizeof(double), s));
   FB_CUDA(cudaMemsetAsync(c.d_lec, 0, 4 * plane * sizeof(double), s));
+  c.launches += 1 + 2 * (depth - height);
   q2m_kernel<<<pt.nLeaves, 256, 0, s>>>(pt.nLeaves, c.n, c.NMleaf, c.NM, c.d_leafStart, c.d_leafCount, c.d_leafFmm,
                                         c.d_Q0, c.d_Q1, sgm, c.d_mom, c.d_mom + plane);
   for (int lev = depth - 1; lev >= height; lev--) {
@@ -575,12 +576,14 @@ bool launch_far_upward(Context &c, const double *sgm) {
 bool launch_m2l_only(Context &c) {
   if (c.h_m2lDst.empty()) return true;
   FB_DISPATCH_ORDER(c.P, launch_m2l_t, c);
+  c.launches += 1;
   FB_CUDA(cudaGetLastError());
   return true;
 }
 
 bool launch_l2p(Context &c, double alpha, double beta, double *out, const double *diagX, double s1, double s2) {
   const size_t plane = (size_t)c.pt.nFmm * c.NM;
+  c.launches += 1;
   l2p_kernel<<<ceil_div(c.n, 256), 256, 0, c.stream>>>(c.n, c.NMleaf, c.NM, c.d_leafOfPanel, c.d_leafFmm, c.d_Q0,
                                                        c.d_Q1, c.d_lec, c.d_lec + plane, c.d_lec + 2 * plane,
                                                        c.d_lec + 3 * plane, alpha, beta, c.d_area, diagX, s1, s2, out);

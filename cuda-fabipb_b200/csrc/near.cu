@@ -365,6 +365,7 @@ bool launch_near(Context &c, const double *sgm, double coef, double *out) {
         (const double4 *)c.d_srcB, c.d_spOff, c.d_spSrc, c.d_spK, sgm, c.d_area, n, kap, -kap, eps, 1.0 / eps,
         kap * kap, coef, out);
   }
+  c.launches += 2;
   FB_CUDA(cudaGetLastError());
   return true;
 }

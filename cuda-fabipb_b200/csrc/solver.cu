@@ -1,0 +1,436 @@
+// solver.cu -- preconditioner and restarted GMRES, resident on the device.
+//
+//   block preconditioner   src/precond_fmm.c:147-263, 553-652: one dense block
+//                          per level (depth-1) cube, 2*nPnls square, entries
+//                          block[i*M+j] from panelIA0(pnlX=j, pnlY=i) which
+//                          LAPACK reads column-major, plus the area diagonal;
+//                          LU-factored once (dgetrf)
+//   cached-LU apply        src/precond_fmm.c:861-953 (dgetrs per block)
+//   diagonal apply         src/precond_fmm.c:664-728
+//   GMRES                  src/gmres.c:153-373 (Templates GMRES, left
+//                          preconditioned, modified Gram-Schmidt basis,
+//                          Givens rotations, x0 = initial guess)
+//
+// B200 design: the block matrices are assembled by a kernel in FP64 (the
+// exact panelIA0 cases), factored with cuSOLVER at setup, and replaced by
+// their explicit inverses, so each preconditioner apply is one block-diagonal
+// GEMV kernel streaming the inverses from HBM instead of ~3 launches per
+// block.  The Krylov vectors live on the device; the Gram-Schmidt dot
+// products are reduced deterministically into a device array and only the
+// (restart+1)-long Hessenberg column crosses to the host per iteration, where
+// the Givens rotations run in FP64 exactly as in the reference.
+#include <cusolverDn.h>
+
+#include <cmath>
+#include <vector>
+
+#include "context.cuh"
+#include "quad.cuh"
+
+namespace fb {
+
+struct PrecondDev {
+  int mode = -1;
+  DevArena arena;
+  int nBlocks = 0;
+  std::vector<int> hStart, hSize;
+  std::vector<long long> hOff;
+  int *d_start = nullptr, *d_size = nullptr;
+  long long *d_off = nullptr;
+  double *d_inv = nullptr;
+  int maxM = 0;
+  // GMRES workspace
+  int restart = 0;
+  double *d_V = nullptr, *d_r = nullptr, *d_av = nullptr, *d_w = nullptr;
+  double *d_h = nullptr, *d_part = nullptr, *d_y = nullptr;
+  int partCap = 0;
+};
+
+void free_precond(Context &c) {
+  if (c.pc) {
+    c.pc->arena.release();
+    delete c.pc;
+    c.pc = nullptr;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// block assembly: A(j, i) = -K1(X=j,Y=i) etc. in column-major M x M
+// ---------------------------------------------------------------------------
+__global__ void pc_assemble_kernel(int nBlocks, const int *__restrict__ bStart, const int *__restrict__ bSize,
+                                   const long long *__restrict__ bOff, const double *__restrict__ vtx,
+                                   const double *__restrict__ nrm, const double *__restrict__ area, int q,
+                                   double kappa, double eps, double s1, double s2, double *A) {
+  const int b = blockIdx.y;
+  if (b >= nBlocks) return;
+  const int hm = bSize[b], st = bStart[b], M = 2 * hm;
+  const long long pairs = (long long)hm * hm;
+  double *Ab = A + bOff[b];
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < pairs;
+       p += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(p / hm), j = (int)(p % hm);  // i: pnlY (column), j: pnlX (row)
+    const int Xi = st + j, Yi = st + i;
+    PanelD X, Y;
+    const double *vx = vtx + 9 * (size_t)Xi, *vy = vtx + 9 * (size_t)Yi;
+    for (int k = 0; k < 3; k++)
+      for (int c = 0; c < 3; c++) { X.v[k][c] = vx[3 * k + c]; Y.v[k][c] = vy[3 * k + c]; }
+    for (int c = 0; c < 3; c++) {
+      X.a[0][c] = X.v[2][c] - X.v[1][c]; X.a[1][c] = X.v[0][c] - X.v[2][c]; X.a[2][c] = X.v[1][c] - X.v[0][c];
+      Y.a[0][c] = Y.v[2][c] - Y.v[1][c]; Y.a[1][c] = Y.v[0][c] - Y.v[2][c]; Y.a[2][c] = Y.v[1][c] - Y.v[0][c];
+      X.n[c] = nrm[3 * (size_t)Xi + c];
+      Y.n[c] = nrm[3 * (size_t)Yi + c];
+    }
+    X.area = area[Xi];
+    Y.area = area[Yi];
+    double K[4];
+    panel_ia0_d(q, kappa, eps, X, Y, Xi == Yi, K, nullptr);
+    double d0 = (i == j) ? s1 * area[Yi] : 0.0;
+    double d1 = (i == j) ? s2 * area[Yi] : 0.0;
+    Ab[(size_t)i * M + j] = -K[1] + d0;
+    Ab[(size_t)i * M + j + hm] = -K[0];
+    Ab[(size_t)(i + hm) * M + j] = -K[3];
+    Ab[(size_t)(i + hm) * M + j + hm] = -K[2] + d1;
+  }
+}
+
+__global__ void identity_kernel(int nBlocks, const int *__restrict__ bSize, const long long *__restrict__ bOff,
+                                double *I) {
+  const int b = blockIdx.y;
+  if (b >= nBlocks) return;
+  const int M = 2 * bSize[b];
+  const long long e = (long long)M * M;
+  double *Ib = I + bOff[b];
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < e; p += (long long)gridDim.x * blockDim.x)
+    Ib[p] = ((p / M) == (p % M)) ? 1.0 : 0.0;
+}
+
+// x = blockdiag(inv) * b, block b gathers its pot/dpdn halves
+__global__ void pc_apply_kernel(int n, const int *__restrict__ bStart, const int *__restrict__ bSize,
+                                const long long *__restrict__ bOff, const double *__restrict__ inv,
+                                const double *__restrict__ rhs, double *x) {
+  extern __shared__ double sb[];
+  const int b = blockIdx.x;
+  const int hm = bSize[b], st = bStart[b], M = 2 * hm;
+  for (int c = threadIdx.x; c < M; c += blockDim.x) sb[c] = (c < hm) ? rhs[st + c] : rhs[n + st + c - hm];
+  __syncthreads();
+  const double *Ib = inv + bOff[b];
+  for (int r = threadIdx.x; r < M; r += blockDim.x) {
+    double y = 0.0;
+    for (int c = 0; c < M; c++) y += Ib[(size_t)c * M + r] * sb[c];
+    if (r < hm) x[st + r] = y;
+    else x[n + st + r - hm] = y;
+  }
+}
+
+__global__ void pc_diag_kernel(int n, const double *__restrict__ area, double s1, double s2,
+                               const double *__restrict__ b, double *x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  x[i] = b[i] / (s1 * area[i]);
+  x[n + i] = b[n + i] / (s2 * area[i]);
+}
+
+bool precond_setup(Context &c, int mode) {
+  free_precond(c);
+  c.pc = new PrecondDev();
+  PrecondDev &p = *c.pc;
+  p.mode = mode;
+  if (mode != 2) return true;   // -1 identity and 3 diagonal need no setup
+  const Octree &t = c.pt.t;
+  const int lev = t.depth - 1;
+  FB_CHECK(lev >= 0, "block preconditioner needs depth >= 1");
+  long long off = 0;
+  for (int cc = t.levStart[lev]; cc < t.levStart[lev + 1]; cc++) {
+    int hm = t.itemCount[cc];
+    p.hStart.push_back(t.itemStart[cc]);
+    p.hSize.push_back(hm);
+    p.hOff.push_back(off);
+    off += 4LL * hm * hm;
+    p.maxM = std::max(p.maxM, 2 * hm);
+  }
+  p.nBlocks = (int)p.hSize.size();
+  FB_CHECK(p.maxM <= 46340, "preconditioner block %d too large (increase -t)", p.maxM);
+  cudaStream_t s = c.stream;
+  double *d_A = nullptr;
+  if (!p.arena.upload(&p.d_start, p.hStart, s) || !p.arena.upload(&p.d_size, p.hSize, s) ||
+      !p.arena.upload(&p.d_off, p.hOff, s) || !p.arena.alloc_n(&p.d_inv, (size_t)off))
+    return false;
+  FB_CUDA(cudaMalloc((void **)&d_A, (size_t)off * sizeof(double)));
+  const double s1 = (1.0 + c.epsilon) / 2.0, s2 = (1.0 + 1.0 / c.epsilon) / 2.0;
+  dim3 grid(64, p.nBlocks);
+  pc_assemble_kernel<<<grid, 128, 0, s>>>(p.nBlocks, p.d_start, p.d_size, p.d_off, c.d_vtx, c.d_nrm, c.d_area,
+                                          c.prm.quad_order, c.prm.kappa, c.epsilon, s1, s2, d_A);
+  identity_kernel<<<grid, 256, 0, s>>>(p.nBlocks, p.d_size, p.d_off, p.d_inv);
+  c.launches += 2;
+  cudaError_t le = cudaGetLastError();
+  if (le != cudaSuccess) {
+    cudaFree(d_A);
+    set_error("preconditioner assembly launch failed: %s", cudaGetErrorString(le));
+    return false;
+  }
+  cusolverDnHandle_t h = nullptr;
+  if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) {
+    cudaFree(d_A);
+    set_error("cusolverDnCreate failed");
+    return false;
+  }
+  cusolverDnSetStream(h, s);
+  int lwork = 0, *d_piv = nullptr, *d_info = nullptr;
+  double *d_work = nullptr;
+  bool ok = true;
+  if (cusolverDnDgetrf_bufferSize(h, p.maxM, p.maxM, d_A, p.maxM, &lwork) != CUSOLVER_STATUS_SUCCESS) ok = false;
+  ok = ok && cudaMalloc((void **)&d_work, (size_t)std::max(lwork, 1) * sizeof(double)) == cudaSuccess;
+  ok = ok && cudaMalloc((void **)&d_piv, (size_t)p.maxM * sizeof(int)) == cudaSuccess;
+  ok = ok && cudaMalloc((void **)&d_info, (size_t)p.nBlocks * sizeof(int)) == cudaSuccess;
+  for (int b = 0; ok && b < p.nBlocks; b++) {
+    int M = 2 * p.hSize[b];
+    if (M == 0) continue;
+    double *Ab = d_A + p.hOff[b], *Ib = p.d_inv + p.hOff[b];
+    if (cusolverDnDgetrf(h, M, M, Ab, M, d_work, d_piv, d_info + b) != CUSOLVER_STATUS_SUCCESS) ok = false;
+    if (ok && cusolverDnDgetrs(h, CUBLAS_OP_N, M, M, Ab, M, d_piv, Ib, M, d_info + b) != CUSOLVER_STATUS_SUCCESS)
+      ok = false;
+  }
+  std::vector<int> info(p.nBlocks, 0);
+  if (ok) ok = cudaMemcpyAsync(info.data(), d_info, info.size() * sizeof(int), cudaMemcpyDeviceToHost, s) == cudaSuccess;
+  if (ok) ok = cudaStreamSynchronize(s) == cudaSuccess;
+  cusolverDnDestroy(h);
+  cudaFree(d_work);
+  cudaFree(d_piv);
+  cudaFree(d_info);
+  cudaFree(d_A);
+  FB_CHECK(ok, "preconditioner factorisation failed: %s", cudaGetErrorString(cudaGetLastError()));
+  for (int b = 0; b < p.nBlocks; b++)
+    FB_CHECK(info[b] == 0, "dgetrf failed in preconditioner block %d (info=%d)", b, info[b]);
+  return true;
+}
+
+bool precond_apply(Context &c, const double *b, double *x) {
+  FB_CHECK(c.pc != nullptr, "preconditioner not set up");
+  PrecondDev &p = *c.pc;
+  if (p.mode == 2) {
+    pc_apply_kernel<<<p.nBlocks, 256, (size_t)p.maxM * sizeof(double), c.stream>>>(c.n, p.d_start, p.d_size, p.d_off,
+                                                                                 p.d_inv, b, x);
+  } else if (p.mode == 3) {
+    pc_diag_kernel<<<ceil_div(c.n, 256), 256, 0, c.stream>>>(c.n, c.d_area, (1.0 + c.epsilon) / 2.0,
+                                                            (1.0 + 1.0 / c.epsilon) / 2.0, b, x);
+  } else {
+    FB_CUDA(cudaMemcpyAsync(x, b, 2 * (size_t)c.n * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
+    return true;
+  }
+  c.launches += 1;
+  FB_CUDA(cudaGetLastError());
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// level-1 kernels with deterministic reductions
+// ---------------------------------------------------------------------------
+constexpr int kRedBlocks = 296;   // 2 x 148 SMs
+constexpr int kRedThreads = 256;
+
+// part[b] = sum over the block's grid-stride share of x.*y
+__global__ void dot_partial_kernel(long long n, const double *__restrict__ x, const double *__restrict__ y,
+                                   double *part) {
+  __shared__ double red[kRedThreads];
+  double s = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    s += x[i] * y[i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+    if ((int)threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// out[0] = sum(part) (or sqrt of it), fixed order
+__global__ void dot_final_kernel(int k, const double *__restrict__ part, double *out, int takeSqrt) {
+  __shared__ double red[kRedThreads];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < k; i += blockDim.x) s += part[i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int m = blockDim.x / 2; m > 0; m >>= 1) {
+    if ((int)threadIdx.x < m) red[threadIdx.x] += red[threadIdx.x + m];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = takeSqrt ? sqrt(red[0]) : red[0];
+}
+
+// y -= (*h) * x
+__global__ void axpy_neg_dev_kernel(long long n, const double *__restrict__ h, const double *__restrict__ x, double *y) {
+  const double a = -(*h);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    y[i] += a * x[i];
+}
+
+// v = w / (*h) when *h > 0, else v = w
+__global__ void scale_copy_dev_kernel(long long n, const double *__restrict__ h, const double *__restrict__ w, double *v) {
+  const double d = *h;
+  const double s = (d > 0.0) ? 1.0 / d : 1.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    v[i] = (d > 0.0) ? w[i] * s : w[i];
+}
+
+__global__ void scale_copy_kernel(long long n, double s, const double *__restrict__ w, double *v) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    v[i] = w[i] * s;
+}
+
+// x += V y  (k columns of length n, column stride ldv)
+__global__ void update_kernel(long long n, int k, const double *__restrict__ V, long long ldv,
+                              const double *__restrict__ y, double *x) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    double s = x[i];
+    for (int j = 0; j < k; j++) s += y[j] * V[(size_t)j * ldv + i];
+    x[i] = s;
+  }
+}
+
+static bool dot_dev(Context &c, long long n, const double *x, const double *y, double *out, bool sq) {
+  PrecondDev &p = *c.pc;
+  dot_partial_kernel<<<kRedBlocks, kRedThreads, 0, c.stream>>>(n, x, y, p.d_part);
+  dot_final_kernel<<<1, kRedThreads, 0, c.stream>>>(kRedBlocks, p.d_part, out, sq ? 1 : 0);
+  c.launches += 2;
+  FB_CUDA(cudaGetLastError());
+  return true;
+}
+
+static bool nrm2_host(Context &c, long long n, const double *x, double *out) {
+  if (!dot_dev(c, n, x, x, c.pc->d_part + kRedBlocks, true)) return false;
+  FB_CUDA(cudaMemcpyAsync(out, c.pc->d_part + kRedBlocks, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  FB_CUDA(cudaStreamSynchronize(c.stream));
+  return true;
+}
+
+// drotg of the reference BLAS: r takes the sign of the larger input
+static void drotg_h(double *a, double *b, double *cc, double *ss) {
+  double aa = *a, bb = *b, roe = (fabs(aa) > fabs(bb)) ? aa : bb, scale = fabs(aa) + fabs(bb), r, z;
+  if (scale == 0.0) {
+    *cc = 1.0; *ss = 0.0; r = 0.0; z = 0.0;
+  } else {
+    r = scale * sqrt((aa / scale) * (aa / scale) + (bb / scale) * (bb / scale));
+    if (roe < 0.0) r = -r;
+    *cc = aa / r;
+    *ss = bb / r;
+    z = 1.0;
+    if (fabs(aa) > fabs(bb)) z = *ss;
+    if (fabs(bb) >= fabs(aa) && *cc != 0.0) z = 1.0 / (*cc);
+  }
+  *a = r;
+  *b = z;
+}
+
+static void rot_h(double *x, double *y, double cc, double ss) {
+  double xv = *x, yv = *y;
+  *x = cc * xv + ss * yv;
+  *y = cc * yv - ss * xv;
+}
+
+static bool gmres_update_dev(Context &c, int it, std::vector<double> &H, int ldh, const std::vector<double> &sv,
+                             double *x) {
+  PrecondDev &p = *c.pc;
+  std::vector<double> y(sv.begin(), sv.begin() + it);
+  for (int j = it - 1; j >= 0; j--) {  // dtrsv upper, no transpose
+    if (y[j] != 0.0) {
+      y[j] /= H[(size_t)j * ldh + j];
+      for (int i = j - 1; i >= 0; i--) y[i] -= y[j] * H[(size_t)j * ldh + i];
+    }
+  }
+  const long long n2 = 2LL * c.n;
+  FB_CUDA(cudaMemcpyAsync(p.d_y, y.data(), it * sizeof(double), cudaMemcpyHostToDevice, c.stream));
+  update_kernel<<<kRedBlocks * 4, 256, 0, c.stream>>>(n2, it, p.d_V, n2, p.d_y, x);
+  c.launches += 1;
+  FB_CUDA(cudaGetLastError());
+  FB_CUDA(cudaStreamSynchronize(c.stream));  // y (host) must outlive the copy
+  return true;
+}
+
+bool gmres_solve(Context &c, const double *b, double *x, int restrt, int maxit, double tol, int *iters, double *resid,
+                 int *info) {
+  FB_CHECK(c.pc != nullptr, "call fabipb_b200_precond_setup before solving (mode -1 for none)");
+  PrecondDev &p = *c.pc;
+  const long long n2 = 2LL * c.n;
+  const int ldh = restrt + 1;
+  cudaStream_t s = c.stream;
+  if (p.restart != restrt || p.d_V == nullptr) {
+    p.restart = restrt;
+    if (!p.arena.alloc_n(&p.d_V, (size_t)n2 * (restrt + 1)) || !p.arena.alloc_n(&p.d_r, (size_t)n2) ||
+        !p.arena.alloc_n(&p.d_av, (size_t)n2) || !p.arena.alloc_n(&p.d_w, (size_t)n2) ||
+        !p.arena.alloc_n(&p.d_h, (size_t)ldh + 1) || !p.arena.alloc_n(&p.d_part, (size_t)kRedBlocks + 2) ||
+        !p.arena.alloc_n(&p.d_y, (size_t)restrt + 1))
+      return false;
+  }
+  std::vector<double> H((size_t)ldh * (restrt + 2), 0.0), sv(restrt + 2, 0.0), hcol(ldh, 0.0);
+  double *cs = &H[(size_t)restrt * ldh], *sn = &H[(size_t)(restrt + 1) * ldh];
+  double bnrm2, rnorm, xn;
+  *info = 0;
+  *iters = maxit;
+  *resid = tol;
+  // av = b (- A x when x != 0); r = P^-1 av
+  FB_CUDA(cudaMemcpyAsync(p.d_av, b, n2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  if (!nrm2_host(c, n2, x, &xn)) return false;
+  if (xn != 0.0) {
+    if (!op_matvec(c, -1.0, x, 1.0, p.d_av)) return false;
+  }
+  if (!precond_apply(c, p.d_av, p.d_r)) return false;
+  if (!nrm2_host(c, n2, b, &bnrm2)) return false;
+  if (bnrm2 == 0.0) bnrm2 = 1.0;
+  if (!nrm2_host(c, n2, p.d_r, &rnorm)) return false;
+  if (rnorm / bnrm2 < tol) return true;
+  *iters = 0;
+  for (;;) {
+    int i = 0;
+    if (!nrm2_host(c, n2, p.d_r, &rnorm)) return false;
+    if (!(rnorm > 0.0) || rnorm != rnorm) {
+      *resid = (rnorm != rnorm) ? rnorm : 0.0;
+      *info = (rnorm != rnorm) ? 2 : 0;
+      return true;
+    }
+    scale_copy_kernel<<<kRedBlocks * 4, 256, 0, s>>>(n2, 1.0 / rnorm, p.d_r, p.d_V);
+    c.launches += 1;
+    sv.assign(restrt + 2, 0.0);
+    sv[0] = rnorm;
+    for (;;) {
+      ++i;
+      ++(*iters);
+      if (!op_matvec(c, 1.0, p.d_V + (size_t)(i - 1) * n2, 0.0, p.d_av)) return false;
+      if (!precond_apply(c, p.d_av, p.d_w)) return false;
+      // modified Gram-Schmidt: h[k] = w.v_k; w -= h[k] v_k
+      for (int k = 0; k < i; k++) {
+        if (!dot_dev(c, n2, p.d_w, p.d_V + (size_t)k * n2, p.d_h + k, false)) return false;
+        axpy_neg_dev_kernel<<<kRedBlocks * 4, 256, 0, s>>>(n2, p.d_h + k, p.d_V + (size_t)k * n2, p.d_w);
+        c.launches += 1;
+      }
+      if (!dot_dev(c, n2, p.d_w, p.d_w, p.d_h + i, true)) return false;
+      scale_copy_dev_kernel<<<kRedBlocks * 4, 256, 0, s>>>(n2, p.d_h + i, p.d_w, p.d_V + (size_t)i * n2);
+      c.launches += 1;
+      FB_CUDA(cudaMemcpyAsync(hcol.data(), p.d_h, (i + 1) * sizeof(double), cudaMemcpyDeviceToHost, s));
+      FB_CUDA(cudaStreamSynchronize(s));
+      double *hc = &H[(size_t)(i - 1) * ldh];
+      for (int k = 0; k <= i; k++) hc[k] = hcol[k];
+      for (int k = 0; k < i - 1; k++) rot_h(&hc[k], &hc[k + 1], cs[k], sn[k]);
+      double aa = hc[i - 1], bb = hc[i];
+      drotg_h(&aa, &bb, &cs[i - 1], &sn[i - 1]);
+      rot_h(&hc[i - 1], &hc[i], cs[i - 1], sn[i - 1]);
+      rot_h(&sv[i - 1], &sv[i], cs[i - 1], sn[i - 1]);
+      *resid = fabs(sv[i]) / bnrm2;
+      if (*resid <= tol) return gmres_update_dev(c, i, H, ldh, sv, x);
+      if (*iters == maxit || i >= restrt) break;
+    }
+    if (!gmres_update_dev(c, i, H, ldh, sv, x)) return false;
+    FB_CUDA(cudaMemcpyAsync(p.d_av, b, n2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    if (!op_matvec(c, -1.0, x, 1.0, p.d_av)) return false;
+    if (!precond_apply(c, p.d_av, p.d_r)) return false;
+    if (!nrm2_host(c, n2, p.d_r, &sv[i])) return false;
+    *resid = sv[i] / bnrm2;
+    if (*resid <= tol) return true;
+    if (*iters == maxit) {
+      *info = 1;
+      return true;
+    }
+  }
+}
+
+}  // namespace fb

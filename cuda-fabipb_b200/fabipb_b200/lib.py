@@ -52,6 +52,8 @@ def load():
     L.fabipb_b200_set_charges.argtypes = [vp, C.c_int, vp, vp]
     L.fabipb_b200_destroy.argtypes = [vp]
     L.fabipb_b200_set_stream.argtypes = [vp, vp]
+    L.fabipb_b200_launch_count.argtypes = [vp]
+    L.fabipb_b200_launch_count.restype = C.c_longlong
     L.fabipb_b200_last_error.restype = C.c_char_p
     L.fabipb_b200_info_get.argtypes = [vp, C.POINTER(Info)]
     L.fabipb_b200_panel_order.argtypes = [vp, vp]
@@ -134,6 +136,12 @@ class Surface:
         pos = np.ascontiguousarray(charges.pos.reshape(-1), dtype=np.float64)
         q = np.ascontiguousarray(charges.q, dtype=np.float64)
         _check(load().fabipb_b200_set_charges(self.h, int(q.shape[0]), _ptr(pos), _ptr(q)), "set_charges")
+
+    def launch_count(self):
+        return int(load().fabipb_b200_launch_count(self.h))
+
+    def set_stream(self, stream_handle):
+        _check(load().fabipb_b200_set_stream(self.h, stream_handle), "set_stream")
 
     def info(self):
         i = Info()

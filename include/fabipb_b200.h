@@ -70,6 +70,8 @@ int fabipb_b200_create(const fabipb_b200_params *p, int n_panels, const double *
 int fabipb_b200_set_charges(void *ctx, int n_charges, const double *pos, const double *q);
 void fabipb_b200_destroy(void *ctx);
 int fabipb_b200_set_stream(void *ctx, void *cuda_stream);
+/* number of CUDA kernels this context has launched so far */
+long long fabipb_b200_launch_count(void *ctx);
 const char *fabipb_b200_last_error(void);
 
 /* tree queries, for parity checks against the reference layouts */

@@ -231,7 +231,7 @@ def ref_env(threads=None):
 
 
 def run_ref_harness(mode, base, out_prefix, opts, sigma=None, threads=None, reps=None, warmup=None,
-                    extra_env=None):
+                    extra_env=None, budget=None):
     """Run oracle/_ref/ref_harness; return stdout.  Mesh files must sit at ``base``."""
     cmd = [REF_HARNESS, mode, base, out_prefix] + list(opts)
     if sigma is not None:
@@ -242,6 +242,8 @@ def run_ref_harness(mode, base, out_prefix, opts, sigma=None, threads=None, reps
         cmd.append("--reps=%d" % reps)
     if warmup is not None:
         cmd.append("--warmup=%d" % warmup)
+    if budget is not None:
+        cmd.append("--budget=%g" % budget)
     env = ref_env(threads)
     if extra_env:
         env.update(extra_env)

@@ -82,6 +82,7 @@ int main(int argc, char **argv) {
   const char *mode, *out, *sigmaPath = NULL, *v;
   char base[512];
   int order = -1, reps = 3, warmup = 1, nPnls = 0, i;
+  double budget = 0.0;
   int sepExplicit = 0, precondExplicit = 0;
   panel *inputLst;
 
@@ -115,6 +116,7 @@ int main(int argc, char **argv) {
     else if (strncmp(a, "--sigma=", 8) == 0) sigmaPath = a + 8;
     else if (strncmp(a, "--reps=", 7) == 0) reps = atoi(a + 7);
     else if (strncmp(a, "--warmup=", 9) == 0) warmup = atoi(a + 9);
+    else if (strncmp(a, "--budget=", 9) == 0) budget = atof(a + 9);
     else { fprintf(stderr, "unknown option %s\n", a); return 2; }
   }
   epsilon = epsilon2 / epsilon1;
@@ -206,7 +208,16 @@ int main(int argc, char **argv) {
       s = s * 6364136223846793005ULL + 1442695040888963407ULL;
       sgm[i] = (double)(s >> 11) / 9007199254740992.0 - 0.5;
     }
-    for (r = 0; r < warmup; r++) MtVmain(&alpha, sgm, &beta, pot);
+    for (r = 0; r < warmup; r++) {
+      double w0 = now();
+      MtVmain(&alpha, sgm, &beta, pot);
+      /* with a time budget, cap the timed repetitions by the warm-up cost */
+      if (budget > 0.0) {
+        int cap = (int)(budget / (now() - w0));
+        if (cap < 1) cap = 1;
+        if (reps > cap) reps = cap;
+      }
+    }
     t0 = now();
     for (r = 0; r < reps; r++) MtVmain(&alpha, sgm, &beta, pot);
     t1 = now();

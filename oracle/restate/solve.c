@@ -184,13 +184,19 @@ int or_gmres(or_sys *s, const double *b, double *x, int restrt, int *iter, doubl
   or_precond_apply(s, w, r);
   bnrm2 = dnrm2_(&n, b, &one);
   if (bnrm2 == 0.0) bnrm2 = 1.0;
-  if (dnrm2_(&n, r, &one) / bnrm2 < tol) { *iter = 0; *resid = dnrm2_(&n, r, &one) / bnrm2; goto done; }
+  /* converged at the initial guess: like gmres.c:232, *iter and *resid keep
+     their input values */
+  if (dnrm2_(&n, r, &one) / bnrm2 < tol) goto done;
   *iter = 0;
   for (;;) {
     i = 0;
     memcpy(v, r, (size_t)n * sizeof(double));
     rnorm = dnrm2_(&n, v, &one);
-    if (!(rnorm > 0.0) || rnorm != rnorm) { *resid = (rnorm != rnorm) ? rnorm : 0.0; info = 2; goto done; }
+    if (!(rnorm > 0.0) || rnorm != rnorm) {
+      *resid = (rnorm != rnorm) ? rnorm : 0.0;
+      info = (rnorm != rnorm) ? 2 : 0;
+      goto done;
+    }
     aa = 1.0 / rnorm;
     for (k = 0; k < n; k++) v[k] *= aa;
     sv[0] = rnorm;

@@ -94,3 +94,72 @@ def test_apply_alpha_beta_semantics(case_dir, golden_meta, oracles):
     got = s.apply(sg, part=lib.ALL, alpha=0.3, beta=-2.0, pot=y0)
     ref = oracles[name].fmm_apply(sg, 0.3, -2.0, y0)
     assert rel_l2(got, ref) < 1e-12
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_rhs_direct(name, case_dir, golden_meta):
+    g = load_golden(name)
+    s, _, ch = surface(case_dir, golden_meta, name, lib.MIXED)
+    s.set_charges(ch)
+    assert rel_l2(s.rhs(use_tree=False), g["rhs"]) < 1e-13
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_rhs_tree(name, case_dir, golden_meta):
+    g = load_golden(name)
+    s, _, ch = surface(case_dir, golden_meta, name, lib.MIXED)
+    s.set_charges(ch)
+    assert rel_l2(s.rhs(use_tree=True), g["rhs_tree"]) < 1e-12
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_energy(name, case_dir, golden_meta):
+    g = load_golden(name)
+    s, _, ch = surface(case_dir, golden_meta, name, lib.MIXED)
+    s.set_charges(ch)
+    e = s.energy_raw(make_golden.seeded_sigma(s.n))
+    ref = float(g["energy_raw"][0])
+    assert abs(e - ref) <= 1e-12 * abs(ref)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_solve_fp64_matches_reference(name, case_dir, golden_meta):
+    """Device GMRES + block-LU preconditioner with the FP64 operator: same
+    iteration count as the reference CLI, energy equal to its %f print."""
+    meta = golden_meta[name]
+    s, _, ch = surface(case_dir, golden_meta, name, lib.FP64)
+    s.set_charges(ch)
+    b = s.rhs(use_tree=False)
+    s.precond_setup(2)
+    x, it, res, info = s.solve(b, b.copy(), restart=meta["opts"]["a"], maxit=100, tol=meta["opts"]["o"])
+    e = s.energy_raw(x) * 2 * np.pi * 332.0716
+    assert info == 0
+    assert it == meta["solve"]["iterations"]
+    assert abs(res - meta["solve"]["residual"]) <= 1e-3 * meta["solve"]["residual"]
+    assert abs(e - meta["solve"]["energy"]) <= 2e-6 + 1e-8 * abs(e)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_solve_mixed_energy(name, case_dir, golden_meta):
+    """FP32 near-field operator inside GMRES: energy within 1e-4 relative of
+    the reference, iteration count within one."""
+    meta = golden_meta[name]
+    s, _, ch = surface(case_dir, golden_meta, name, lib.MIXED)
+    s.set_charges(ch)
+    b = s.rhs(use_tree=False)
+    s.precond_setup(2)
+    x, it, res, info = s.solve(b, b.copy(), restart=meta["opts"]["a"], maxit=100, tol=meta["opts"]["o"])
+    e = s.energy_raw(x) * 2 * np.pi * 332.0716
+    assert info == 0
+    assert abs(it - meta["solve"]["iterations"]) <= 1
+    assert abs(e - meta["solve"]["energy"]) <= 1e-4 * abs(meta["solve"]["energy"])
+
+
+def test_precond_apply_matches_oracle(case_dir, golden_meta, oracles):
+    name = "star2048"
+    s, _, _ = surface(case_dir, golden_meta, name, lib.FP64)
+    s.precond_setup(2)
+    orc = oracles[name]
+    orc.precond_setup(2)
+    b = make_golden.seeded_sigma(s.n, 9)
+    assert rel_l2(s.precond_apply(b), orc.precond_apply(b)) < 1e-11
