@@ -148,6 +148,50 @@ bool scale_vec(Context &c, double *v, double a, long long n) {
   return true;
 }
 
+int create_context(const fabipb_b200_params *p, int n, const double *vtx, const double *normal,
+                   const double *area, bool dense, void **out) {
+  if (out) *out = nullptr;
+  if (p == nullptr || vtx == nullptr || normal == nullptr || area == nullptr || out == nullptr || n <= 0) {
+    set_error("fabipb_b200_create: invalid arguments");
+    return 0;
+  }
+  auto t0 = std::chrono::steady_clock::now();
+  Context *c = new Context();
+  c->prm = *p;
+  c->n = n;
+  c->epsilon = p->eps2 / p->eps1;
+  c->mixed = (p->precision == FABIPB_B200_MIXED);
+  c->device = p->device;
+  c->dense = dense;
+  bool ok = true;
+  if (cudaSetDevice(p->device) != cudaSuccess) {
+    set_error("cudaSetDevice(%d) failed", p->device);
+    ok = false;
+  }
+  if (ok && cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    set_error("cudaStreamCreate failed");
+    ok = false;
+  }
+  c->ownStream = ok;
+  ok = ok && init_quad_tables();
+  ok = ok && setup_geometry(*c, vtx, normal, area);
+  ok = ok && setup_near(*c);
+  ok = ok && setup_fmm(*c);
+  if (ok && cudaStreamSynchronize(c->stream) != cudaSuccess) {
+    set_error("setup kernels failed: %s", cudaGetErrorString(cudaGetLastError()));
+    ok = false;
+  }
+  if (!ok) {
+    std::string keep = get_error();
+    delete c;
+    set_error("%s", keep.c_str());
+    return 0;
+  }
+  c->setupSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  *out = c;
+  return 1;
+}
+
 }  // namespace fb
 
 using namespace fb;
@@ -216,45 +260,7 @@ const char *fabipb_b200_last_error(void) { return get_error(); }
 
 int fabipb_b200_create(const fabipb_b200_params *p, int n, const double *vtx, const double *normal,
                        const double *area, void **out) {
-  if (out) *out = nullptr;
-  if (p == nullptr || vtx == nullptr || normal == nullptr || area == nullptr || out == nullptr || n <= 0) {
-    set_error("fabipb_b200_create: invalid arguments");
-    return 0;
-  }
-  auto t0 = std::chrono::steady_clock::now();
-  Context *c = new Context();
-  c->prm = *p;
-  c->n = n;
-  c->epsilon = p->eps2 / p->eps1;
-  c->mixed = (p->precision == FABIPB_B200_MIXED);
-  c->device = p->device;
-  bool ok = true;
-  if (cudaSetDevice(p->device) != cudaSuccess) {
-    set_error("cudaSetDevice(%d) failed", p->device);
-    ok = false;
-  }
-  if (ok && cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
-    set_error("cudaStreamCreate failed");
-    ok = false;
-  }
-  c->ownStream = ok;
-  ok = ok && init_quad_tables();
-  ok = ok && setup_geometry(*c, vtx, normal, area);
-  ok = ok && setup_near(*c);
-  ok = ok && setup_fmm(*c);
-  if (ok && cudaStreamSynchronize(c->stream) != cudaSuccess) {
-    set_error("setup kernels failed: %s", cudaGetErrorString(cudaGetLastError()));
-    ok = false;
-  }
-  if (!ok) {
-    std::string keep = get_error();
-    delete c;
-    set_error("%s", keep.c_str());
-    return 0;
-  }
-  c->setupSeconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-  *out = c;
-  return 1;
+  return create_context(p, n, vtx, normal, area, false, out);
 }
 
 void fabipb_b200_destroy(void *ctx) {

@@ -61,6 +61,7 @@ bool setup_charges(Context &c, int m, const double *pos, const double *q) {
 
 // charge-tree Taylor order of a level (chargeTree.c:117-129)
 static int charge_order(const Context &c, int level) {
+  if (!c.chargeOrders.empty()) return std::min(c.chargeOrders[level], c.P);
   int order;
   if (c.prm.charge_order > 0) order = c.prm.charge_order;
   else order = std::max(c.pt.ordMom[level], 4);
@@ -263,6 +264,9 @@ __device__ void walk_point(int mode, const double *qp, const double *nx, double 
         if (mode == 0) {
           y0 += sm * d0[i];
           y1 += sm * (nx[0] * d0[e1] + nx[1] * d0[e2] + nx[2] * d0[e3]);
+        } else if (mode == 2) {
+          y0 += sm * dk[i];
+          y1 += sm * eps * (nx[0] * dk[e1] + nx[1] * dk[e2] + nx[2] * dk[e3]);
         } else {
           y0 += sm * (d0[i] - dk[i]);
           const double dn0 = nx[0] * d0[e1] + nx[1] * d0[e2] + nx[2] * d0[e3];
@@ -293,8 +297,13 @@ __device__ void walk_point(int mode, const double *qp, const double *nx, double 
           const double rn = sqrt(r2), G0 = kFourPiI / rn, ek = exp(-kappa * rn);
           const double Gk = ek * G0, coef = (kappa * rn + 1.0) * ek;
           const double dG0dn = -ip * G0 / r2, dGkdn = coef * dG0dn;
-          y[0] += chr[j] * (G0 - Gk);
-          y[1] += chr[j] * (eps * dGkdn - dG0dn);
+          if (mode == 2) {
+            y[0] += chr[j] * Gk;
+            y[1] += chr[j] * eps * dGkdn;
+          } else {
+            y[0] += chr[j] * (G0 - Gk);
+            y[1] += chr[j] * (eps * dGkdn - dG0dn);
+          }
         }
       }
       continue;
@@ -341,11 +350,13 @@ __global__ void tree_walk_kernel(int mode, int n, int q, const double *__restric
     if (mode == 0) {
       rhs[X] = fac * o0;
       rhs[n + X] = fac * o1;
+    } else if (mode == 2) {
+      e = -o0 * sgm[X + n] + o1 * sgm[X];   // rhsReuseEnergyWorker, treecode.c:889-910
     } else {
       e = o0 * sgm[X + n] + o1 * sgm[X];
     }
   }
-  if (mode == 1) {
+  if (mode != 0) {
     red[threadIdx.x] = e;
     __syncthreads();
     for (int s = blockDim.x / 2; s > 0; s >>= 1) {
@@ -367,11 +378,12 @@ __global__ void sum_partials_kernel(int k, const double *__restrict__ p, double 
 template <int PM>
 static void launch_walk(Context &c, int mode, const double *sgm, double *rhs, double *partial) {
   ChargeTreeDev &d = *c.ct;
-  const double theta = (mode == 0) ? c.prm.rhs_theta : c.prm.energy_theta;
+  // the screened-only walk uses the RHS acceptance ratio (treecode.c:731)
+  const double theta = (mode == 1) ? c.prm.energy_theta : c.prm.rhs_theta;
   tree_walk_kernel<PM><<<ceil_div(c.n, 256), 256, 0, c.stream>>>(
       mode, c.n, c.prm.quad_order, c.d_vtx, c.d_nrm, c.d_area, theta, d.height, d.depth, c.prm.kappa, c.epsilon,
       c.NM, d.d_ctr, d.d_rad, d.d_level, d.d_kidStart, d.d_kidCount, d.d_itemStart, d.d_itemCount, d.d_order,
-      d.d_mom, d.d_pos, d.d_chr, kFourPiI / c.prm.eps1, sgm, rhs, partial);
+      d.d_mom, d.d_pos, d.d_chr, c.rhsFac != 0.0 ? c.rhsFac : kFourPiI / c.prm.eps1, sgm, rhs, partial);
 }
 
 #define FB_DISPATCH_WALK(P, ...)                      \
@@ -393,7 +405,7 @@ bool launch_rhs(Context &c, int useTree, double *rhs) {
   if (!useTree) {
     rhs_direct_kernel<<<ceil_div(c.n, 128), 128, 0, c.stream>>>(c.n, c.nChar, c.prm.quad_order, c.d_vtx, c.d_nrm,
                                                                 c.d_area, c.ct->d_posOrig, c.ct->d_chrOrig,
-                                                                kFourPiI / c.prm.eps1, rhs);
+                                                                c.rhsFac != 0.0 ? c.rhsFac : kFourPiI / c.prm.eps1, rhs);
     FB_CUDA(cudaGetLastError());
     return true;
   }
@@ -404,7 +416,7 @@ bool launch_rhs(Context &c, int useTree, double *rhs) {
   return true;
 }
 
-bool launch_energy(Context &c, const double *sgm, double *raw_host) {
+bool launch_energy_mode(Context &c, const double *sgm, int mode, double *raw_host) {
   FB_CHECK(c.ct != nullptr && c.nChar > 0, "no charges set (fabipb_b200_set_charges)");
   if (!build_charge_tree(c)) return false;
   ChargeTreeDev &d = *c.ct;
@@ -413,12 +425,113 @@ bool launch_energy(Context &c, const double *sgm, double *raw_host) {
     if (!d.arena.alloc_n(&d.d_partial, (size_t)blocks + 1)) return false;
     d.partialCap = blocks + 1;
   }
-  FB_DISPATCH_WALK(c.P, c, 1, sgm, nullptr, d.d_partial);
+  FB_DISPATCH_WALK(c.P, c, mode, sgm, nullptr, d.d_partial);
   c.launches += 2;
   sum_partials_kernel<<<1, 32, 0, c.stream>>>(blocks, d.d_partial, d.d_partial + blocks);
   FB_CUDA(cudaGetLastError());
   FB_CUDA(cudaMemcpyAsync(raw_host, d.d_partial + blocks, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
   FB_CUDA(cudaStreamSynchronize(c.stream));
+  return true;
+}
+
+}  // namespace fb
+
+namespace fb {
+
+bool launch_energy(Context &c, const double *sgm, double *raw_host) { return launch_energy_mode(c, sgm, 1, raw_host); }
+
+__global__ void coulomb_dot_kernel(int n, double eps1, const double *__restrict__ rhs, const double *__restrict__ sgm,
+                                   double *part) {
+  __shared__ double red[256];
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    s += eps1 * (rhs[i] * sgm[i + n] - rhs[i + n] * sgm[i]);
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int k = blockDim.x / 2; k > 0; k >>= 1) {
+    if ((int)threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// eps1 * sum_i (rhs0_i sgm1_i - rhs1_i sgm0_i)  (rhsReuseCoulombDotWorker, treecode.c:912-925)
+bool abi_coulomb_dot(Context &c, const double *rhs, const double *sgm, double eps1, double *dot) {
+  const int blocks = 296;
+  double *part = nullptr;
+  FB_CUDA(cudaMallocAsync((void **)&part, (blocks + 1) * sizeof(double), c.stream));
+  coulomb_dot_kernel<<<blocks, 256, 0, c.stream>>>(c.n, eps1, rhs, sgm, part);
+  sum_partials_kernel<<<1, 32, 0, c.stream>>>(blocks, part, part + blocks);
+  c.launches += 2;
+  cudaError_t e = cudaMemcpyAsync(dot, part + blocks, sizeof(double), cudaMemcpyDeviceToHost, c.stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+  cudaFreeAsync(part, c.stream);
+  FB_CHECK(e == cudaSuccess, "Coulomb dot failed: %s", cudaGetErrorString(e));
+  return true;
+}
+
+// one-point disjoint coefficients K = Ax*Ay*KER4(mX - mY) for listed pairs;
+// pairs that share a vertex are skipped (done = 0)
+__global__ void disjoint_pairs_kernel(long long nPairs, const double *__restrict__ vtx, const double *__restrict__ nrm,
+                                      const double *__restrict__ area, const int *__restrict__ dst,
+                                      const int *__restrict__ src, double kappa, double eps, double *k) {
+  long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nPairs) return;
+  const int Xi = dst[t], Yi = src[t];
+  PanelD X, Y;
+  const double *vx = vtx + 9 * (size_t)Xi, *vy = vtx + 9 * (size_t)Yi;
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++) { X.v[a][b] = vx[3 * a + b]; Y.v[a][b] = vy[3 * a + b]; }
+  int ix[3], iy[3];
+  double *out = k + 5 * (size_t)t;
+  if (common_vtx(X, Y, Xi == Yi, ix, iy) != 0) { out[4] = 0.0; return; }
+  double r[3], y[4];
+  for (int c = 0; c < 3; c++) {
+    double mx = X.v[0][c] + 0.5 * ((X.v[1][c] - X.v[0][c]) + 0.5 * (X.v[2][c] - X.v[1][c]));
+    double my = Y.v[0][c] + 0.5 * ((Y.v[1][c] - Y.v[0][c]) + 0.5 * (Y.v[2][c] - Y.v[1][c]));
+    r[c] = mx - my;
+  }
+  ker4_d(kappa, eps, r, nrm + 3 * (size_t)Xi, nrm + 3 * (size_t)Yi, y);
+  const double AA = area[Xi] * area[Yi];
+  for (int i = 0; i < 4; i++) out[i] = AA * y[i];
+  out[4] = 1.0;
+}
+
+bool abi_disjoint_pairs(const double *vtx, const double *nrm, const double *area, long long nPairs, const int *dst,
+                        const int *src, double kappa, double eps, double *k0, double *k1, double *k2, double *k3,
+                        int *done, cudaStream_t s) {
+  int maxIdx = 0;
+  for (long long t = 0; t < nPairs; t++) maxIdx = std::max(maxIdx, std::max(dst[t], src[t]));
+  const size_t np = (size_t)maxIdx + 1;
+  DevArena a;
+  double *d_vtx, *d_nrm, *d_area, *d_k;
+  int *d_dst, *d_src;
+  bool ok = a.alloc_n(&d_vtx, 9 * np) && a.alloc_n(&d_nrm, 3 * np) && a.alloc_n(&d_area, np) &&
+            a.alloc_n(&d_dst, (size_t)nPairs) && a.alloc_n(&d_src, (size_t)nPairs) && a.alloc_n(&d_k, 5 * (size_t)nPairs);
+  std::vector<double> hk;
+  if (ok) ok = cudaMemcpyAsync(d_vtx, vtx, 9 * np * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+               cudaMemcpyAsync(d_nrm, nrm, 3 * np * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+               cudaMemcpyAsync(d_area, area, np * sizeof(double), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+               cudaMemcpyAsync(d_dst, dst, nPairs * sizeof(int), cudaMemcpyHostToDevice, s) == cudaSuccess &&
+               cudaMemcpyAsync(d_src, src, nPairs * sizeof(int), cudaMemcpyHostToDevice, s) == cudaSuccess;
+  if (ok) {
+    disjoint_pairs_kernel<<<ceil_div(nPairs, 256), 256, 0, s>>>(nPairs, d_vtx, d_nrm, d_area, d_dst, d_src, kappa,
+                                                                eps, d_k);
+    hk.resize(5 * (size_t)nPairs);
+    ok = cudaGetLastError() == cudaSuccess &&
+         cudaMemcpyAsync(hk.data(), d_k, hk.size() * sizeof(double), cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+         cudaStreamSynchronize(s) == cudaSuccess;
+  }
+  a.release();
+  FB_CHECK(ok, "disjoint pair coefficients failed: %s", cudaGetErrorString(cudaGetLastError()));
+  for (long long t = 0; t < nPairs; t++) {
+    if (hk[5 * t + 4] == 0.0) {
+      if (done) done[t] = 0;
+      continue;
+    }
+    k0[t] = hk[5 * t]; k1[t] = hk[5 * t + 1]; k2[t] = hk[5 * t + 2]; k3[t] = hk[5 * t + 3];
+    if (done) done[t] = 1;
+  }
   return true;
 }
 

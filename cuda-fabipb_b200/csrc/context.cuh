@@ -60,11 +60,15 @@ struct Context {
   int *d_mOff = nullptr, *d_mLst = nullptr;    // (alpha-k, k) per alpha
   int *d_kidFirst = nullptr, *d_kidCount = nullptr;  // FMM indices of the children
   int *d_ordM2L = nullptr;                     // per FMM cube
+  int nConvList = 0;                           // entries of d_lst
 
   // ---- scratch vectors for host-pointer calls ------------------------
   double *d_x = nullptr, *d_y = nullptr, *d_w = nullptr;
 
   // ---- charges, RHS, energy -------------------------------------------
+  std::vector<int> chargeOrders;           // per-level charge-tree order (host policy)
+  double rhsFac = 0.0;                     // RHS scale override (0: 1/(4 pi eps1))
+  bool dense = false;                      // near field over every leaf pair (direct mode)
   int nChar = 0;
   std::vector<double> h_pos, h_chr;
   ChargeTreeDev *ct = nullptr;
@@ -101,6 +105,10 @@ bool gmres_solve(Context &c, const double *b, double *x, int restart, int maxit,
                  int *iters, double *resid, int *info);
 void free_charges(Context &c);
 void free_precond(Context &c);
+
+// create a context (dense = every leaf pair is near: the direct operator)
+int create_context(const fabipb_b200_params *p, int n, const double *vtx, const double *nrm, const double *area,
+                   bool dense, void **out);
 
 // composite operators (device vectors)
 bool op_apply(Context &c, int part, double alpha, const double *sgm, double beta, double *pot);

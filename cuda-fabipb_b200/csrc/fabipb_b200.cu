@@ -6,3 +6,4 @@
 #include "charges.cu"
 #include "solver.cu"
 #include "api.cu"
+#include "abi.cu"

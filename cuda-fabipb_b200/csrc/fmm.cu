@@ -93,20 +93,24 @@ __device__ __forceinline__ double conv_entry(const double *t, int g) {
   return f1 * f2 * f3 * c_ifact3[g];
 }
 
-// D^alpha G0 and D^alpha Gk at x for |alpha| <= order (setupDerivs).  The
-// reference fills one table per derivative level p from level p+1; keeping
-// only two levels gives the same entries with O(nMom) scratch.
+// D^alpha G0 and D^alpha Gk at x for |alpha| <= order (setupDerivs,
+// src/expan.c:138-209).  The reference fills one table per derivative level
+// p from level p+1; an entry of total degree d at level p reads only degrees
+// d-1 and d-2 of level p+1, so sweeping each level from the highest degree
+// down lets one table per kernel be updated in place.  Entry e of the result
+// lives at d0[e*stride] (stride 1 for a private array, the block width for a
+// shared-memory column).
 template <int PM>
-__device__ void derivs(int order, const double *x, double kappa, bool coulombOnly, double *d0, double *dk) {
-  constexpr int NM = nmom_c(PM);
+__device__ void derivs_inplace(int order, const double *x, double kappa, bool coulombOnly, double *d0, double *dk,
+                               int stride) {
   double G0[PM + 2], Gk[PM + 2];
-  double r = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+  const double r = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
   if (coulombOnly) {
-    double r2 = -1.0 / (r * r);
+    const double r2 = -1.0 / (r * r);
     G0[0] = kFourPiI / r;
     for (int k = 0; k < order; k++) G0[k + 1] = (2 * k + 1) * r2 * G0[k];
   } else {
-    double rexp = exp(-kappa * r), r1 = 1.0 / r, rr2 = r1 * r1, nr2 = -rr2, k2 = kappa * kappa;
+    const double rexp = exp(-kappa * r), r1 = 1.0 / r, rr2 = r1 * r1, nr2 = -rr2, k2 = kappa * kappa;
     G0[0] = r1 * kFourPiI;
     Gk[0] = rexp * G0[0];
     G0[1] = nr2 * G0[0];
@@ -116,61 +120,43 @@ __device__ void derivs(int order, const double *x, double kappa, bool coulombOnl
       Gk[k + 1] = rr2 * (k2 * Gk[k - 1] - (2 * k + 1) * Gk[k]);
     }
   }
-  double pa0[NM], pak[NM];  // level p+1
-  // level `order`: only the radial value
-  pa0[0] = G0[order];
-  if (!coulombOnly) pak[0] = Gk[order];
+  d0[0] = G0[order];
+  if (!coulombOnly) dk[0] = Gk[order];
   for (int p = order - 1; p >= 0; p--) {
-    int rows = order - p;
-    int ne;
-    double cu0[NM], cuk[NM];
-    cu0[0] = G0[p];
-    if (!coulombOnly) cuk[0] = Gk[p];
-    ne = ((rows + 1) * (rows + 2) * (rows + 3)) / 6;
-    for (int e = 1; e < ne; e++) {
-      char4 m = c_mi[e];
-      double v0, vk = 0.0;
+    const int rows = order - p;
+    const int ne = ((rows + 1) * (rows + 2) * (rows + 3)) / 6;
+    for (int e = ne - 1; e >= 1; e--) {
+      const char4 m = c_mi[e];
+      int a, b = -1;
+      double xa, fb = 0.0;
       if (m.x >= 1) {
-        int a = IDX(m.x - 1, m.y, m.z);
-        v0 = pa0[a] * x[0];
-        if (!coulombOnly) vk = pak[a] * x[0];
-        if (m.x >= 2) {
-          int b = IDX(m.x - 2, m.y, m.z);
-          v0 += pa0[b] * (m.x - 1);
-          if (!coulombOnly) vk += pak[b] * (m.x - 1);
-        }
+        a = IDX(m.x - 1, m.y, m.z); xa = x[0];
+        if (m.x >= 2) { b = IDX(m.x - 2, m.y, m.z); fb = m.x - 1; }
       } else if (m.y >= 1) {
-        int a = IDX(0, m.y - 1, m.z);
-        v0 = pa0[a] * x[1];
-        if (!coulombOnly) vk = pak[a] * x[1];
-        if (m.y >= 2) {
-          int b = IDX(0, m.y - 2, m.z);
-          v0 += pa0[b] * (m.y - 1);
-          if (!coulombOnly) vk += pak[b] * (m.y - 1);
-        }
+        a = IDX(0, m.y - 1, m.z); xa = x[1];
+        if (m.y >= 2) { b = IDX(0, m.y - 2, m.z); fb = m.y - 1; }
       } else {
-        int a = IDX(0, 0, m.z - 1);
-        v0 = pa0[a] * x[2];
-        if (!coulombOnly) vk = pak[a] * x[2];
-        if (m.z >= 2) {
-          int b = IDX(0, 0, m.z - 2);
-          v0 += pa0[b] * (m.z - 1);
-          if (!coulombOnly) vk += pak[b] * (m.z - 1);
-        }
+        a = IDX(0, 0, m.z - 1); xa = x[2];
+        if (m.z >= 2) { b = IDX(0, 0, m.z - 2); fb = m.z - 1; }
       }
-      cu0[e] = v0;
-      if (!coulombOnly) cuk[e] = vk;
+      double v0 = d0[a * stride] * xa;
+      if (b >= 0) v0 += d0[b * stride] * fb;
+      d0[e * stride] = v0;
+      if (!coulombOnly) {
+        double vk = dk[a * stride] * xa;
+        if (b >= 0) vk += dk[b * stride] * fb;
+        dk[e * stride] = vk;
+      }
     }
-    for (int e = 0; e < ne; e++) {
-      pa0[e] = cu0[e];
-      if (!coulombOnly) pak[e] = cuk[e];
-    }
+    d0[0] = G0[p];
+    if (!coulombOnly) dk[0] = Gk[p];
   }
-  int nOut = ((order + 1) * (order + 2) * (order + 3)) / 6;
-  for (int e = 0; e < nOut; e++) {
-    d0[e] = pa0[e];
-    if (!coulombOnly) dk[e] = pak[e];
-  }
+}
+
+template <int PM>
+__device__ __forceinline__ void derivs(int order, const double *x, double kappa, bool coulombOnly, double *d0,
+                                       double *dk) {
+  derivs_inplace<PM>(order, x, kappa, coulombOnly, d0, dk, 1);
 }
 
 // ------------------------------------------------------------------------
@@ -308,69 +294,108 @@ __global__ void m2m_kernel(int first, int count, int NM, int ordOut, int ordIn, 
 
 
 
-// M2L: one block per destination cube with a non-empty interaction list.
-// Threads < batch build the derivative tensors of one source each into
-// shared memory; then thread alpha accumulates the four local coefficients
-// over the batch (convM2L: l[alpha] += sum_beta c[beta] veck[alpha+beta]).
+// M2L: one block (128 threads) per destination cube with a non-empty
+// interaction list, sources in batches of 64.  Threads 0..63 each build the
+// derivative tensors D^a G0, D^a Gk of one source into shared-memory columns
+// while threads 64..127 stage the sign-weighted source moments; then thread
+// (alpha, half) accumulates the four local coefficients over half of the batch
+// (convM2L: l[alpha] += sum_beta c[beta] veck[alpha+beta]), and the two halves
+// are added at the end.  No atomics: every destination cube is one block.
 template <int PM>
-__global__ void __launch_bounds__(64)
+struct M2LShape {
+  static constexpr int NMP = nmom_c(PM);
+  static constexpr int B = PM <= 5 ? 64 : 32;               // sources per batch
+  static constexpr int S = B + 1;                           // padded column stride
+  static constexpr int AP = ((NMP + 31) / 32) * 32;         // threads per half
+  static constexpr int T = 2 * (AP > B ? AP : B);           // block size
+};
+
+template <int PM>
+__global__ void __launch_bounds__(M2LShape<PM>::T)
 m2l_kernel(int nDst, const int *__restrict__ dstList, const int *__restrict__ m2lOff,
            const int *__restrict__ m2lSrc, const double *__restrict__ ctr, const int *__restrict__ ordOfCube,
            const int *__restrict__ lstOff, const int *__restrict__ lst, int NM, double kappa, double eps,
            const double *__restrict__ momPot, const double *__restrict__ momDpdn, double *lec1, double *lec2,
            double *lec3, double *lec4) {
-  constexpr int NMP = nmom_c(PM);
-  constexpr int kM2LBatch = PM <= 5 ? 8 : 4;   // shared memory: 5*batch*nMom doubles
-  __shared__ double sc1[kM2LBatch][NMP], sc2[kM2LBatch][NMP];
-  __shared__ double sv1[kM2LBatch][NMP], sv2[kM2LBatch][NMP], sv3[kM2LBatch][NMP];
+  typedef M2LShape<PM> Sh;
+  constexpr int NMP = Sh::NMP, B = Sh::B, S = Sh::S, H = Sh::T / 2;
+  extern __shared__ double sm[];
+  double *sD0 = sm, *sDk = sD0 + NMP * S, *sC1 = sDk + NMP * S, *sC2 = sC1 + NMP * S;
+  int *sOff = (int *)(sC2 + NMP * S);
+  int *sLst = sOff + NMP + 1;
   if ((int)blockIdx.x >= nDst) return;
   const int f = dstList[blockIdx.x];
   const int order = ordOfCube[f];
   const int nm = ((order + 1) * (order + 2) * (order + 3)) / 6;
   const int o0 = m2lOff[f], o1 = m2lOff[f + 1];
-  const int al = threadIdx.x;
+  const int nl = lstOff[NMP];
+  for (int i = threadIdx.x; i <= NMP; i += blockDim.x) sOff[i] = lstOff[i];
+  for (int i = threadIdx.x; i < nl; i += blockDim.x) sLst[i] = lst[i];
+  const int t = threadIdx.x;
+  const int al = t % H, half = t / H;
   const int degA = (al < nm) ? c_mi[al].w : 0;
+  const double ieps = 1.0 / eps;
+  const double cx = ctr[3 * f], cy = ctr[3 * f + 1], cz = ctr[3 * f + 2];
   double l1 = 0.0, l2 = 0.0, l3 = 0.0, l4 = 0.0;
-  for (int b0 = o0; b0 < o1; b0 += kM2LBatch) {
-    const int nb = min(kM2LBatch, o1 - b0);
-    if (threadIdx.x < nb) {
-      const int t = threadIdx.x;
-      const int s = m2lSrc[b0 + t];
-      double r[3] = {ctr[3 * f] - ctr[3 * s], ctr[3 * f + 1] - ctr[3 * s + 1], ctr[3 * f + 2] - ctr[3 * s + 2]};
-      double d0[NMP], dk[NMP];
-      derivs<PM>(order, r, kappa, false, d0, dk);
-      for (int e = 0; e < nm; e++) {
-        const double sg = c_sgn3[e];
-        sc1[t][e] = sg * momPot[(size_t)s * NM + e];
-        sc2[t][e] = sg * momDpdn[(size_t)s * NM + e];
-        sv1[t][e] = d0[e] - dk[e];
-        sv2[t][e] = eps * dk[e] - d0[e];
-        sv3[t][e] = d0[e] - dk[e] / eps;
+  for (int b0 = o0; b0 < o1; b0 += B) {
+    const int nb = min(B, o1 - b0);
+    if (t < B) {
+      if (t < nb) {
+        const int s = m2lSrc[b0 + t];
+        const double r[3] = {cx - ctr[3 * s], cy - ctr[3 * s + 1], cz - ctr[3 * s + 2]};
+        derivs_inplace<PM>(order, r, kappa, false, sD0 + t, sDk + t, S);
+      }
+    } else if (t < 2 * B) {
+      const int j = t - B;
+      if (j < nb) {
+        const int s = m2lSrc[b0 + j];
+        for (int e = 0; e < nm; e++) {
+          const double sg = c_sgn3[e];
+          sC1[e * S + j] = sg * momPot[(size_t)s * NM + e];
+          sC2[e * S + j] = sg * momDpdn[(size_t)s * NM + e];
+        }
       }
     }
     __syncthreads();
     if (al < nm) {
-      const int q0 = lstOff[al], q1 = lstOff[al + 1];
-      for (int t = 0; t < nb; t++) {
-        for (int q = q0; q < q1; q++) {
-          const int ent = lst[q];
-          const int ib = ent & 1023, ig = (ent >> 10) & 1023, db = ent >> 20;
-          if (db > order - degA) break;
-          l1 += sc2[t][ib] * sv1[t][ig];
-          l2 += sc1[t][ib] * sv2[t][ig];
-          l3 += sc2[t][ib] * sv3[t][ig];
-          l4 -= sc1[t][ib] * sv1[t][ig];
+      const int q0 = sOff[al], q1 = sOff[al + 1];
+      const int hb = (B + 1) / 2;
+      const int j0 = half * hb, j1 = min(nb, j0 + hb);
+      for (int q = q0; q < q1; q++) {
+        const int ent = sLst[q];
+        const int ib = ent & 1023, ig = (ent >> 10) & 1023, db = ent >> 20;
+        if (db > order - degA) break;
+        const double *pc1 = sC1 + ib * S, *pc2 = sC2 + ib * S;
+        const double *p0 = sD0 + ig * S, *pk = sDk + ig * S;
+        for (int j = j0; j < j1; j++) {
+          const double d0 = p0[j], dk = pk[j], c1 = pc1[j], c2 = pc2[j];
+          const double v1 = d0 - dk;
+          l1 += c2 * v1;
+          l2 += c1 * (eps * dk - d0);
+          l3 += c2 * (d0 - dk * ieps);
+          l4 -= c1 * v1;
         }
       }
     }
     __syncthreads();
   }
-  if (al < nm) {
-    lec1[(size_t)f * NM + al] += l1;
-    lec2[(size_t)f * NM + al] += l2;
-    lec3[(size_t)f * NM + al] += l3;
-    lec4[(size_t)f * NM + al] += l4;
+  // combine the two halves (the moment columns are free scratch now)
+  if (half == 1 && al < nm) {
+    sC1[al] = l1; sC1[H + al] = l2; sC1[2 * H + al] = l3; sC1[3 * H + al] = l4;
   }
+  __syncthreads();
+  if (half == 0 && al < nm) {
+    lec1[(size_t)f * NM + al] += l1 + sC1[al];
+    lec2[(size_t)f * NM + al] += l2 + sC1[H + al];
+    lec3[(size_t)f * NM + al] += l3 + sC1[2 * H + al];
+    lec4[(size_t)f * NM + al] += l4 + sC1[3 * H + al];
+  }
+}
+
+template <int PM>
+size_t m2l_smem_bytes(int nList) {
+  typedef M2LShape<PM> Sh;
+  return 4 * (size_t)Sh::NMP * Sh::S * sizeof(double) + (Sh::NMP + 1 + nList) * sizeof(int);
 }
 
 // L2L: one block per child cube of one level (parents one level up)
@@ -454,7 +479,13 @@ static void launch_leaf_moments(Context &c, int order) {
 template <int PM>
 static void launch_m2l_t(Context &c) {
   const size_t plane = (size_t)c.pt.nFmm * c.NM;
-  m2l_kernel<PM><<<(unsigned)c.h_m2lDst.size(), 64, 0, c.stream>>>(
+  const size_t shm = m2l_smem_bytes<PM>(c.nConvList);
+  static int attrDone[kMaxOrder + 1] = {0};
+  if (!attrDone[PM]) {
+    cudaFuncSetAttribute(m2l_kernel<PM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm + 4096);
+    attrDone[PM] = 1;
+  }
+  m2l_kernel<PM><<<(unsigned)c.h_m2lDst.size(), M2LShape<PM>::T, shm, c.stream>>>(
       (int)c.h_m2lDst.size(), c.d_m2lDst, c.d_m2lOff, c.d_m2lSrc, c.d_cubeCtr, c.d_ordM2L, c.d_lstOff, c.d_lst,
       c.NM, c.prm.kappa, c.epsilon, c.d_mom, c.d_mom + plane, c.d_lec, c.d_lec + plane, c.d_lec + 2 * plane,
       c.d_lec + 3 * plane);
@@ -503,6 +534,7 @@ bool setup_fmm(Context &c) {
   }
   lstOff[c.NM] = (int)lst.size();
   mOff[c.NM] = (int)mLst.size();
+  c.nConvList = (int)lst.size();
   if (!c.arena.upload(&c.d_lstOff, lstOff, s) || !c.arena.upload(&c.d_lst, lst, s) ||
       !c.arena.upload(&c.d_mOff, mOff, s) || !c.arena.upload(&c.d_mLst, mLst, s))
     return false;

@@ -241,6 +241,19 @@ bool setup_near(Context &c) {
               c.prm.quad_order);
     return false;
   }
+  // the direct operator: every leaf is near every leaf
+  if (c.dense) {
+    PanelTree &w = c.pt;
+    w.nearOff.assign(w.nLeaves + 1, 0);
+    w.nearSrc.clear();
+    w.nearDst.clear();
+    for (int L = 0; L < w.nLeaves; L++) {
+      w.nearOff[L] = (int)w.nearSrc.size();
+      for (int S = 0; S < w.nLeaves; S++) { w.nearSrc.push_back(S); w.nearDst.push_back(L); }
+    }
+    w.nearOff[w.nLeaves] = (int)w.nearSrc.size();
+    if (!c.arena.upload(&c.d_nearOff, w.nearOff, s) || !c.arena.upload(&c.d_nearSrc, w.nearSrc, s)) return false;
+  }
   // warp tasks: (leaf, group of 32 targets)
   std::vector<int2> work;
   c.maxLeaf = 0;
