@@ -30,6 +30,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -291,10 +292,13 @@ def run_ours(args):
         peak = n_sm * 64 * 2 * sm_mhz * 1e6 / 1e12
         peak_src = "FP64 SIMT FMA pipe: %d SMs x 64 lanes x 2 flop x %.0f MHz (median SM clock sampled)" % (n_sm, sm_mhz)
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "near_apply_%s_traffic.json" % args.precision)
+    # DRAM bytes per launch from the committed ncu summary of this kernel and workload
+    tname = "near_apply_kernel_%s_%s.md" % ("float" if prec == lib.MIXED else "double", args.case)
+    prof = os.path.join(ROOT, "profiles", tname)
     if os.path.exists(prof):
         with open(prof) as fp:
-            traffic = json.load(fp).get("dram_bytes_per_launch")
+            m = re.search(r"dram_bytes_per_launch \| (\d+)", fp.read())
+        traffic = int(m.group(1)) if m else None
     cpu = None
     if not args.no_cpu_baseline:
         v, kind, cores, sample = cpu_reference_rate(base, opts, args.cpu_reps, 1, budget=30.0)
