@@ -7,3 +7,4 @@
 #include "solver.cu"
 #include "api.cu"
 #include "abi.cu"
+#include "noalloc.cu"

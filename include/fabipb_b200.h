@@ -95,6 +95,16 @@ int fabipb_b200_rhs(void *ctx, int use_tree, double *rhs, int on_device);
 /* raw solvation energy sum (before 2*pi*332.0716), panel-charge-tree walk
    (applyPanelChargeTreeEnergy, src/treecode.c:927) */
 int fabipb_b200_energy(void *ctx, const double *sgm, double *raw, int on_device);
+/* the same energy sum, allocating nothing: sgm (2N) and raw (1 double) are
+   DEVICE pointers, the work is queued on the context's stream and *raw is
+   ready when that stream reaches it.  Per-block partial sums go to a fixed
+   128 KiB array in the library's device image (limit 4,194,304 panels); the
+   charge tree must already exist (one fabipb_b200_energy or tree
+   fabipb_b200_rhs call builds it).  The first call on a device looks up the
+   array's address and should come before any stream capture; calls that
+   overlap on one GPU share the array and race.  No counterpart in the
+   reference, whose energy path allocates per call. */
+int fabipb_b200_energy_noalloc(void *ctx, const double *sgm, double *raw);
 /* preconditioner (src/precond_fmm.c): mode 2 block LU, 3 diagonal, -1 none */
 int fabipb_b200_precond_setup(void *ctx, int mode);
 int fabipb_b200_precond_apply(void *ctx, const double *b, double *x, int on_device);
