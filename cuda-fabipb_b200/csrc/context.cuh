@@ -61,6 +61,8 @@ struct Context {
   int *d_kidFirst = nullptr, *d_kidCount = nullptr;  // FMM indices of the children
   int *d_ordM2L = nullptr;                     // per FMM cube
   int nConvList = 0;                           // entries of d_lst
+  long long nM2LPairs = 0;
+  double2 *d_m2lTens = nullptr;                // [nMom][pairs] (D G0, D Gk) per M2L pair
 
   // ---- scratch vectors for host-pointer calls ------------------------
   double *d_x = nullptr, *d_y = nullptr, *d_w = nullptr;

@@ -20,6 +20,8 @@
 #include <cmath>
 #include <vector>
 
+#include <utility>
+
 #include "context.cuh"
 
 namespace fb {
@@ -301,101 +303,278 @@ __global__ void m2m_kernel(int first, int count, int NM, int ordOut, int ordIn, 
 // (alpha, half) accumulates the four local coefficients over half of the batch
 // (convM2L: l[alpha] += sum_beta c[beta] veck[alpha+beta]), and the two halves
 // are added at the end.  No atomics: every destination cube is one block.
+// M2L derivative tensors depend only on the geometry (r = x_dst - x_src), so
+// they are built once at setup for every interaction pair and stored
+// entry-major as (D^e G0, D^e Gk) pairs, tens[e][pair], which makes the
+// per-matvec loads of a warp's 32 consecutive pairs coalesced.
+template <int PM>
+__global__ void m2l_tensor_kernel(long long nPairs, const int *__restrict__ pairSrc, const int *__restrict__ pairDst,
+                                  const double *__restrict__ ctr, const int *__restrict__ ordOfCube, double kappa,
+                                  double2 *tens) {
+  constexpr int NMP = nmom_c(PM);
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nPairs) return;
+  const int s = pairSrc[k], f = pairDst[k];
+  const int order = ordOfCube[f];
+  const double r[3] = {ctr[3 * f] - ctr[3 * s], ctr[3 * f + 1] - ctr[3 * s + 1], ctr[3 * f + 2] - ctr[3 * s + 2]};
+  double d0[NMP], dk[NMP];
+  derivs<PM>(order, r, kappa, false, d0, dk);
+  const int nm = ((order + 1) * (order + 2) * (order + 3)) / 6;
+  for (int e = 0; e < NMP; e++)
+    tens[(size_t)e * nPairs + k] = e < nm ? make_double2(d0[e], dk[e]) : make_double2(0.0, 0.0);
+}
+
+// Sum four values over the 32 lanes with six shuffles: after the call lane 0
+// holds the total of v[0], lane 8 of v[1], lane 16 of v[2], lane 24 of v[3].
+__device__ __forceinline__ double warp_sum4(double a, double b, double c, double d, int lane) {
+  const bool hi16 = lane & 16;
+  double s0 = hi16 ? a : c, s1 = hi16 ? b : d;      // sent away
+  double k0 = hi16 ? c : a, k1 = hi16 ? d : b;      // kept
+  k0 += __shfl_xor_sync(0xffffffffu, s0, 16);
+  k1 += __shfl_xor_sync(0xffffffffu, s1, 16);
+  const bool hi8 = lane & 8;
+  double k = hi8 ? k1 : k0;
+  k += __shfl_xor_sync(0xffffffffu, hi8 ? k0 : k1, 8);
+  k += __shfl_xor_sync(0xffffffffu, k, 4);
+  k += __shfl_xor_sync(0xffffffffu, k, 2);
+  k += __shfl_xor_sync(0xffffffffu, k, 1);
+  return k;
+}
+
+// M2L conv: one warp per destination cube.  Lanes take 32 interaction pairs
+// at a time and stage their sources' sign-weighted moments in a per-lane
+// shared-memory column; the warp then walks the (alpha, beta) list of the
+// cube's order in lock step and, per output coefficient alpha, reduces the
+// four partial sums over the lanes into a per-warp shared accumulator.
+// convM2L (src/expan.c:258-290): l1 += c2*(G0-Gk), l2 += c1*(eps Gk - G0),
+// l3 += c2*(G0 - Gk/eps), l4 -= c1*(G0-Gk), c = sgn3 .* moments.
 template <int PM>
 struct M2LShape {
   static constexpr int NMP = nmom_c(PM);
-  static constexpr int B = PM <= 5 ? 64 : 32;               // sources per batch
-  static constexpr int S = B + 1;                           // padded column stride
-  static constexpr int AP = ((NMP + 31) / 32) * 32;         // threads per half
-  static constexpr int T = 2 * (AP > B ? AP : B);           // block size
+  static constexpr int W = PM <= 4 ? 4 : (PM <= 6 ? 2 : 1);   // warps per block
+  static constexpr size_t warpBytes = (size_t)NMP * 32 * sizeof(double2) + 4 * NMP * sizeof(double);
+  static constexpr size_t bytes = W * warpBytes;
 };
 
 template <int PM>
-__global__ void __launch_bounds__(M2LShape<PM>::T)
+__global__ void __launch_bounds__(M2LShape<PM>::W * 32)
 m2l_kernel(int nDst, const int *__restrict__ dstList, const int *__restrict__ m2lOff,
-           const int *__restrict__ m2lSrc, const double *__restrict__ ctr, const int *__restrict__ ordOfCube,
-           const int *__restrict__ lstOff, const int *__restrict__ lst, int NM, double kappa, double eps,
+           const int *__restrict__ m2lSrc, const int *__restrict__ ordOfCube, const int *__restrict__ lstOff,
+           const int *__restrict__ lst, long long nPairs, const double2 *__restrict__ tens, int NM, double eps,
            const double *__restrict__ momPot, const double *__restrict__ momDpdn, double *lec1, double *lec2,
            double *lec3, double *lec4) {
   typedef M2LShape<PM> Sh;
-  constexpr int NMP = Sh::NMP, B = Sh::B, S = Sh::S, H = Sh::T / 2;
-  extern __shared__ double sm[];
-  double *sD0 = sm, *sDk = sD0 + NMP * S, *sC1 = sDk + NMP * S, *sC2 = sC1 + NMP * S;
-  int *sOff = (int *)(sC2 + NMP * S);
-  int *sLst = sOff + NMP + 1;
-  if ((int)blockIdx.x >= nDst) return;
-  const int f = dstList[blockIdx.x];
+  constexpr int NMP = Sh::NMP;
+  extern __shared__ double2 m2lSmem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2 *sC = m2lSmem + (size_t)warp * (Sh::warpBytes / sizeof(double2));
+  double *sAcc = reinterpret_cast<double *>(sC + NMP * 32);   // [4][NMP]
+  const int bi = blockIdx.x * Sh::W + warp;
+  if (bi >= nDst) return;  // warp-uniform
+  const int f = dstList[bi];
   const int order = ordOfCube[f];
   const int nm = ((order + 1) * (order + 2) * (order + 3)) / 6;
   const int o0 = m2lOff[f], o1 = m2lOff[f + 1];
-  const int nl = lstOff[NMP];
-  for (int i = threadIdx.x; i <= NMP; i += blockDim.x) sOff[i] = lstOff[i];
-  for (int i = threadIdx.x; i < nl; i += blockDim.x) sLst[i] = lst[i];
-  const int t = threadIdx.x;
-  const int al = t % H, half = t / H;
-  const int degA = (al < nm) ? c_mi[al].w : 0;
   const double ieps = 1.0 / eps;
-  const double cx = ctr[3 * f], cy = ctr[3 * f + 1], cz = ctr[3 * f + 2];
-  double l1 = 0.0, l2 = 0.0, l3 = 0.0, l4 = 0.0;
-  for (int b0 = o0; b0 < o1; b0 += B) {
-    const int nb = min(B, o1 - b0);
-    if (t < B) {
-      if (t < nb) {
-        const int s = m2lSrc[b0 + t];
-        const double r[3] = {cx - ctr[3 * s], cy - ctr[3 * s + 1], cz - ctr[3 * s + 2]};
-        derivs_inplace<PM>(order, r, kappa, false, sD0 + t, sDk + t, S);
-      }
-    } else if (t < 2 * B) {
-      const int j = t - B;
-      if (j < nb) {
-        const int s = m2lSrc[b0 + j];
-        for (int e = 0; e < nm; e++) {
-          const double sg = c_sgn3[e];
-          sC1[e * S + j] = sg * momPot[(size_t)s * NM + e];
-          sC2[e * S + j] = sg * momDpdn[(size_t)s * NM + e];
-        }
-      }
+  for (int e = lane; e < 4 * NMP; e += 32) sAcc[e] = 0.0;
+  for (int b0 = o0; b0 < o1; b0 += 32) {
+    const int k = b0 + lane;
+    const bool live = k < o1;
+    const int s = live ? m2lSrc[k] : 0;
+    for (int e = 0; e < nm; e++) {
+      const double sg = c_sgn3[e];
+      sC[e * 32 + lane] = live ? make_double2(sg * momPot[(size_t)s * NM + e], sg * momDpdn[(size_t)s * NM + e])
+                               : make_double2(0.0, 0.0);
     }
-    __syncthreads();
-    if (al < nm) {
-      const int q0 = sOff[al], q1 = sOff[al + 1];
-      const int hb = (B + 1) / 2;
-      const int j0 = half * hb, j1 = min(nb, j0 + hb);
+    __syncwarp();
+    const double2 *T = tens + (live ? k : o0);
+    for (int al = 0; al < nm; al++) {
+      const int q0 = __ldg(lstOff + al), q1 = __ldg(lstOff + al + 1);
+      const int lim = order - c_mi[al].w;
+      double l1 = 0.0, l2 = 0.0, l3 = 0.0, l4 = 0.0;
+#pragma unroll 4
       for (int q = q0; q < q1; q++) {
-        const int ent = sLst[q];
-        const int ib = ent & 1023, ig = (ent >> 10) & 1023, db = ent >> 20;
-        if (db > order - degA) break;
-        const double *pc1 = sC1 + ib * S, *pc2 = sC2 + ib * S;
-        const double *p0 = sD0 + ig * S, *pk = sDk + ig * S;
-        for (int j = j0; j < j1; j++) {
-          const double d0 = p0[j], dk = pk[j], c1 = pc1[j], c2 = pc2[j];
-          const double v1 = d0 - dk;
-          l1 += c2 * v1;
-          l2 += c1 * (eps * dk - d0);
-          l3 += c2 * (d0 - dk * ieps);
-          l4 -= c1 * v1;
-        }
+        const int ent = __ldg(lst + q);
+        if ((ent >> 20) > lim) break;   // |beta| beyond this cube's order
+        const int ib = ent & 1023, ig = (ent >> 10) & 1023;
+        const double2 d = T[(size_t)ig * nPairs];
+        const double2 c = sC[ib * 32 + lane];
+        const double v1 = d.x - d.y;
+        l1 += c.y * v1;
+        l2 += c.x * (eps * d.y - d.x);
+        l3 += c.y * (d.x - d.y * ieps);
+        l4 -= c.x * v1;
       }
+      const double t = warp_sum4(l1, l2, l3, l4, lane);
+      if ((lane & 7) == 0) sAcc[(lane >> 3) * NMP + al] += t;
     }
-    __syncthreads();
+    __syncwarp();
   }
-  // combine the two halves (the moment columns are free scratch now)
-  if (half == 1 && al < nm) {
-    sC1[al] = l1; sC1[H + al] = l2; sC1[2 * H + al] = l3; sC1[3 * H + al] = l4;
-  }
-  __syncthreads();
-  if (half == 0 && al < nm) {
-    lec1[(size_t)f * NM + al] += l1 + sC1[al];
-    lec2[(size_t)f * NM + al] += l2 + sC1[H + al];
-    lec3[(size_t)f * NM + al] += l3 + sC1[2 * H + al];
-    lec4[(size_t)f * NM + al] += l4 + sC1[3 * H + al];
+  for (int e = lane; e < nm; e += 32) {
+    const size_t o = (size_t)f * NM + e;
+    lec1[o] += sAcc[e];
+    lec2[o] += sAcc[NMP + e];
+    lec3[o] += sAcc[2 * NMP + e];
+    lec4[o] += sAcc[3 * NMP + e];
   }
 }
 
+// Graded position of the multi-index (a, b, c): degree n = a+b+c first, then
+// a ascending, then b ascending (the order of the expansion tables).
+__host__ __device__ constexpr int gidx(int a, int b, int c) {
+  return ((a + b + c) * (a + b + c + 1) * (a + b + c + 2)) / 6 + a * (a + b + c + 1) - (a * (a - 1)) / 2 + b;
+}
+
+// M2L conv for orders up to 4 as straight-line code: every (alpha, beta)
+// entry of the convolution is a compile-time step, so each lane holds its
+// pair's derivative tensors in registers (loaded once per batch, all loads in
+// flight together), reads its source's moments from a padded shared-memory
+// column, and keeps the four raw sums S1 = sum c2 G0, S2 = sum c2 Gk,
+// S3 = sum c1 G0, S4 = sum c1 Gk per output coefficient, with the sign
+// (-1)^|beta| folded in.  The convM2L combinations (src/expan.c:258-290) are
+// formed once at the end: l1 = S1 - S2, l2 = eps S4 - S3, l3 = S1 - S2/eps,
+// l4 = S4 - S3.
+struct M2LEntry {
+  int al, ib, ig, dal, dsum, first, last;
+};
+
+// Entry q of the alpha-major (alpha, beta) list with |alpha + beta| <= PM.
 template <int PM>
-size_t m2l_smem_bytes(int nList) {
-  typedef M2LShape<PM> Sh;
-  return 4 * (size_t)Sh::NMP * Sh::S * sizeof(double) + (Sh::NMP + 1 + nList) * sizeof(int);
+__host__ __device__ constexpr M2LEntry m2l_entry(int q) {
+  int i = 0;
+  for (int n = 0; n <= PM; n++)
+    for (int a = 0; a <= n; a++)
+      for (int b = 0; b <= n - a; b++) {
+        const int c = n - a - b;
+        for (int m = 0; m <= PM - n; m++)
+          for (int a2 = 0; a2 <= m; a2++)
+            for (int b2 = 0; b2 <= m - a2; b2++, i++) {
+              if (i != q) continue;
+              const int c2 = m - a2 - b2;
+              M2LEntry e{gidx(a, b, c), gidx(a2, b2, c2), gidx(a + a2, b + b2, c + c2), n, n + m,
+                         m == 0 ? 1 : 0, (m == PM - n && a2 == m) ? 1 : 0};
+              return e;
+            }
+      }
+  return M2LEntry{0, 0, 0, 0, 0, 0, 0};
+}
+
+template <int PM>
+__host__ __device__ constexpr int m2l_entries() {
+  int i = 0;
+  for (int n = 0; n <= PM; n++) i += ((n + 1) * (n + 2) / 2) * nmom_c(PM - n);   // alphas of degree n x betas
+  return i;
+}
+
+// resident blocks per SM the register allocation of m2l_unrolled_kernel aims at
+#ifndef FB_M2L_MIN_BLOCKS
+#define FB_M2L_MIN_BLOCKS 3
+#endif
+
+template <int PM>
+struct M2LUnrolledShape {
+  static constexpr int NMP = nmom_c(PM);
+  static constexpr int W = 4;                         // warps per block
+  static constexpr size_t warpElems = (size_t)NMP * 32 + 2 * NMP;   // moment columns + [4][NMP] sums
+  static constexpr size_t bytes = W * warpElems * sizeof(double2);
+};
+
+// Moment column of source j, coefficient e: XOR-swizzled so that both the
+// staging stores (lanes over e) and the conv reads (lanes over j) are free of
+// bank conflicts.
+__device__ __forceinline__ int m2l_slot(int e, int j) { return e * 32 + (j ^ (e & 31)); }
+
+struct M2LSums {
+  double s1, s2, s3, s4;
+};
+
+// One (alpha, beta) entry.  FULL: the cube's order is PM, every entry counts.
+// The four sums of a coefficient are reduced over the lanes (component v's
+// total lands in lane 8v) and added to the warp's shared sums sAcc[v][alpha].
+template <int PM, int Q, bool FULL>
+__device__ __forceinline__ void m2l_step(M2LSums &S, const double2 *sC, const double2 (&T)[nmom_c(PM)], int lane,
+                                         int order, double *sAcc) {
+  constexpr M2LEntry E = m2l_entry<PM>(Q);
+  if (E.first) S.s1 = S.s2 = S.s3 = S.s4 = 0.0;
+  if (FULL || E.dsum <= order) {
+    const double2 mo = sC[m2l_slot(E.ib, lane)];
+    const double2 d = T[E.ig];
+    if ((E.dsum - E.dal) & 1) {
+      S.s1 -= mo.y * d.x; S.s2 -= mo.y * d.y; S.s3 -= mo.x * d.x; S.s4 -= mo.x * d.y;
+    } else {
+      S.s1 += mo.y * d.x; S.s2 += mo.y * d.y; S.s3 += mo.x * d.x; S.s4 += mo.x * d.y;
+    }
+  }
+  if (E.last && (FULL || E.dal <= order)) {
+    const double t = warp_sum4(S.s1, S.s2, S.s3, S.s4, lane);
+    if ((lane & 7) == 0) sAcc[(lane >> 3) * nmom_c(PM) + E.al] += t;
+  }
+}
+
+template <int PM, bool FULL, int... Q>
+__device__ __forceinline__ void m2l_steps(std::integer_sequence<int, Q...>, M2LSums &S, const double2 *sC,
+                                          const double2 (&T)[nmom_c(PM)], int lane, int order, double *sAcc) {
+  (m2l_step<PM, Q, FULL>(S, sC, T, lane, order, sAcc), ...);
+}
+
+template <int PM>
+__global__ void __launch_bounds__(128, FB_M2L_MIN_BLOCKS)
+m2l_unrolled_kernel(int nDst, const int *__restrict__ dstList, const int *__restrict__ m2lOff,
+                    const int *__restrict__ m2lSrc, const int *__restrict__ ordOfCube, long long nPairs,
+                    const double2 *__restrict__ tens, int NM, double eps, const double *__restrict__ momPot,
+                    const double *__restrict__ momDpdn, double *lec1, double *lec2, double *lec3, double *lec4) {
+  typedef M2LUnrolledShape<PM> Sh;
+  constexpr int NMP = Sh::NMP;
+  extern __shared__ double2 m2luSmem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2 *sC = m2luSmem + (size_t)warp * Sh::warpElems;
+  double *sAcc = reinterpret_cast<double *>(sC + NMP * 32);   // [4][NMP]
+  const int bi = blockIdx.x * Sh::W + warp;
+  if (bi >= nDst) return;  // warp-uniform
+  const int f = dstList[bi];
+  const int order = ordOfCube[f];
+  const int o0 = m2lOff[f], o1 = m2lOff[f + 1];
+  for (int e = lane; e < 4 * NMP; e += 32) sAcc[e] = 0.0;
+  for (int b0 = o0; b0 < o1; b0 += 32) {
+    const int k = b0 + lane;
+    const bool live = k < o1;
+    const int nb = min(32, o1 - b0);
+    const int mySrc = live ? m2lSrc[k] : 0;
+    __syncwarp();   // the previous batch's reads of sC are done
+    // stage the batch's moments: one source at a time, lanes over coefficients
+#pragma unroll 1
+    for (int j = 0; j < 32; j++) {
+      const int sj = __shfl_sync(0xffffffffu, mySrc, j);
+#pragma unroll
+      for (int e0 = 0; e0 < NMP; e0 += 32) {
+        const int e = e0 + lane;
+        if (e < NMP)
+          sC[m2l_slot(e, j)] = j < nb ? make_double2(momPot[(size_t)sj * NM + e], momDpdn[(size_t)sj * NM + e])
+                                      : make_double2(0.0, 0.0);
+      }
+    }
+    double2 T[NMP];
+    const double2 *tp = tens + (live ? k : o0);
+#pragma unroll
+    for (int e = 0; e < NMP; e++) T[e] = tp[(size_t)e * nPairs];
+    __syncwarp();
+    M2LSums S{0.0, 0.0, 0.0, 0.0};
+    if (order == PM)
+      m2l_steps<PM, true>(std::make_integer_sequence<int, m2l_entries<PM>()>{}, S, sC, T, lane, order, sAcc);
+    else
+      m2l_steps<PM, false>(std::make_integer_sequence<int, m2l_entries<PM>()>{}, S, sC, T, lane, order, sAcc);
+  }
+  __syncwarp();
+  const int nm = ((order + 1) * (order + 2) * (order + 3)) / 6;
+  const double ieps = 1.0 / eps;
+  for (int e = lane; e < nm; e += 32) {
+    const double S1 = sAcc[e], S2 = sAcc[NMP + e], S3 = sAcc[2 * NMP + e], S4 = sAcc[3 * NMP + e];
+    const size_t o = (size_t)f * NM + e;
+    lec1[o] += S1 - S2;
+    lec2[o] += eps * S4 - S3;
+    lec3[o] += S1 - S2 * ieps;
+    lec4[o] += S4 - S3;
+  }
 }
 
 // L2L: one block per child cube of one level (parents one level up)
@@ -479,16 +658,37 @@ static void launch_leaf_moments(Context &c, int order) {
 template <int PM>
 static void launch_m2l_t(Context &c) {
   const size_t plane = (size_t)c.pt.nFmm * c.NM;
-  const size_t shm = m2l_smem_bytes<PM>(c.nConvList);
   static int attrDone[kMaxOrder + 1] = {0};
+  if (PM <= 4) {
+    typedef M2LUnrolledShape<PM <= 4 ? PM : 4> Sh;
+    if (!attrDone[PM]) {
+      cudaFuncSetAttribute(m2l_unrolled_kernel<PM <= 4 ? PM : 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)Sh::bytes);
+      attrDone[PM] = 1;
+    }
+    const unsigned grid = ceil_div((long long)c.h_m2lDst.size(), Sh::W);
+    m2l_unrolled_kernel<PM <= 4 ? PM : 4><<<grid, Sh::W * 32, Sh::bytes, c.stream>>>(
+        (int)c.h_m2lDst.size(), c.d_m2lDst, c.d_m2lOff, c.d_m2lSrc, c.d_ordM2L, c.nM2LPairs, c.d_m2lTens, c.NM,
+        c.epsilon, c.d_mom, c.d_mom + plane, c.d_lec, c.d_lec + plane, c.d_lec + 2 * plane, c.d_lec + 3 * plane);
+    return;
+  }
+  typedef M2LShape<PM> Sh;
   if (!attrDone[PM]) {
-    cudaFuncSetAttribute(m2l_kernel<PM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm + 4096);
+    cudaFuncSetAttribute(m2l_kernel<PM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::bytes);
     attrDone[PM] = 1;
   }
-  m2l_kernel<PM><<<(unsigned)c.h_m2lDst.size(), M2LShape<PM>::T, shm, c.stream>>>(
-      (int)c.h_m2lDst.size(), c.d_m2lDst, c.d_m2lOff, c.d_m2lSrc, c.d_cubeCtr, c.d_ordM2L, c.d_lstOff, c.d_lst,
-      c.NM, c.prm.kappa, c.epsilon, c.d_mom, c.d_mom + plane, c.d_lec, c.d_lec + plane, c.d_lec + 2 * plane,
+  const unsigned grid = ceil_div((long long)c.h_m2lDst.size(), Sh::W);
+  m2l_kernel<PM><<<grid, Sh::W * 32, Sh::bytes, c.stream>>>(
+      (int)c.h_m2lDst.size(), c.d_m2lDst, c.d_m2lOff, c.d_m2lSrc, c.d_ordM2L, c.d_lstOff, c.d_lst, c.nM2LPairs,
+      c.d_m2lTens, c.NM, c.epsilon, c.d_mom, c.d_mom + plane, c.d_lec, c.d_lec + plane, c.d_lec + 2 * plane,
       c.d_lec + 3 * plane);
+}
+
+template <int PM>
+static void launch_m2l_tensors(Context &c, const int *d_pairDst) {
+  m2l_tensor_kernel<PM><<<ceil_div(c.nM2LPairs, 128), 128, 0, c.stream>>>(c.nM2LPairs, c.d_m2lSrc, d_pairDst,
+                                                                         c.d_cubeCtr, c.d_ordM2L, c.prm.kappa,
+                                                                         c.d_m2lTens);
 }
 
 #define FB_DISPATCH_ORDER(P, FN, ...)        \
@@ -565,6 +765,18 @@ bool setup_fmm(Context &c) {
     return false;
   if (!c.arena.alloc_n(&c.d_mom, 2 * (size_t)pt.nFmm * c.NM) || !c.arena.alloc_n(&c.d_lec, 4 * (size_t)pt.nFmm * c.NM))
     return false;
+  // M2L derivative tensors, once per geometry
+  c.nM2LPairs = (long long)pt.m2lSrc.size();
+  if (c.nM2LPairs > 0) {
+    std::vector<int> pairDst(pt.m2lSrc.size());
+    for (int f = 0; f < pt.nFmm; f++)
+      for (int k = pt.m2lOff[f]; k < pt.m2lOff[f + 1]; k++) pairDst[k] = f;
+    int *d_pairDst = nullptr;
+    if (!c.arena.upload(&d_pairDst, pairDst, s)) return false;
+    if (!c.arena.alloc_n(&c.d_m2lTens, (size_t)c.NM * c.nM2LPairs)) return false;
+    FB_DISPATCH_ORDER(c.P, launch_m2l_tensors, c, d_pairDst);
+    FB_CUDA(cudaGetLastError());
+  }
   // leaf matrices
   if (!c.arena.alloc_n(&c.d_Q0, (size_t)c.NMleaf * c.n) || !c.arena.alloc_n(&c.d_Q1, (size_t)c.NMleaf * c.n))
     return false;
