@@ -40,10 +40,21 @@ struct Vec4<double> {
   typedef double4 t;
 };
 
-__device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
+// FP32: the single MUFU instructions (PTX rsqrt.approx / ex2.approx, flush
+// to zero; relative error ~2^-22, far below the FP32 P2P tolerance).  FP64:
+// the library functions.
+__device__ __forceinline__ float rsqrt_t(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 __device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
-// e^{-kappa r}: float uses the MUFU ex2 path with kexp = -kappa*log2(e)
-__device__ __forceinline__ float expneg_t(float kexp, float r) { return exp2f(kexp * r); }
+// e^{-kappa r}: float evaluates 2^(kexp r) with kexp = -kappa*log2(e)
+__device__ __forceinline__ float expneg_t(float kexp, float r) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(kexp * r));
+  return y;
+}
 __device__ __forceinline__ double expneg_t(double kexp, double r) { return exp(kexp * r); }
 
 template <typename T>
@@ -83,9 +94,17 @@ __global__ void near_pack_kernel(int n, const typename Vec4<T>::t *__restrict__ 
 }
 
 constexpr int kNearWarps = 4;
+// resident blocks per SM the register allocation of near_apply_kernel aims at
+#ifndef FB_NEAR_MIN_BLOCKS
+#define FB_NEAR_MIN_BLOCKS 8
+#endif
 
+// One warp per task (leaf L, group of up to 32 target panels).  A full group
+// puts one target on each lane; a partial group of mt targets gives each
+// target k = 32/mt lanes, which take every k-th source of a tile, and their
+// partial sums are added at the end, so short groups keep most lanes busy.
 template <typename T>
-__global__ void __launch_bounds__(kNearWarps * 32)
+__global__ void __launch_bounds__(kNearWarps * 32, FB_NEAR_MIN_BLOCKS)
 near_apply_kernel(int nWork, const int2 *__restrict__ work, const int *__restrict__ leafStart,
                   const int *__restrict__ leafCount, const int *__restrict__ nearOff,
                   const int *__restrict__ nearSrc, const double *__restrict__ leafCtr,
@@ -98,15 +117,19 @@ near_apply_kernel(int nWork, const int2 *__restrict__ work, const int *__restric
   typedef typename Vec4<T>::t V;
   __shared__ V sA[kNearWarps][32];
   __shared__ V sB[kNearWarps][32];
+  __shared__ T sR[kNearWarps][2][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int task = blockIdx.x * kNearWarps + warp;
   if (task >= nWork) return;  // warp-uniform
   const int2 wk = work[task];
   const int L = wk.x;
   const int base = leafStart[L], cnt = leafCount[L];
-  const int ti = 32 * wk.y + lane;
-  const bool valid = ti < cnt;
-  const int X = base + (valid ? ti : 0);
+  const int g0 = 32 * wk.y;
+  const int mt = min(32, cnt - g0);   // targets in this group
+  const int k = 32 / mt;              // lanes per target
+  const int t = lane / k, sub = lane - t * k;
+  const bool valid = t < mt;
+  const int X = base + g0 + (valid ? t : 0);
   const V tp = tgtP[X], tn = tgtN[X];
   const double cx = leafCtr[3 * L], cy = leafCtr[3 * L + 1], cz = leafCtr[3 * L + 2];
   T acc0 = (T)0, acc1 = (T)0;
@@ -125,7 +148,7 @@ near_apply_kernel(int nWork, const int2 *__restrict__ work, const int *__restric
       }
       __syncwarp();
 #pragma unroll 4
-      for (int jj = 0; jj < m; jj++) {
+      for (int jj = sub; jj < m; jj += k) {
         const V a = sA[warp][jj];
         const V b = sB[warp][jj];
         const T dx = tx - a.x, dy = ty - a.y, dz = tz - a.z;
@@ -152,7 +175,17 @@ near_apply_kernel(int nWork, const int2 *__restrict__ work, const int *__restric
       __syncwarp();
     }
   }
-  if (!valid) return;
+  if (k > 1) {   // warp-uniform: add the k partial sums of each target
+    sR[warp][0][lane] = acc0;
+    sR[warp][1][lane] = acc1;
+    __syncwarp();
+    if (valid && sub == 0)
+      for (int i = 1; i < k; i++) {
+        acc0 += sR[warp][0][lane + i];
+        acc1 += sR[warp][1][lane + i];
+      }
+  }
+  if (!valid || sub != 0) return;
   double e0 = 0.0, e1 = 0.0;
   const int s1 = spOff[X + 1];
   for (int e = spOff[X]; e < s1; e++) {
@@ -254,17 +287,31 @@ bool setup_near(Context &c) {
     w.nearOff[w.nLeaves] = (int)w.nearSrc.size();
     if (!c.arena.upload(&c.d_nearOff, w.nearOff, s) || !c.arena.upload(&c.d_nearSrc, w.nearSrc, s)) return false;
   }
-  // warp tasks: (leaf, group of 32 targets)
+  // warp tasks: (leaf, group of 32 targets), the most expensive first so the
+  // last wave of the grid holds the short tasks (a warp's time ~ sources / k,
+  // k = lanes per target)
   std::vector<int2> work;
+  std::vector<long long> cost;
   c.maxLeaf = 0;
   c.nearPanelPairs = 0;
   for (int L = 0; L < pt.nLeaves; L++) {
     int cnt = pt.leafCount[L];
     c.maxLeaf = std::max(c.maxLeaf, cnt);
-    for (int g = 0; g * 32 < cnt; g++) work.push_back(make_int2(L, g));
     long long srcs = 0;
     for (int p = pt.nearOff[L]; p < pt.nearOff[L + 1]; p++) srcs += pt.leafCount[pt.nearSrc[p]];
     c.nearPanelPairs += srcs * cnt;
+    for (int g = 0; g * 32 < cnt; g++) {
+      work.push_back(make_int2(L, g));
+      cost.push_back(srcs / (32 / std::min(32, cnt - 32 * g)));
+    }
+  }
+  {
+    std::vector<int> ord(work.size());
+    for (size_t i = 0; i < ord.size(); i++) ord[i] = (int)i;
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    std::vector<int2> sorted(work.size());
+    for (size_t i = 0; i < ord.size(); i++) sorted[i] = work[ord[i]];
+    work.swap(sorted);
   }
   c.nWork = (int)work.size();
   if (!c.arena.upload(&c.d_work, work, s)) return false;
