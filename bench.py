@@ -198,6 +198,46 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def solve_report(pan, ch, opts, device, st):
+    """Full solves of the same case in both precisions: direct RHS, block-LU
+    preconditioner, device GMRES from x0 = b (as the reference CLI), energy.
+    Times are CUDA-event times on the library's stream (the calls are
+    synchronous); setup = context (tree, near field, FMM lists) + RHS +
+    preconditioner."""
+    import torch
+    from fabipb_b200 import lib
+    out = {}
+    kcal = 2.0 * np.pi * 332.0716
+    for tag, prec in (("mixed", lib.MIXED), ("fp64", lib.FP64)):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        ev[0].record(st)
+        prm = lib.params(order=opts["order"], depth=opts["depth"], sep_ratio=opts["sep_ratio"], eps1=opts["eps1"],
+                         eps2=opts["eps2"], precision=prec, device=device)
+        s = lib.Surface(pan, prm, ch)
+        s.set_stream(st.cuda_stream)
+        b = s.rhs(use_tree=False)
+        s.precond_setup(2)
+        ev[1].record(st)
+        x, it, res, info = s.solve(b, b.copy(), restart=opts["restart"], maxit=100, tol=opts["tol"])
+        ev[2].record(st)
+        e = s.energy_raw(x) * kcal
+        ev[3].record(st)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - w0
+        out[tag] = {"gmres_s": ev[1].elapsed_time(ev[2]) / 1000.0, "setup_s": ev[0].elapsed_time(ev[1]) / 1000.0,
+                    "energy_s": ev[2].elapsed_time(ev[3]) / 1000.0, "wall_s": wall, "iterations": it,
+                    "residual": res, "info": info, "energy_kcal_mol": e}
+        s.close()
+    m, f = out["mixed"], out["fp64"]
+    out["energy_rel_err_mixed_vs_fp64"] = abs(m["energy_kcal_mol"] - f["energy_kcal_mol"]) / abs(f["energy_kcal_mol"])
+    out["gmres_speedup_mixed_vs_fp64"] = f["gmres_s"] / m["gmres_s"]
+    out["tol"] = opts["tol"]
+    out["restart"] = opts["restart"]
+    return out
+
+
 def run_ours(args):
     import torch
     from fabipb_b200 import lib, meshio
@@ -299,6 +339,7 @@ def run_ours(args):
         with open(prof) as fp:
             m = re.search(r"dram_bytes_per_launch \| (\d+)", fp.read())
         traffic = int(m.group(1)) if m else None
+    solve = None if args.no_solve else solve_report(pan, ch, opts, local, stream)
     cpu = None
     if not args.no_cpu_baseline:
         v, kind, cores, sample = cpu_reference_rate(base, opts, args.cpu_reps, 1, budget=30.0)
@@ -325,6 +366,7 @@ def run_ours(args):
         "gpu_launches": launches,
         "clocks": clocks,
         "setup_s": info["setup_seconds"],
+        "solve": solve,
     }
     if pg:
         pg.destroy_process_group()
@@ -343,6 +385,7 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=90.0,
                     help="seconds of timed reference matvecs at most (--impl reference)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-solve", action="store_true", help="skip the mixed/FP64 solve report")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

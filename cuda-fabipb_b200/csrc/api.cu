@@ -11,6 +11,31 @@
 
 namespace fb {
 
+bool trace_enabled() {
+  static const bool on = getenv("FABIPB_B200_TRACE") != nullptr;
+  return on;
+}
+
+static double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+StageTimer::StageTimer(const char *sc, cudaStream_t s) : scope(sc), stream(s), on(trace_enabled()), t(0.0) {
+  if (on) {
+    cudaStreamSynchronize(stream);
+    t = now_ms();
+  }
+}
+
+void StageTimer::mark(const char *stage) {
+  if (!on) return;
+  cudaStreamSynchronize(stream);
+  const double n = now_ms();
+  fprintf(stderr, "[fabipb_b200] %s.%s %.3f ms\n", scope, stage, n - t);
+  t = n;
+}
+
+
 static thread_local char g_err[1024] = "";
 
 void set_error(const char *fmt, ...) {
@@ -73,9 +98,11 @@ Context::~Context() {
 
 bool setup_geometry(Context &c, const double *vtx, const double *nrm, const double *area) {
   const int n = c.n;
+  StageTimer tm("create", c.stream);
   if (!build_panel_tree(c.pt, n, vtx, c.prm.depth, c.prm.height, c.prm.sep_ratio, c.prm.order,
                         c.prm.order_mom))
     return false;
+  tm.mark("octree_host");
   const PanelTree &pt = c.pt;
   c.h_vtx.resize(9 * (size_t)n);
   c.h_nrm.resize(3 * (size_t)n);
@@ -173,10 +200,14 @@ int create_context(const fabipb_b200_params *p, int n, const double *vtx, const 
     ok = false;
   }
   c->ownStream = ok;
+  StageTimer tm("create", c->stream);
   ok = ok && init_quad_tables();
   ok = ok && setup_geometry(*c, vtx, normal, area);
+  tm.mark("tree_and_geometry");
   ok = ok && setup_near(*c);
+  tm.mark("near_setup");
   ok = ok && setup_fmm(*c);
+  tm.mark("fmm_setup");
   if (ok && cudaStreamSynchronize(c->stream) != cudaSuccess) {
     set_error("setup kernels failed: %s", cudaGetErrorString(cudaGetLastError()));
     ok = false;
@@ -392,9 +423,12 @@ int fabipb_b200_set_charges(void *ctx, int m, const double *pos, const double *q
 int fabipb_b200_rhs(void *ctx, int use_tree, double *rhs, int on_device) {
   if (!valid_ctx(ctx) || rhs == nullptr) return 0;
   Context *c = (Context *)ctx;
-  return with_vectors(c, nullptr, rhs, false, on_device, [&](const double *, double *y) {
+  StageTimer tm("rhs", c->stream);
+  int ok = with_vectors(c, nullptr, rhs, false, on_device, [&](const double *, double *y) {
     return launch_rhs(*c, use_tree, y);
   });
+  tm.mark(use_tree ? "tree" : "direct");
+  return ok;
 }
 
 int fabipb_b200_energy(void *ctx, const double *sgm, double *raw, int on_device) {
@@ -443,9 +477,11 @@ int fabipb_b200_solve(void *ctx, const double *b, double *x, int restart, int ma
   Context *c = (Context *)ctx;
   int it = 0, inf = 0;
   double res = 0.0;
+  StageTimer tm("solve", c->stream);
   int ok = with_vectors(c, b, x, true, on_device, [&](const double *bd, double *xd) {
     return gmres_solve(*c, bd, xd, restart, maxit, tol, &it, &res, &inf);
   });
+  tm.mark("gmres");
   if (iters) *iters = it;
   if (resid) *resid = res;
   if (info) *info = inf;

@@ -24,6 +24,20 @@ __host__ __device__ constexpr int nmom_c(int p) { return ((p + 1) * (p + 2) * (p
 void set_error(const char *fmt, ...);
 const char *get_error();
 
+// Stage timing, the counterpart of the reference's -B=1 stage report: with
+// FABIPB_B200_TRACE set in the environment every mark() synchronises the
+// stream and prints "[fabipb_b200] scope.stage ms" to stderr; unset, mark()
+// does nothing and nothing is synchronised.
+bool trace_enabled();
+struct StageTimer {
+  const char *scope;
+  cudaStream_t stream;
+  bool on;
+  double t;
+  StageTimer(const char *sc, cudaStream_t s);
+  void mark(const char *stage);
+};
+
 // Throws nothing: CUDA failures are turned into a recorded message and a
 // false return so every C entry point can report 0.
 #define FB_CUDA(call)                                                              \

@@ -765,6 +765,7 @@ bool setup_fmm(Context &c) {
     return false;
   if (!c.arena.alloc_n(&c.d_mom, 2 * (size_t)pt.nFmm * c.NM) || !c.arena.alloc_n(&c.d_lec, 4 * (size_t)pt.nFmm * c.NM))
     return false;
+  StageTimer tm("fmm_setup", s);
   // M2L derivative tensors, once per geometry
   c.nM2LPairs = (long long)pt.m2lSrc.size();
   if (c.nM2LPairs > 0) {
@@ -781,8 +782,10 @@ bool setup_fmm(Context &c) {
   if (!c.arena.alloc_n(&c.d_Q0, (size_t)c.NMleaf * c.n) || !c.arena.alloc_n(&c.d_Q1, (size_t)c.NMleaf * c.n))
     return false;
   FB_CHECK(c.leafOrder >= 1, "leaf moment order %d must be >= 1", c.leafOrder);
+  tm.mark("m2l_tensors");
   FB_DISPATCH_ORDER(c.leafOrder, launch_leaf_moments, c, c.leafOrder);
   FB_CUDA(cudaGetLastError());
+  tm.mark("leaf_moments");
   return true;
 }
 

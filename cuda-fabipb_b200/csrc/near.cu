@@ -94,17 +94,46 @@ __global__ void near_pack_kernel(int n, const typename Vec4<T>::t *__restrict__ 
 }
 
 constexpr int kNearWarps = 4;
-// resident blocks per SM the register allocation of near_apply_kernel aims at
+// resident blocks per SM the register allocation of near_apply_kernel<float> aims at
 #ifndef FB_NEAR_MIN_BLOCKS
 #define FB_NEAR_MIN_BLOCKS 8
 #endif
+
+// One disjoint pair, one-point rule: the four KER4 kernels (src/kernel.c:109-147)
+// at d = target - source, times the source weights a.w = A*sigma_dpdn and
+// b.w = A*sigma_pot (the 4 pi and the target area are applied once at the end).
+template <typename T, typename V>
+__device__ __forceinline__ void near_pair(const V a, const V b, T tx, T ty, T tz, const V tn, T kappa, T kexp, T eps,
+                                          T ieps, T kap2, T &acc0, T &acc1) {
+  const T dx = tx - a.x, dy = ty - a.y, dz = tz - a.z;
+  const T r2 = dx * dx + dy * dy + dz * dz;
+  const T g = r2 > (T)0 ? rsqrt_t(r2) : (T)0;   // 1/r, 0 for the coincident pair
+  const T r = r2 * g;
+  const T e = expneg_t(kexp, r);
+  const T c = (kappa * r + (T)1) * e;           // (kappa r + 1) e^{-kappa r}
+  const T g2 = g * g;
+  const T h = g2 * g;
+  const T ipX = tn.x * dx + tn.y * dy + tn.z * dz;
+  const T ipY = b.x * dx + b.y * dy + b.z * dz;
+  const T ip0 = tn.x * b.x + tn.y * b.y + tn.z * b.z;
+  const T t1 = ipY * h;                          // dG0/dn_y * 4 pi
+  const T t2 = ipX * h;                          // dG0/dn_x * 4 pi
+  const T u = ipX * t1;
+  const T y0 = g - g * e;                        // G0 - Gk
+  const T y1 = t1 * (eps * c - (T)1);            // eps dGk/dn_y - dG0/dn_y
+  const T y2 = t2 * (c * ieps - (T)1);           // dGk/dn_x / eps - dG0/dn_x
+  const T dd = (ip0 * g - (T)3 * u) * g2;        // d2 G0 / dn_x dn_y
+  const T y3 = dd * (c - (T)1) - kap2 * e * u;
+  acc0 += y0 * a.w + y1 * b.w;
+  acc1 += y2 * a.w + y3 * b.w;
+}
 
 // One warp per task (leaf L, group of up to 32 target panels).  A full group
 // puts one target on each lane; a partial group of mt targets gives each
 // target k = 32/mt lanes, which take every k-th source of a tile, and their
 // partial sums are added at the end, so short groups keep most lanes busy.
 template <typename T>
-__global__ void __launch_bounds__(kNearWarps * 32, FB_NEAR_MIN_BLOCKS)
+__global__ void __launch_bounds__(kNearWarps * 32, sizeof(T) == 4 ? FB_NEAR_MIN_BLOCKS : 1)
 near_apply_kernel(int nWork, const int2 *__restrict__ work, const int *__restrict__ leafStart,
                   const int *__restrict__ leafCount, const int *__restrict__ nearOff,
                   const int *__restrict__ nearSrc, const double *__restrict__ leafCtr,
@@ -147,30 +176,14 @@ near_apply_kernel(int nWork, const int2 *__restrict__ work, const int *__restric
         sB[warp][lane] = srcB[sb + j0 + lane];
       }
       __syncwarp();
+      if (k == 1) {   // warp-uniform: a full group, unit stride
 #pragma unroll 4
-      for (int jj = sub; jj < m; jj += k) {
-        const V a = sA[warp][jj];
-        const V b = sB[warp][jj];
-        const T dx = tx - a.x, dy = ty - a.y, dz = tz - a.z;
-        const T r2 = dx * dx + dy * dy + dz * dz;
-        const T g = r2 > (T)0 ? rsqrt_t(r2) : (T)0;   // 1/r, 0 for the coincident pair
-        const T r = r2 * g;
-        const T e = expneg_t(kexp, r);
-        const T c = (kappa * r + (T)1) * e;           // (kappa r + 1) e^{-kappa r}
-        const T g2 = g * g;
-        const T h = g2 * g;
-        const T ipX = tn.x * dx + tn.y * dy + tn.z * dz;
-        const T ipY = b.x * dx + b.y * dy + b.z * dz;
-        const T ip0 = tn.x * b.x + tn.y * b.y + tn.z * b.z;
-        const T t1 = ipY * h;                          // dG0/dn_y * 4 pi
-        const T t2 = ipX * h;                          // dG0/dn_x * 4 pi
-        const T y0 = g - g * e;                        // G0 - Gk
-        const T y1 = t1 * (eps * c - (T)1);            // eps dGk/dn_y - dG0/dn_y
-        const T y2 = t2 * (c * ieps - (T)1);           // dGk/dn_x / eps - dG0/dn_x
-        const T dd = (ip0 * g - (T)3 * t1 * ipX) * g2; // d2 G0 / dn_x dn_y
-        const T y3 = dd * (c - (T)1) - kap2 * e * ipX * t1;
-        acc0 += y0 * a.w + y1 * b.w;
-        acc1 += y2 * a.w + y3 * b.w;
+        for (int jj = 0; jj < m; jj++)
+          near_pair(sA[warp][jj], sB[warp][jj], tx, ty, tz, tn, kappa, kexp, eps, ieps, kap2, acc0, acc1);
+      } else {
+#pragma unroll 4
+        for (int jj = sub; jj < m; jj += k)
+          near_pair(sA[warp][jj], sB[warp][jj], tx, ty, tz, tn, kappa, kexp, eps, ieps, kap2, acc0, acc1);
       }
       __syncwarp();
     }
@@ -316,6 +329,7 @@ bool setup_near(Context &c) {
   c.nWork = (int)work.size();
   if (!c.arena.upload(&c.d_work, work, s)) return false;
 
+  StageTimer tm("near_setup", s);
   // special pairs: panels sharing a vertex (exact coordinates), restricted to
   // near leaf pairs, plus the panel itself
   std::unordered_map<VKey, int, VKeyHash> vid;
@@ -374,6 +388,7 @@ bool setup_near(Context &c) {
     spOff[X + 1] = (int)spSrc.size();
   }
   c.nSpecial = (long long)spSrc.size();
+  tm.mark("special_pairs_host");
   int *d_spDst = nullptr;
   if (!c.arena.upload(&c.d_spOff, spOff, s)) return false;
   if (!c.arena.upload(&c.d_spSrc, spSrc, s)) return false;
@@ -386,6 +401,7 @@ bool setup_near(Context &c) {
     FB_CUDA(cudaGetLastError());
   }
 
+  tm.mark("special_coeff");
   // static target geometry relative to the leaf centres
   size_t vb = c.mixed ? sizeof(float4) : sizeof(double4);
   if (!c.arena.alloc(&c.d_tgtP, vb * n) || !c.arena.alloc(&c.d_tgtN, vb * n) ||

@@ -36,6 +36,8 @@ struct PrecondDev {
   std::vector<int> hStart, hSize;
   std::vector<long long> hOff;
   int *d_start = nullptr, *d_size = nullptr;
+  int2 *d_tiles = nullptr;   // (block, first row) tiles of the apply
+  int nTiles = 0;
   long long *d_off = nullptr;
   double *d_inv = nullptr;
   int maxM = 0;
@@ -105,20 +107,46 @@ __global__ void identity_kernel(int nBlocks, const int *__restrict__ bSize, cons
 }
 
 // x = blockdiag(inv) * b, block b gathers its pot/dpdn halves
-__global__ void pc_apply_kernel(int n, const int *__restrict__ bStart, const int *__restrict__ bSize,
-                                const long long *__restrict__ bOff, const double *__restrict__ inv,
-                                const double *__restrict__ rhs, double *x) {
-  extern __shared__ double sb[];
-  const int b = blockIdx.x;
+// Block-diagonal apply with the explicit inverses, one thread block per tile
+// of kPcRows rows of one diagonal block (tiles of large blocks spread over
+// many SMs).  Thread (row, quarter) sums a quarter of the columns; the
+// column-major inverse makes a warp's loads 32 consecutive doubles.  The
+// reference's per-block solve order (x = [pot; dpdn] of the cube's panels)
+// is src/precond_fmm.c:861-953.
+constexpr int kPcRows = 64, kPcSplit = 4;
+
+// streams the block factorisations are spread over
+#ifndef FB_PC_STREAMS
+#define FB_PC_STREAMS 16
+#endif
+
+template <typename TI>
+__global__ void __launch_bounds__(kPcRows * kPcSplit)
+pc_apply_kernel(int n, const int2 *__restrict__ tiles, const int *__restrict__ bStart, const int *__restrict__ bSize,
+                const long long *__restrict__ bOff, const TI *__restrict__ inv, const double *__restrict__ rhs,
+                double *x) {
+  __shared__ double red[kPcSplit][kPcRows];
+  const int2 tl = tiles[blockIdx.x];
+  const int b = tl.x, r0 = tl.y;
   const int hm = bSize[b], st = bStart[b], M = 2 * hm;
-  for (int c = threadIdx.x; c < M; c += blockDim.x) sb[c] = (c < hm) ? rhs[st + c] : rhs[n + st + c - hm];
+  const int rr = threadIdx.x % kPcRows, q = threadIdx.x / kPcRows;
+  const int r = r0 + rr;
+  const TI *Ib = inv + bOff[b];
+  const int c0 = (int)(((long long)M * q) / kPcSplit), c1 = (int)(((long long)M * (q + 1)) / kPcSplit);
+  double y = 0.0;
+  if (r < M) {
+#pragma unroll 4
+    for (int c = c0; c < c1; c++) {
+      const double xc = (c < hm) ? rhs[st + c] : rhs[n + st + c - hm];
+      y += (double)Ib[(size_t)c * M + r] * xc;
+    }
+  }
+  red[q][rr] = y;
   __syncthreads();
-  const double *Ib = inv + bOff[b];
-  for (int r = threadIdx.x; r < M; r += blockDim.x) {
-    double y = 0.0;
-    for (int c = 0; c < M; c++) y += Ib[(size_t)c * M + r] * sb[c];
-    if (r < hm) x[st + r] = y;
-    else x[n + st + r - hm] = y;
+  if (q == 0 && r < M) {
+    const double t = ((red[0][rr] + red[1][rr]) + red[2][rr]) + red[3][rr];
+    if (r < hm) x[st + r] = t;
+    else x[n + st + r - hm] = t;
   }
 }
 
@@ -149,10 +177,16 @@ bool precond_setup(Context &c, int mode) {
     p.maxM = std::max(p.maxM, 2 * hm);
   }
   p.nBlocks = (int)p.hSize.size();
+  std::vector<int2> tiles;
+  for (int b = 0; b < p.nBlocks; b++)
+    for (int r0 = 0; r0 < 2 * p.hSize[b]; r0 += kPcRows) tiles.push_back(make_int2(b, r0));
+  p.nTiles = (int)tiles.size();
   FB_CHECK(p.maxM <= 46340, "preconditioner block %d too large (increase -t)", p.maxM);
   cudaStream_t s = c.stream;
+  StageTimer tm("precond_setup", s);
   double *d_A = nullptr;
   if (!p.arena.upload(&p.d_start, p.hStart, s) || !p.arena.upload(&p.d_size, p.hSize, s) ||
+      !p.arena.upload(&p.d_tiles, tiles, s) ||
       !p.arena.upload(&p.d_off, p.hOff, s) || !p.arena.alloc_n(&p.d_inv, (size_t)off))
     return false;
   FB_CUDA(cudaMalloc((void **)&d_A, (size_t)off * sizeof(double)));
@@ -168,34 +202,66 @@ bool precond_setup(Context &c, int mode) {
     set_error("preconditioner assembly launch failed: %s", cudaGetErrorString(le));
     return false;
   }
-  cusolverDnHandle_t h = nullptr;
-  if (cusolverDnCreate(&h) != CUSOLVER_STATUS_SUCCESS) {
-    cudaFree(d_A);
-    set_error("cusolverDnCreate failed");
-    return false;
+  tm.mark("assemble");
+  // LU and explicit inverse of every block with cuSOLVER, spread over several
+  // streams: a single block of a few hundred rows keeps only a few SMs busy,
+  // so independent blocks run side by side.
+  const int ns = std::min(FB_PC_STREAMS, std::max(p.nBlocks, 1));
+  std::vector<cusolverDnHandle_t> hs(ns, nullptr);
+  std::vector<cudaStream_t> ss(ns, nullptr);
+  std::vector<double *> works(ns, nullptr);
+  std::vector<int *> pivs(ns, nullptr);
+  int lwork = 0, *d_info = nullptr;
+  cudaEvent_t evA = nullptr;
+  bool ok = cudaEventCreateWithFlags(&evA, cudaEventDisableTiming) == cudaSuccess;
+  ok = ok && cudaEventRecord(evA, s) == cudaSuccess;
+  for (int k = 0; ok && k < ns; k++) {
+    ok = cudaStreamCreateWithFlags(&ss[k], cudaStreamNonBlocking) == cudaSuccess &&
+         cusolverDnCreate(&hs[k]) == CUSOLVER_STATUS_SUCCESS && cusolverDnSetStream(hs[k], ss[k]) == CUSOLVER_STATUS_SUCCESS &&
+         cudaStreamWaitEvent(ss[k], evA, 0) == cudaSuccess;
   }
-  cusolverDnSetStream(h, s);
-  int lwork = 0, *d_piv = nullptr, *d_info = nullptr;
-  double *d_work = nullptr;
-  bool ok = true;
-  if (cusolverDnDgetrf_bufferSize(h, p.maxM, p.maxM, d_A, p.maxM, &lwork) != CUSOLVER_STATUS_SUCCESS) ok = false;
-  ok = ok && cudaMalloc((void **)&d_work, (size_t)std::max(lwork, 1) * sizeof(double)) == cudaSuccess;
-  ok = ok && cudaMalloc((void **)&d_piv, (size_t)p.maxM * sizeof(int)) == cudaSuccess;
+  if (ok && cusolverDnDgetrf_bufferSize(hs[0], p.maxM, p.maxM, d_A, p.maxM, &lwork) != CUSOLVER_STATUS_SUCCESS) ok = false;
+  for (int k = 0; ok && k < ns; k++)
+    ok = cudaMalloc((void **)&works[k], (size_t)std::max(lwork, 1) * sizeof(double)) == cudaSuccess &&
+         cudaMalloc((void **)&pivs[k], (size_t)p.maxM * sizeof(int)) == cudaSuccess;
   ok = ok && cudaMalloc((void **)&d_info, (size_t)p.nBlocks * sizeof(int)) == cudaSuccess;
-  for (int b = 0; ok && b < p.nBlocks; b++) {
+  // largest blocks first so the streams finish together
+  std::vector<int> order(p.nBlocks);
+  for (int b = 0; b < p.nBlocks; b++) order[b] = b;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return p.hSize[a] > p.hSize[b]; });
+  for (int q = 0; ok && q < p.nBlocks; q++) {
+    const int b = order[q], k = q % ns;
     int M = 2 * p.hSize[b];
     if (M == 0) continue;
     double *Ab = d_A + p.hOff[b], *Ib = p.d_inv + p.hOff[b];
-    if (cusolverDnDgetrf(h, M, M, Ab, M, d_work, d_piv, d_info + b) != CUSOLVER_STATUS_SUCCESS) ok = false;
-    if (ok && cusolverDnDgetrs(h, CUBLAS_OP_N, M, M, Ab, M, d_piv, Ib, M, d_info + b) != CUSOLVER_STATUS_SUCCESS)
+    if (cusolverDnDgetrf(hs[k], M, M, Ab, M, works[k], pivs[k], d_info + b) != CUSOLVER_STATUS_SUCCESS) ok = false;
+    if (ok && cusolverDnDgetrs(hs[k], CUBLAS_OP_N, M, M, Ab, M, pivs[k], Ib, M, d_info + b) != CUSOLVER_STATUS_SUCCESS)
       ok = false;
   }
+  // join: the main stream waits for every factor stream
+  for (int k = 0; k < ns; k++) {
+    if (!ss[k]) continue;
+    cudaEvent_t ev = nullptr;
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess) {
+      cudaEventRecord(ev, ss[k]);
+      cudaStreamWaitEvent(s, ev, 0);
+      cudaEventDestroy(ev);
+    } else {
+      ok = false;
+    }
+  }
+  tm.mark("factor_invert");
   std::vector<int> info(p.nBlocks, 0);
   if (ok) ok = cudaMemcpyAsync(info.data(), d_info, info.size() * sizeof(int), cudaMemcpyDeviceToHost, s) == cudaSuccess;
   if (ok) ok = cudaStreamSynchronize(s) == cudaSuccess;
-  cusolverDnDestroy(h);
-  cudaFree(d_work);
-  cudaFree(d_piv);
+  for (int k = 0; k < ns; k++) {
+    if (ss[k]) cudaStreamSynchronize(ss[k]);
+    if (hs[k]) cusolverDnDestroy(hs[k]);
+    if (ss[k]) cudaStreamDestroy(ss[k]);
+    cudaFree(works[k]);
+    cudaFree(pivs[k]);
+  }
+  if (evA) cudaEventDestroy(evA);
   cudaFree(d_info);
   cudaFree(d_A);
   FB_CHECK(ok, "preconditioner factorisation failed: %s", cudaGetErrorString(cudaGetLastError()));
@@ -208,8 +274,8 @@ bool precond_apply(Context &c, const double *b, double *x) {
   FB_CHECK(c.pc != nullptr, "preconditioner not set up");
   PrecondDev &p = *c.pc;
   if (p.mode == 2) {
-    pc_apply_kernel<<<p.nBlocks, 256, (size_t)p.maxM * sizeof(double), c.stream>>>(c.n, p.d_start, p.d_size, p.d_off,
-                                                                                 p.d_inv, b, x);
+    pc_apply_kernel<double><<<p.nTiles, kPcRows * kPcSplit, 0, c.stream>>>(c.n, p.d_tiles, p.d_start, p.d_size,
+                                                                           p.d_off, p.d_inv, b, x);
   } else if (p.mode == 3) {
     pc_diag_kernel<<<ceil_div(c.n, 256), 256, 0, c.stream>>>(c.n, c.d_area, (1.0 + c.epsilon) / 2.0,
                                                             (1.0 + 1.0 / c.epsilon) / 2.0, b, x);
@@ -288,6 +354,66 @@ __global__ void update_kernel(long long n, int k, const double *__restrict__ V, 
   }
 }
 
+// Sum of kRedBlocks partials in a fixed order (the dot_final_kernel order),
+// by every thread block alike; returns the total to all threads.
+__device__ __forceinline__ double block_sum_partials(const double *__restrict__ part, double *red) {
+  double s = 0.0;
+  for (int i = threadIdx.x; i < kRedBlocks; i += blockDim.x) s += part[i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int m = blockDim.x / 2; m > 0; m >>= 1) {
+    if ((int)threadIdx.x < m) red[threadIdx.x] += red[threadIdx.x + m];
+    __syncthreads();
+  }
+  const double t = red[0];
+  __syncthreads();
+  return t;
+}
+
+__device__ __forceinline__ void block_store_partial(double acc, double *red, double *partOut) {
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int m = blockDim.x / 2; m > 0; m >>= 1) {
+    if ((int)threadIdx.x < m) red[threadIdx.x] += red[threadIdx.x + m];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partOut[blockIdx.x] = red[0];
+}
+
+// One modified Gram-Schmidt column (gmres.c's ddot + daxpy pair) as a single
+// launch on kRedBlocks blocks: every block reduces the partials of
+// h_k = w.v_k in the same order, block 0 stores h_k, each block updates its
+// grid-stride share w -= h_k v_k and leaves its partial of the next product,
+// w.v_next (or w.w when v_next is null).  The grid partition is that of
+// dot_partial_kernel, so the values equal the separate dot/axpy sequence.
+__global__ void __launch_bounds__(kRedThreads)
+mgs_step_kernel(long long n, const double *__restrict__ partIn, double *hk, const double *__restrict__ vk,
+                const double *__restrict__ vnext, double *w, double *partOut) {
+  __shared__ double red[kRedThreads];
+  const double h = block_sum_partials(partIn, red);
+  if (blockIdx.x == 0 && threadIdx.x == 0) *hk = h;
+  const double a = -h;
+  double acc = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double wi = w[i] + a * vk[i];
+    w[i] = wi;
+    acc += wi * (vnext ? vnext[i] : wi);
+  }
+  block_store_partial(acc, red, partOut);
+}
+
+// h_i = sqrt(w.w) from the partials; v_i = w / h_i (w itself when h_i is 0)
+__global__ void __launch_bounds__(kRedThreads)
+mgs_norm_scale_kernel(long long n, const double *__restrict__ partIn, double *hi, const double *__restrict__ w,
+                      double *v) {
+  __shared__ double red[kRedThreads];
+  const double d = sqrt(block_sum_partials(partIn, red));
+  if (blockIdx.x == 0 && threadIdx.x == 0) *hi = d;
+  const double sc = (d > 0.0) ? 1.0 / d : 1.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    v[i] = (d > 0.0) ? w[i] * sc : w[i];
+}
+
 static bool dot_dev(Context &c, long long n, const double *x, const double *y, double *out, bool sq) {
   PrecondDev &p = *c.pc;
   dot_partial_kernel<<<kRedBlocks, kRedThreads, 0, c.stream>>>(n, x, y, p.d_part);
@@ -358,7 +484,7 @@ bool gmres_solve(Context &c, const double *b, double *x, int restrt, int maxit, 
     p.restart = restrt;
     if (!p.arena.alloc_n(&p.d_V, (size_t)n2 * (restrt + 1)) || !p.arena.alloc_n(&p.d_r, (size_t)n2) ||
         !p.arena.alloc_n(&p.d_av, (size_t)n2) || !p.arena.alloc_n(&p.d_w, (size_t)n2) ||
-        !p.arena.alloc_n(&p.d_h, (size_t)ldh + 1) || !p.arena.alloc_n(&p.d_part, (size_t)kRedBlocks + 2) ||
+        !p.arena.alloc_n(&p.d_h, (size_t)ldh + 1) || !p.arena.alloc_n(&p.d_part, 2 * (size_t)kRedBlocks + 2) ||
         !p.arena.alloc_n(&p.d_y, (size_t)restrt + 1))
       return false;
   }
@@ -397,15 +523,20 @@ bool gmres_solve(Context &c, const double *b, double *x, int restrt, int maxit, 
       ++(*iters);
       if (!op_matvec(c, 1.0, p.d_V + (size_t)(i - 1) * n2, 0.0, p.d_av)) return false;
       if (!precond_apply(c, p.d_av, p.d_w)) return false;
-      // modified Gram-Schmidt: h[k] = w.v_k; w -= h[k] v_k
+      // modified Gram-Schmidt: h[k] = w.v_k; w -= h[k] v_k, one launch per
+      // column with the partial sums ping-ponged between two buffers
+      double *partA = p.d_part, *partB = p.d_part + kRedBlocks;
+      dot_partial_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(n2, p.d_w, p.d_V, partA);
       for (int k = 0; k < i; k++) {
-        if (!dot_dev(c, n2, p.d_w, p.d_V + (size_t)k * n2, p.d_h + k, false)) return false;
-        axpy_neg_dev_kernel<<<kRedBlocks * 4, 256, 0, s>>>(n2, p.d_h + k, p.d_V + (size_t)k * n2, p.d_w);
-        c.launches += 1;
+        const double *vnext = (k + 1 < i) ? p.d_V + (size_t)(k + 1) * n2 : nullptr;
+        mgs_step_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(n2, partA, p.d_h + k, p.d_V + (size_t)k * n2, vnext,
+                                                           p.d_w, partB);
+        std::swap(partA, partB);
       }
-      if (!dot_dev(c, n2, p.d_w, p.d_w, p.d_h + i, true)) return false;
-      scale_copy_dev_kernel<<<kRedBlocks * 4, 256, 0, s>>>(n2, p.d_h + i, p.d_w, p.d_V + (size_t)i * n2);
-      c.launches += 1;
+      mgs_norm_scale_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(n2, partA, p.d_h + i, p.d_w,
+                                                               p.d_V + (size_t)i * n2);
+      c.launches += i + 2;
+      FB_CUDA(cudaGetLastError());
       FB_CUDA(cudaMemcpyAsync(hcol.data(), p.d_h, (i + 1) * sizeof(double), cudaMemcpyDeviceToHost, s));
       FB_CUDA(cudaStreamSynchronize(s));
       double *hc = &H[(size_t)(i - 1) * ldh];
