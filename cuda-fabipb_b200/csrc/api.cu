@@ -92,6 +92,7 @@ bool init_quad_tables() {
 Context::~Context() {
   free_charges(*this);
   free_precond(*this);
+  free_adjoint(*this);
   arena.release();
   if (ownStream && stream) cudaStreamDestroy(stream);
 }
@@ -133,10 +134,10 @@ bool setup_geometry(Context &c, const double *vtx, const double *nrm, const doub
 }
 
 // pot = beta*pot + alpha*K_part*sgm
-bool op_apply(Context &c, int part, double alpha, const double *sgm, double beta, double *pot) {
+bool op_apply(Context &c, int part, double alpha, const double *sgm, double beta, double *pot, bool adjoint) {
   if (part & FABIPB_B200_FAR) {
-    if (!launch_far_upward(c, sgm)) return false;
-    if (!launch_l2p(c, alpha, beta, pot, nullptr, 0.0, 0.0)) return false;
+    if (!launch_far_upward(c, sgm, adjoint)) return false;
+    if (!launch_l2p(c, alpha, beta, pot, nullptr, 0.0, 0.0, adjoint)) return false;
   } else if (beta != 1.0) {
     // scale pot by beta through L2P with alpha = 0 would still read lec;
     // a plain scale is cheaper
@@ -148,18 +149,18 @@ bool op_apply(Context &c, int part, double alpha, const double *sgm, double beta
     }
   }
   if (part & FABIPB_B200_NEAR) {
-    if (!launch_near(c, sgm, alpha, pot)) return false;
+    if (!launch_near(c, sgm, alpha, pot, adjoint)) return false;
   }
   return true;
 }
 
-// y = alpha*(D - K)x + beta*y, D = diag(s1*A, s2*A) (MtVmain)
-bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y) {
+// y = alpha*(D - K)x + beta*y, D = diag(s1*A, s2*A) (MtVmain); adjoint: (D - K^T)
+bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y, bool adjoint) {
   double s1 = (1.0 + c.epsilon) / 2.0 * alpha;
   double s2 = (1.0 + 1.0 / c.epsilon) / 2.0 * alpha;
-  if (!launch_far_upward(c, x)) return false;
-  if (!launch_l2p(c, -alpha, beta, y, x, s1, s2)) return false;
-  if (!launch_near(c, x, -alpha, y)) return false;
+  if (!launch_far_upward(c, x, adjoint)) return false;
+  if (!launch_l2p(c, -alpha, beta, y, x, s1, s2, adjoint)) return false;
+  if (!launch_near(c, x, -alpha, y, adjoint)) return false;
   return true;
 }
 
@@ -401,6 +402,27 @@ int fabipb_b200_matvec(void *ctx, double alpha, const double *x, double beta, do
   });
 }
 
+int fabipb_b200_apply_adjoint(void *ctx, int part, double alpha, const double *lam, double beta, double *out,
+                              int on_device) {
+  if (!valid_ctx(ctx) || lam == nullptr || out == nullptr) return 0;
+  Context *c = (Context *)ctx;
+  if (part < 1 || part > 3) {
+    set_error("fabipb_b200_apply_adjoint: part must be NEAR, FAR or ALL");
+    return 0;
+  }
+  return with_vectors(c, lam, out, beta != 0.0, on_device, [&](const double *x, double *y) {
+    return op_apply(*c, part, alpha, x, beta, y, true);
+  });
+}
+
+int fabipb_b200_matvec_adjoint(void *ctx, double alpha, const double *x, double beta, double *y, int on_device) {
+  if (!valid_ctx(ctx) || x == nullptr || y == nullptr) return 0;
+  Context *c = (Context *)ctx;
+  return with_vectors(c, x, y, beta != 0.0, on_device, [&](const double *xd, double *yd) {
+    return op_matvec(*c, alpha, xd, beta, yd, true);
+  });
+}
+
 }  // extern "C"
 
 extern "C" {
@@ -412,6 +434,7 @@ int fabipb_b200_set_charges(void *ctx, int m, const double *pos, const double *q
   }
   Context *c = (Context *)ctx;
   cudaSetDevice(c->device);
+  free_adjoint(*c);   // a forward solve of the old charges is void
   if (!setup_charges(*c, m, pos, q)) return 0;
   if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
     set_error("charge setup failed: %s", cudaGetErrorString(cudaGetLastError()));

@@ -13,6 +13,7 @@ namespace fb {
 
 struct ChargeTreeDev;
 struct PrecondDev;
+struct AdjointDev;
 struct GraphCache;
 
 struct Context {
@@ -43,6 +44,7 @@ struct Context {
   long long nSpecial = 0;
   int *d_spOff = nullptr, *d_spSrc = nullptr;  // CSR by destination panel
   double4 *d_spK = nullptr;                    // exact minus one-point coefficient
+  double4 *d_spKT = nullptr;                   // the same for the transposed operator (built on first use)
 
   // ---- FMM ----------------------------------------------------------
   int P = 0, NM = 0;                       // max order, nmom(max order)
@@ -63,6 +65,10 @@ struct Context {
   int nConvList = 0;                           // entries of d_lst
   long long nM2LPairs = 0;
   double2 *d_m2lTens = nullptr;                // [nMom][pairs] (D G0, D Gk) per M2L pair
+  // transposed M2L lists (adjoint operator, built on first use)
+  bool m2lAdjReady = false;
+  std::vector<int> h_m2lDstT;
+  int *d_m2lDstT = nullptr, *d_m2lOffT = nullptr, *d_m2lSrcT = nullptr, *d_m2lPairT = nullptr;
 
   // ---- scratch vectors for host-pointer calls ------------------------
   double *d_x = nullptr, *d_y = nullptr, *d_w = nullptr;
@@ -77,6 +83,7 @@ struct Context {
 
   // ---- preconditioner and GMRES ---------------------------------------
   PrecondDev *pc = nullptr;
+  AdjointDev *adj = nullptr;               // forward/backward state (gradients)
   GraphCache *graphs = nullptr;
 
   double setupSeconds = 0.0;
@@ -92,28 +99,33 @@ bool setup_charges(Context &c, int m, const double *pos, const double *q);
 
 // device operators on device vectors (stream-ordered, no synchronisation)
 // near:  out += coef * K_near * sgm
-bool launch_near(Context &c, const double *sgm, double coef, double *out);
+bool launch_near(Context &c, const double *sgm, double coef, double *out, bool adjoint = false);
 // upward pass + interaction + downward pass: leaves local expansions in d_lec
-bool launch_far_upward(Context &c, const double *sgm);
+// (adjoint: the transposed far operator's upward half, see fmm.cu)
+bool launch_far_upward(Context &c, const double *sgm, bool adjoint = false);
 // L2P: out = beta*out + alpha*far + diag*(area .* x) (diag part optional)
 bool launch_l2p(Context &c, double alpha, double beta, double *out, const double *diagX,
-                double s1, double s2);
-bool launch_m2l_only(Context &c);
+                double s1, double s2, bool adjoint = false);
+bool launch_m2l_only(Context &c, bool adjoint = false);
 bool launch_rhs(Context &c, int useTree, double *rhs);
 bool launch_energy(Context &c, const double *sgm, double *raw_host);
 bool precond_setup(Context &c, int mode);
-bool precond_apply(Context &c, const double *b, double *x);
+// (adjoint: the transposed preconditioner and operator, for A^T lambda = e)
+bool precond_apply(Context &c, const double *b, double *x, bool adjoint = false);
 bool gmres_solve(Context &c, const double *b, double *x, int restart, int maxit, double tol,
-                 int *iters, double *resid, int *info);
+                 int *iters, double *resid, int *info, bool adjoint = false);
 void free_charges(Context &c);
 void free_precond(Context &c);
+void free_adjoint(Context &c);
+bool dot_to_host(Context &c, long long n, const double *x, const double *y, double *out);
 
 // create a context (dense = every leaf pair is near: the direct operator)
 int create_context(const fabipb_b200_params *p, int n, const double *vtx, const double *nrm, const double *area,
                    bool dense, void **out);
 
 // composite operators (device vectors)
-bool op_apply(Context &c, int part, double alpha, const double *sgm, double beta, double *pot);
-bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y);
+// (adjoint: the transposed operator K^T, and (D - K)^T)
+bool op_apply(Context &c, int part, double alpha, const double *sgm, double beta, double *pot, bool adjoint = false);
+bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y, bool adjoint = false);
 
 }  // namespace fb

@@ -7,4 +7,5 @@
 #include "solver.cu"
 #include "api.cu"
 #include "abi.cu"
+#include "adjoint.cu"
 #include "noalloc.cu"

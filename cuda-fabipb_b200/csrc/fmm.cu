@@ -232,10 +232,12 @@ __global__ void leaf_moments_kernel(int n, int order, const double *__restrict__
 // ------------------------------------------------------------------------
 
 // Q2M: one block per leaf, warp w sums rows m = w, w+8, ... over the leaf panels
+// swap = 1 reads the two halves of sgm exchanged (the adjoint of L2P:
+// momPot <- Q1 . second half, momDpdn <- Q0 . first half).
 __global__ void q2m_kernel(int nLeaves, int n, int NMleaf, int NM, const int *__restrict__ leafStart,
                            const int *__restrict__ leafCount, const int *__restrict__ leafFmm,
                            const double *__restrict__ Q0, const double *__restrict__ Q1,
-                           const double *__restrict__ sgm, double *momPot, double *momDpdn) {
+                           const double *__restrict__ sgm, int swap, double *momPot, double *momDpdn) {
   int L = blockIdx.x;
   if (L >= nLeaves) return;
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
@@ -243,8 +245,8 @@ __global__ void q2m_kernel(int nLeaves, int n, int NMleaf, int NM, const int *__
   for (int m = warp; m < NMleaf; m += nw) {
     double sp = 0.0, sd = 0.0;
     for (int j = lane; j < cnt; j += 32) {
-      sp += Q1[(size_t)m * n + st + j] * sgm[st + j];
-      sd += Q0[(size_t)m * n + st + j] * sgm[n + st + j];
+      sp += Q1[(size_t)m * n + st + j] * sgm[(swap ? n : 0) + st + j];
+      sd += Q0[(size_t)m * n + st + j] * sgm[(swap ? 0 : n) + st + j];
     }
     for (int o = 16; o > 0; o >>= 1) {
       sp += __shfl_xor_sync(0xffffffffu, sp, o);
@@ -356,13 +358,22 @@ struct M2LShape {
   static constexpr size_t bytes = W * warpBytes;
 };
 
-template <int PM>
+//
+// ADJ: the transposed interaction.  The lists are those of the transposed
+// pairs (the destination is the forward source; pairIdx gives the forward
+// pair whose tensor D(x_f - x_s) is used), momPot/momDpdn carry the adjoint
+// local expansions (g34, g12) of the forward destinations, the sign goes with
+// the output index, and the outputs are the adjoint moments
+//   lec1 (pot)  += sgn (eps S2 - S1 - S3 + S4),
+//   lec2 (dpdn) += sgn (S1 + S3 - S2 - S4/eps),
+// with S1 = sum g12 G0, S2 = sum g12 Gk, S3 = sum g34 G0, S4 = sum g34 Gk.
+template <int PM, bool ADJ>
 __global__ void __launch_bounds__(M2LShape<PM>::W * 32)
 m2l_kernel(int nDst, const int *__restrict__ dstList, const int *__restrict__ m2lOff,
-           const int *__restrict__ m2lSrc, const int *__restrict__ ordOfCube, const int *__restrict__ lstOff,
-           const int *__restrict__ lst, long long nPairs, const double2 *__restrict__ tens, int NM, double eps,
-           const double *__restrict__ momPot, const double *__restrict__ momDpdn, double *lec1, double *lec2,
-           double *lec3, double *lec4) {
+           const int *__restrict__ m2lSrc, const int *__restrict__ pairIdx, const int *__restrict__ ordOfCube,
+           const int *__restrict__ lstOff, const int *__restrict__ lst, long long nPairs,
+           const double2 *__restrict__ tens, int NM, double eps, const double *__restrict__ momPot,
+           const double *__restrict__ momDpdn, double *lec1, double *lec2, double *lec3, double *lec4) {
   typedef M2LShape<PM> Sh;
   constexpr int NMP = Sh::NMP;
   extern __shared__ double2 m2lSmem[];
@@ -382,12 +393,12 @@ m2l_kernel(int nDst, const int *__restrict__ dstList, const int *__restrict__ m2
     const bool live = k < o1;
     const int s = live ? m2lSrc[k] : 0;
     for (int e = 0; e < nm; e++) {
-      const double sg = c_sgn3[e];
+      const double sg = ADJ ? 1.0 : c_sgn3[e];
       sC[e * 32 + lane] = live ? make_double2(sg * momPot[(size_t)s * NM + e], sg * momDpdn[(size_t)s * NM + e])
                                : make_double2(0.0, 0.0);
     }
     __syncwarp();
-    const double2 *T = tens + (live ? k : o0);
+    const double2 *T = tens + (ADJ ? pairIdx[live ? k : o0] : (live ? k : o0));
     for (int al = 0; al < nm; al++) {
       const int q0 = __ldg(lstOff + al), q1 = __ldg(lstOff + al + 1);
       const int lim = order - c_mi[al].w;
@@ -399,11 +410,18 @@ m2l_kernel(int nDst, const int *__restrict__ dstList, const int *__restrict__ m2
         const int ib = ent & 1023, ig = (ent >> 10) & 1023;
         const double2 d = T[(size_t)ig * nPairs];
         const double2 c = sC[ib * 32 + lane];
-        const double v1 = d.x - d.y;
-        l1 += c.y * v1;
-        l2 += c.x * (eps * d.y - d.x);
-        l3 += c.y * (d.x - d.y * ieps);
-        l4 -= c.x * v1;
+        if (ADJ) {   // raw sums S1..S4
+          l1 += c.y * d.x;
+          l2 += c.y * d.y;
+          l3 += c.x * d.x;
+          l4 += c.x * d.y;
+        } else {
+          const double v1 = d.x - d.y;
+          l1 += c.y * v1;
+          l2 += c.x * (eps * d.y - d.x);
+          l3 += c.y * (d.x - d.y * ieps);
+          l4 -= c.x * v1;
+        }
       }
       const double t = warp_sum4(l1, l2, l3, l4, lane);
       if ((lane & 7) == 0) sAcc[(lane >> 3) * NMP + al] += t;
@@ -412,10 +430,17 @@ m2l_kernel(int nDst, const int *__restrict__ dstList, const int *__restrict__ m2
   }
   for (int e = lane; e < nm; e += 32) {
     const size_t o = (size_t)f * NM + e;
-    lec1[o] += sAcc[e];
-    lec2[o] += sAcc[NMP + e];
-    lec3[o] += sAcc[2 * NMP + e];
-    lec4[o] += sAcc[3 * NMP + e];
+    if (ADJ) {
+      const double sg = c_sgn3[e];
+      const double S1 = sAcc[e], S2 = sAcc[NMP + e], S3 = sAcc[2 * NMP + e], S4 = sAcc[3 * NMP + e];
+      lec1[o] += sg * (eps * S2 - S1 - S3 + S4);
+      lec2[o] += sg * (S1 + S3 - S2 - S4 * ieps);
+    } else {
+      lec1[o] += sAcc[e];
+      lec2[o] += sAcc[NMP + e];
+      lec3[o] += sAcc[2 * NMP + e];
+      lec4[o] += sAcc[3 * NMP + e];
+    }
   }
 }
 
@@ -491,7 +516,7 @@ struct M2LSums {
 // One (alpha, beta) entry.  FULL: the cube's order is PM, every entry counts.
 // The four sums of a coefficient are reduced over the lanes (component v's
 // total lands in lane 8v) and added to the warp's shared sums sAcc[v][alpha].
-template <int PM, int Q, bool FULL>
+template <int PM, int Q, bool FULL, bool ADJ>
 __device__ __forceinline__ void m2l_step(M2LSums &S, const double2 *sC, const double2 (&T)[nmom_c(PM)], int lane,
                                          int order, double *sAcc) {
   constexpr M2LEntry E = m2l_entry<PM>(Q);
@@ -499,7 +524,7 @@ __device__ __forceinline__ void m2l_step(M2LSums &S, const double2 *sC, const do
   if (FULL || E.dsum <= order) {
     const double2 mo = sC[m2l_slot(E.ib, lane)];
     const double2 d = T[E.ig];
-    if ((E.dsum - E.dal) & 1) {
+    if ((ADJ ? E.dal : E.dsum - E.dal) & 1) {   // (-1)^|input|, or (-1)^|output| transposed
       S.s1 -= mo.y * d.x; S.s2 -= mo.y * d.y; S.s3 -= mo.x * d.x; S.s4 -= mo.x * d.y;
     } else {
       S.s1 += mo.y * d.x; S.s2 += mo.y * d.y; S.s3 += mo.x * d.x; S.s4 += mo.x * d.y;
@@ -511,16 +536,18 @@ __device__ __forceinline__ void m2l_step(M2LSums &S, const double2 *sC, const do
   }
 }
 
-template <int PM, bool FULL, int... Q>
+template <int PM, bool FULL, bool ADJ, int... Q>
 __device__ __forceinline__ void m2l_steps(std::integer_sequence<int, Q...>, M2LSums &S, const double2 *sC,
                                           const double2 (&T)[nmom_c(PM)], int lane, int order, double *sAcc) {
-  (m2l_step<PM, Q, FULL>(S, sC, T, lane, order, sAcc), ...);
+  (m2l_step<PM, Q, FULL, ADJ>(S, sC, T, lane, order, sAcc), ...);
 }
 
-template <int PM>
+// ADJ: the transposed interaction, as for m2l_kernel.
+template <int PM, bool ADJ>
 __global__ void __launch_bounds__(128, FB_M2L_MIN_BLOCKS)
 m2l_unrolled_kernel(int nDst, const int *__restrict__ dstList, const int *__restrict__ m2lOff,
-                    const int *__restrict__ m2lSrc, const int *__restrict__ ordOfCube, long long nPairs,
+                    const int *__restrict__ m2lSrc, const int *__restrict__ pairIdx,
+                    const int *__restrict__ ordOfCube, long long nPairs,
                     const double2 *__restrict__ tens, int NM, double eps, const double *__restrict__ momPot,
                     const double *__restrict__ momDpdn, double *lec1, double *lec2, double *lec3, double *lec4) {
   typedef M2LUnrolledShape<PM> Sh;
@@ -554,15 +581,15 @@ m2l_unrolled_kernel(int nDst, const int *__restrict__ dstList, const int *__rest
       }
     }
     double2 T[NMP];
-    const double2 *tp = tens + (live ? k : o0);
+    const double2 *tp = tens + (ADJ ? pairIdx[live ? k : o0] : (live ? k : o0));
 #pragma unroll
     for (int e = 0; e < NMP; e++) T[e] = tp[(size_t)e * nPairs];
     __syncwarp();
     M2LSums S{0.0, 0.0, 0.0, 0.0};
     if (order == PM)
-      m2l_steps<PM, true>(std::make_integer_sequence<int, m2l_entries<PM>()>{}, S, sC, T, lane, order, sAcc);
+      m2l_steps<PM, true, ADJ>(std::make_integer_sequence<int, m2l_entries<PM>()>{}, S, sC, T, lane, order, sAcc);
     else
-      m2l_steps<PM, false>(std::make_integer_sequence<int, m2l_entries<PM>()>{}, S, sC, T, lane, order, sAcc);
+      m2l_steps<PM, false, ADJ>(std::make_integer_sequence<int, m2l_entries<PM>()>{}, S, sC, T, lane, order, sAcc);
   }
   __syncwarp();
   const int nm = ((order + 1) * (order + 2) * (order + 3)) / 6;
@@ -570,10 +597,15 @@ m2l_unrolled_kernel(int nDst, const int *__restrict__ dstList, const int *__rest
   for (int e = lane; e < nm; e += 32) {
     const double S1 = sAcc[e], S2 = sAcc[NMP + e], S3 = sAcc[2 * NMP + e], S4 = sAcc[3 * NMP + e];
     const size_t o = (size_t)f * NM + e;
-    lec1[o] += S1 - S2;
-    lec2[o] += eps * S4 - S3;
-    lec3[o] += S1 - S2 * ieps;
-    lec4[o] += S4 - S3;
+    if (ADJ) {   // sign already folded in
+      lec1[o] += eps * S2 - S1 - S3 + S4;
+      lec2[o] += S1 + S3 - S2 - S4 * ieps;
+    } else {
+      lec1[o] += S1 - S2;
+      lec2[o] += eps * S4 - S3;
+      lec3[o] += S1 - S2 * ieps;
+      lec4[o] += S4 - S3;
+    }
   }
 }
 
@@ -623,7 +655,7 @@ __global__ void l2p_kernel(int n, int NMleaf, int NM, const int *__restrict__ le
                            const double *__restrict__ Q1, const double *__restrict__ lec1,
                            const double *__restrict__ lec2, const double *__restrict__ lec3,
                            const double *__restrict__ lec4, double alpha, double beta, const double *__restrict__ area,
-                           const double *__restrict__ diagX, double s1, double s2, double *out) {
+                           const double *__restrict__ diagX, double s1, double s2, int swap, double *out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const size_t f = (size_t)leafFmm[leafOfPanel[i]] * NM;
@@ -631,6 +663,11 @@ __global__ void l2p_kernel(int n, int NMleaf, int NM, const int *__restrict__ le
   for (int m = 0; m < NMleaf; m++) {
     a += Q0[(size_t)m * n + i] * (lec1[f + m] + lec2[f + m]);
     b += Q1[(size_t)m * n + i] * (lec3[f + m] + lec4[f + m]);
+  }
+  if (swap) {   // the adjoint of Q2M: the Q0 value belongs to the dpdn half
+    const double t = a;
+    a = b;
+    b = t;
   }
   double o0 = (beta == 0.0) ? 0.0 : beta * out[i];
   double o1 = (beta == 0.0) ? 0.0 : beta * out[n + i];
@@ -655,33 +692,53 @@ static void launch_leaf_moments(Context &c, int order) {
                                                                    c.d_leafOfPanel, c.d_leafCtr, c.d_Q0, c.d_Q1);
 }
 
+// Forward: moments (d_mom) -> local expansions (4 planes of d_lec).
+// Adjoint: adjoint locals g12, g34 (planes 0, 1 of d_lec) -> adjoint moments
+// (pot, dpdn: planes 0, 1 of d_mom) over the transposed pair lists.
 template <int PM>
-static void launch_m2l_t(Context &c) {
+static void launch_m2l_t(Context &c, bool adj) {
   const size_t plane = (size_t)c.pt.nFmm * c.NM;
-  static int attrDone[kMaxOrder + 1] = {0};
+  const int nDst = adj ? (int)c.h_m2lDstT.size() : (int)c.h_m2lDst.size();
+  const int *dst = adj ? c.d_m2lDstT : c.d_m2lDst, *off = adj ? c.d_m2lOffT : c.d_m2lOff;
+  const int *src = adj ? c.d_m2lSrcT : c.d_m2lSrc, *pairIdx = adj ? c.d_m2lPairT : nullptr;
+  const double *inPot = adj ? c.d_lec + plane : c.d_mom, *inDpdn = adj ? c.d_lec : c.d_mom + plane;
+  double *o1 = adj ? c.d_mom : c.d_lec, *o2 = adj ? c.d_mom + plane : c.d_lec + plane;
+  double *o3 = c.d_lec + 2 * plane, *o4 = c.d_lec + 3 * plane;
+  static int attrDone[2][kMaxOrder + 1] = {{0}};
   if (PM <= 4) {
-    typedef M2LUnrolledShape<PM <= 4 ? PM : 4> Sh;
-    if (!attrDone[PM]) {
-      cudaFuncSetAttribute(m2l_unrolled_kernel<PM <= 4 ? PM : 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)Sh::bytes);
-      attrDone[PM] = 1;
+    constexpr int PU = PM <= 4 ? PM : 4;
+    typedef M2LUnrolledShape<PU> Sh;
+    if (!attrDone[adj][PM]) {
+      cudaFuncSetAttribute(adj ? m2l_unrolled_kernel<PU, true> : m2l_unrolled_kernel<PU, false>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::bytes);
+      attrDone[adj][PM] = 1;
     }
-    const unsigned grid = ceil_div((long long)c.h_m2lDst.size(), Sh::W);
-    m2l_unrolled_kernel<PM <= 4 ? PM : 4><<<grid, Sh::W * 32, Sh::bytes, c.stream>>>(
-        (int)c.h_m2lDst.size(), c.d_m2lDst, c.d_m2lOff, c.d_m2lSrc, c.d_ordM2L, c.nM2LPairs, c.d_m2lTens, c.NM,
-        c.epsilon, c.d_mom, c.d_mom + plane, c.d_lec, c.d_lec + plane, c.d_lec + 2 * plane, c.d_lec + 3 * plane);
+    const unsigned grid = ceil_div((long long)nDst, Sh::W);
+    if (adj)
+      m2l_unrolled_kernel<PU, true><<<grid, Sh::W * 32, Sh::bytes, c.stream>>>(
+          nDst, dst, off, src, pairIdx, c.d_ordM2L, c.nM2LPairs, c.d_m2lTens, c.NM, c.epsilon, inPot, inDpdn, o1, o2,
+          o3, o4);
+    else
+      m2l_unrolled_kernel<PU, false><<<grid, Sh::W * 32, Sh::bytes, c.stream>>>(
+          nDst, dst, off, src, pairIdx, c.d_ordM2L, c.nM2LPairs, c.d_m2lTens, c.NM, c.epsilon, inPot, inDpdn, o1, o2,
+          o3, o4);
     return;
   }
   typedef M2LShape<PM> Sh;
-  if (!attrDone[PM]) {
-    cudaFuncSetAttribute(m2l_kernel<PM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::bytes);
-    attrDone[PM] = 1;
+  if (!attrDone[adj][PM]) {
+    cudaFuncSetAttribute(adj ? m2l_kernel<PM, true> : m2l_kernel<PM, false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::bytes);
+    attrDone[adj][PM] = 1;
   }
-  const unsigned grid = ceil_div((long long)c.h_m2lDst.size(), Sh::W);
-  m2l_kernel<PM><<<grid, Sh::W * 32, Sh::bytes, c.stream>>>(
-      (int)c.h_m2lDst.size(), c.d_m2lDst, c.d_m2lOff, c.d_m2lSrc, c.d_ordM2L, c.d_lstOff, c.d_lst, c.nM2LPairs,
-      c.d_m2lTens, c.NM, c.epsilon, c.d_mom, c.d_mom + plane, c.d_lec, c.d_lec + plane, c.d_lec + 2 * plane,
-      c.d_lec + 3 * plane);
+  const unsigned grid = ceil_div((long long)nDst, Sh::W);
+  if (adj)
+    m2l_kernel<PM, true><<<grid, Sh::W * 32, Sh::bytes, c.stream>>>(nDst, dst, off, src, pairIdx, c.d_ordM2L,
+                                                                    c.d_lstOff, c.d_lst, c.nM2LPairs, c.d_m2lTens,
+                                                                    c.NM, c.epsilon, inPot, inDpdn, o1, o2, o3, o4);
+  else
+    m2l_kernel<PM, false><<<grid, Sh::W * 32, Sh::bytes, c.stream>>>(nDst, dst, off, src, pairIdx, c.d_ordM2L,
+                                                                     c.d_lstOff, c.d_lst, c.nM2LPairs, c.d_m2lTens,
+                                                                     c.NM, c.epsilon, inPot, inDpdn, o1, o2, o3, o4);
 }
 
 template <int PM>
@@ -789,51 +846,93 @@ bool setup_fmm(Context &c) {
   return true;
 }
 
-bool launch_far_upward(Context &c, const double *sgm) {
+// Transposed M2L lists (built on the first adjoint apply): for every cube s
+// the forward pairs (f <- s) as entries (source f, forward pair index), f
+// ascending.
+static bool setup_m2l_adjoint(Context &c) {
+  if (c.m2lAdjReady) return true;
+  const PanelTree &pt = c.pt;
+  std::vector<int> offT(pt.nFmm + 1, 0), srcT(pt.m2lSrc.size()), pairT(pt.m2lSrc.size());
+  for (size_t k = 0; k < pt.m2lSrc.size(); k++) offT[pt.m2lSrc[k] + 1]++;
+  for (int f = 0; f < pt.nFmm; f++) offT[f + 1] += offT[f];
+  std::vector<int> cur(offT.begin(), offT.end() - 1);
+  for (int f = 0; f < pt.nFmm; f++)   // f ascending within each transposed list
+    for (int k = pt.m2lOff[f]; k < pt.m2lOff[f + 1]; k++) {
+      const int sidx = pt.m2lSrc[k];
+      srcT[cur[sidx]] = f;
+      pairT[cur[sidx]++] = k;
+    }
+  c.h_m2lDstT.clear();
+  for (int f = 0; f < pt.nFmm; f++)
+    if (offT[f + 1] > offT[f]) c.h_m2lDstT.push_back(f);
+  if (!c.arena.upload(&c.d_m2lOffT, offT, c.stream) || !c.arena.upload(&c.d_m2lSrcT, srcT, c.stream) ||
+      !c.arena.upload(&c.d_m2lPairT, pairT, c.stream) || !c.arena.upload(&c.d_m2lDstT, c.h_m2lDstT, c.stream))
+    return false;
+  c.m2lAdjReady = true;
+  return true;
+}
+
+// Forward: Q2M, M2M, M2L, L2L; the leaves' local expansions end in d_lec.
+// Adjoint (the transposed far operator, read right to left): L2P^T (Q2M with
+// the halves exchanged) -> g12, g34 in d_lec planes 0, 1; L2L^T, which is the
+// M2M shift; M2L^T into d_mom planes 0, 1 (adjoint moments pot, dpdn); M2M^T,
+// which is the L2L shift; launch_l2p(adjoint) then applies Q2M^T.
+bool launch_far_upward(Context &c, const double *sgm, bool adjoint) {
   const PanelTree &pt = c.pt;
   const int depth = pt.t.depth, height = pt.t.height;
   cudaStream_t s = c.stream;
   const size_t plane = (size_t)pt.nFmm * c.NM;
+  if (adjoint && !setup_m2l_adjoint(c)) return false;
   FB_CUDA(cudaMemsetAsync(c.d_mom, 0, 2 * plane * sizeof(double), s));
   FB_CUDA(cudaMemsetAsync(c.d_lec, 0, 4 * plane * sizeof(double), s));
   c.launches += 1 + 2 * (depth - height);
+  // upward arrays: moments (forward) or adjoint locals (adjoint)
+  double *up1 = adjoint ? c.d_lec + plane : c.d_mom, *up2 = adjoint ? c.d_lec : c.d_mom + plane;
   q2m_kernel<<<pt.nLeaves, 256, 0, s>>>(pt.nLeaves, c.n, c.NMleaf, c.NM, c.d_leafStart, c.d_leafCount, c.d_leafFmm,
-                                        c.d_Q0, c.d_Q1, sgm, c.d_mom, c.d_mom + plane);
+                                        c.d_Q0, c.d_Q1, sgm, adjoint ? 1 : 0, up1, up2);
   for (int lev = depth - 1; lev >= height; lev--) {
     int ordOut = pt.ordMom[lev], ordIn = pt.ordMom[lev + 1];
     int thr = std::max(32, ((nmom(ordOut) + 31) / 32) * 32);
     size_t shm = 3 * (size_t)nmom(ordOut) * sizeof(double);
     m2m_kernel<<<pt.fmmLevelCount[lev], thr, shm, s>>>(pt.fmmLevelStart[lev], pt.fmmLevelCount[lev], c.NM, ordOut,
                                                        ordIn, c.d_kidFirst, c.d_kidCount, c.d_cubeCtr, c.d_mOff,
-                                                       c.d_mLst, c.d_mom, c.d_mom + plane);
+                                                       c.d_mLst, up1, up2);
   }
-  if (!launch_m2l_only(c)) return false;
+  if (!launch_m2l_only(c, adjoint)) return false;
+  // downward arrays: 4 local planes (forward) or the 2 adjoint moment planes
+  // plus 2 scratch planes (adjoint)
+  double *d1 = adjoint ? c.d_mom : c.d_lec, *d2 = adjoint ? c.d_mom + plane : c.d_lec + plane;
   for (int lev = height; lev < depth; lev++) {
     int ordIn = pt.ordMom[lev], ordOut = pt.ordMom[lev + 1];
     int thr = std::max(32, ((nmom(ordOut) + 31) / 32) * 32);
     size_t shm = 5 * (size_t)nmom(ordIn) * sizeof(double);
     l2l_kernel<<<pt.fmmLevelCount[lev + 1], thr, shm, s>>>(
         pt.fmmLevelStart[lev + 1], pt.fmmLevelCount[lev + 1], c.NM, ordIn, ordOut, c.d_fmmParent, c.d_cubeCtr,
-        c.d_lstOff, c.d_lst, c.d_lec, c.d_lec + plane, c.d_lec + 2 * plane, c.d_lec + 3 * plane);
+        c.d_lstOff, c.d_lst, d1, d2, c.d_lec + 2 * plane, c.d_lec + 3 * plane);
   }
+  if (adjoint) FB_CUDA(cudaMemsetAsync(c.d_lec + 2 * plane, 0, 2 * plane * sizeof(double), s));
   FB_CUDA(cudaGetLastError());
   return true;
 }
 
-bool launch_m2l_only(Context &c) {
-  if (c.h_m2lDst.empty()) return true;
-  FB_DISPATCH_ORDER(c.P, launch_m2l_t, c);
+bool launch_m2l_only(Context &c, bool adjoint) {
+  if ((adjoint ? c.h_m2lDstT : c.h_m2lDst).empty()) return true;
+  FB_DISPATCH_ORDER(c.P, launch_m2l_t, c, adjoint);
   c.launches += 1;
   FB_CUDA(cudaGetLastError());
   return true;
 }
 
-bool launch_l2p(Context &c, double alpha, double beta, double *out, const double *diagX, double s1, double s2) {
+bool launch_l2p(Context &c, double alpha, double beta, double *out, const double *diagX, double s1, double s2,
+                bool adjoint) {
   const size_t plane = (size_t)c.pt.nFmm * c.NM;
   c.launches += 1;
+  // adjoint: Q0 . (adjoint dpdn moments + 0) -> dpdn half, Q1 . (adjoint pot moments + 0) -> pot half
+  const double *l1 = adjoint ? c.d_mom + plane : c.d_lec, *l2 = c.d_lec + (adjoint ? 2 : 1) * plane;
+  const double *l3 = adjoint ? c.d_mom : c.d_lec + 2 * plane, *l4 = c.d_lec + 3 * plane;
   l2p_kernel<<<ceil_div(c.n, 256), 256, 0, c.stream>>>(c.n, c.NMleaf, c.NM, c.d_leafOfPanel, c.d_leafFmm, c.d_Q0,
-                                                       c.d_Q1, c.d_lec, c.d_lec + plane, c.d_lec + 2 * plane,
-                                                       c.d_lec + 3 * plane, alpha, beta, c.d_area, diagX, s1, s2, out);
+                                                       c.d_Q1, l1, l2, l3, l4, alpha, beta, c.d_area, diagX, s1, s2,
+                                                       adjoint ? 1 : 0, out);
   FB_CUDA(cudaGetLastError());
   return true;
 }

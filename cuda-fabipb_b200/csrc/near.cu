@@ -102,7 +102,14 @@ constexpr int kNearWarps = 4;
 // One disjoint pair, one-point rule: the four KER4 kernels (src/kernel.c:109-147)
 // at d = target - source, times the source weights a.w = A*sigma_dpdn and
 // b.w = A*sigma_pot (the 4 pi and the target area are applied once at the end).
-template <typename T, typename V>
+//
+// ADJ: the transposed pair block.  With d = target - source, swapping the
+// roles of the two panels gives K0 and K3 unchanged, K1(s,t) = -t2 (eps c - 1)
+// and K2(s,t) = -t1 (c/eps - 1), so
+//   out_pot  += y3 * a.w - t2 (eps c - 1) * b.w
+//   out_dpdn += y0 * b.w - t1 (c/eps - 1) * a.w
+// with a.w = A*lambda_dpdn and b.w = A*lambda_pot of the source panel.
+template <bool ADJ, typename T, typename V>
 __device__ __forceinline__ void near_pair(const V a, const V b, T tx, T ty, T tz, const V tn, T kappa, T kexp, T eps,
                                           T ieps, T kap2, T &acc0, T &acc1) {
   const T dx = tx - a.x, dy = ty - a.y, dz = tz - a.z;
@@ -124,15 +131,20 @@ __device__ __forceinline__ void near_pair(const V a, const V b, T tx, T ty, T tz
   const T y2 = t2 * (c * ieps - (T)1);           // dGk/dn_x / eps - dG0/dn_x
   const T dd = (ip0 * g - (T)3 * u) * g2;        // d2 G0 / dn_x dn_y
   const T y3 = dd * (c - (T)1) - kap2 * e * u;
-  acc0 += y0 * a.w + y1 * b.w;
-  acc1 += y2 * a.w + y3 * b.w;
+  if (ADJ) {
+    acc0 += y3 * a.w - t2 * (eps * c - (T)1) * b.w;
+    acc1 += y0 * b.w - t1 * (c * ieps - (T)1) * a.w;
+  } else {
+    acc0 += y0 * a.w + y1 * b.w;
+    acc1 += y2 * a.w + y3 * b.w;
+  }
 }
 
 // One warp per task (leaf L, group of up to 32 target panels).  A full group
 // puts one target on each lane; a partial group of mt targets gives each
 // target k = 32/mt lanes, which take every k-th source of a tile, and their
 // partial sums are added at the end, so short groups keep most lanes busy.
-template <typename T>
+template <typename T, bool ADJ>
 __global__ void __launch_bounds__(kNearWarps * 32, sizeof(T) == 4 ? FB_NEAR_MIN_BLOCKS : 1)
 near_apply_kernel(int nWork, const int2 *__restrict__ work, const int *__restrict__ leafStart,
                   const int *__restrict__ leafCount, const int *__restrict__ nearOff,
@@ -179,11 +191,11 @@ near_apply_kernel(int nWork, const int2 *__restrict__ work, const int *__restric
       if (k == 1) {   // warp-uniform: a full group, unit stride
 #pragma unroll 4
         for (int jj = 0; jj < m; jj++)
-          near_pair(sA[warp][jj], sB[warp][jj], tx, ty, tz, tn, kappa, kexp, eps, ieps, kap2, acc0, acc1);
+          near_pair<ADJ>(sA[warp][jj], sB[warp][jj], tx, ty, tz, tn, kappa, kexp, eps, ieps, kap2, acc0, acc1);
       } else {
 #pragma unroll 4
         for (int jj = sub; jj < m; jj += k)
-          near_pair(sA[warp][jj], sB[warp][jj], tx, ty, tz, tn, kappa, kexp, eps, ieps, kap2, acc0, acc1);
+          near_pair<ADJ>(sA[warp][jj], sB[warp][jj], tx, ty, tz, tn, kappa, kexp, eps, ieps, kap2, acc0, acc1);
       }
       __syncwarp();
     }
@@ -418,28 +430,69 @@ bool setup_near(Context &c) {
   return true;
 }
 
-bool launch_near(Context &c, const double *sgm, double coef, double *out) {
+template <typename T, bool ADJ>
+static void launch_near_t(Context &c, const double *sgm, double coef, double *out) {
+  typedef typename Vec4<T>::t V;
   const int n = c.n;
   cudaStream_t s = c.stream;
   const double kap = c.prm.kappa, eps = c.epsilon;
-  unsigned grid = ceil_div(c.nWork, kNearWarps);
+  const unsigned grid = ceil_div(c.nWork, kNearWarps);
+  const double kexp = sizeof(T) == 4 ? -kap * 1.4426950408889634 : -kap;   // float: exp2 argument
+  near_pack_kernel<T><<<ceil_div(n, 256), 256, 0, s>>>(n, (const V *)c.d_tgtP, (const V *)c.d_tgtN, c.d_area, sgm,
+                                                       (V *)c.d_srcA, (V *)c.d_srcB);
+  near_apply_kernel<T, ADJ><<<grid, kNearWarps * 32, 0, s>>>(
+      c.nWork, c.d_work, c.d_leafStart, c.d_leafCount, c.d_nearOff, c.d_nearSrc, c.d_leafCtr, (const V *)c.d_tgtP,
+      (const V *)c.d_tgtN, (const V *)c.d_srcA, (const V *)c.d_srcB, c.d_spOff, c.d_spSrc,
+      ADJ ? c.d_spKT : c.d_spK, sgm, c.d_area, n, (T)kap, (T)kexp, (T)eps, (T)(1.0 / eps), (T)(kap * kap), coef, out);
+}
+
+// Transposed special-pair table: entry (X, Y) of row X holds the correction
+// of the pair (Y, X) arranged for the ADJ epilogue
+// (out_pot += dK3(Y,X) l_dpdn + dK1(Y,X) l_pot, out_dpdn += dK2(Y,X) l_dpdn + dK0(Y,X) l_pot).
+__global__ void special_transpose_kernel(long long nSp, const long long *__restrict__ mate, const double4 *__restrict__ spK,
+                                         double4 *spKT) {
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nSp) return;
+  const double4 d = spK[mate[e]];
+  spKT[e] = make_double4(d.w, d.y, d.z, d.x);
+}
+
+static bool setup_near_adjoint(Context &c) {
+  if (c.d_spKT) return true;
+  // the special-pair set is symmetric (shared vertex, near leaf pairs): find
+  // for every entry (X, Y) the entry (Y, X)
+  const int n = c.n;
+  std::vector<int> spOff(n + 1), spSrc((size_t)c.nSpecial);
+  FB_CUDA(cudaMemcpyAsync(spOff.data(), c.d_spOff, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  if (c.nSpecial > 0)
+    FB_CUDA(cudaMemcpyAsync(spSrc.data(), c.d_spSrc, c.nSpecial * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  FB_CUDA(cudaStreamSynchronize(c.stream));
+  std::vector<long long> mate((size_t)c.nSpecial);
+  for (int X = 0; X < n; X++)
+    for (int e = spOff[X]; e < spOff[X + 1]; e++) {
+      const int Y = spSrc[e];
+      const int *b = spSrc.data() + spOff[Y], *en = spSrc.data() + spOff[Y + 1];
+      const int *hit = std::find(b, en, X);
+      FB_CHECK(hit != en, "special pair (%d,%d) has no mirror entry", X, Y);
+      mate[e] = (long long)(hit - spSrc.data());
+    }
+  long long *d_mate = nullptr;
+  if (!c.arena.upload(&d_mate, mate, c.stream)) return false;
+  if (!c.arena.alloc_n(&c.d_spKT, (size_t)std::max<long long>(c.nSpecial, 1))) return false;
+  if (c.nSpecial > 0)
+    special_transpose_kernel<<<ceil_div(c.nSpecial, 256), 256, 0, c.stream>>>(c.nSpecial, d_mate, c.d_spK, c.d_spKT);
+  FB_CUDA(cudaGetLastError());
+  return true;
+}
+
+bool launch_near(Context &c, const double *sgm, double coef, double *out, bool adjoint) {
+  if (adjoint && !setup_near_adjoint(c)) return false;
   if (c.mixed) {
-    near_pack_kernel<float><<<ceil_div(n, 256), 256, 0, s>>>(n, (const float4 *)c.d_tgtP, (const float4 *)c.d_tgtN,
-                                                             c.d_area, sgm, (float4 *)c.d_srcA, (float4 *)c.d_srcB);
-    near_apply_kernel<float><<<grid, kNearWarps * 32, 0, s>>>(
-        c.nWork, c.d_work, c.d_leafStart, c.d_leafCount, c.d_nearOff, c.d_nearSrc, c.d_leafCtr,
-        (const float4 *)c.d_tgtP, (const float4 *)c.d_tgtN, (const float4 *)c.d_srcA, (const float4 *)c.d_srcB,
-        c.d_spOff, c.d_spSrc, c.d_spK, sgm, c.d_area, n, (float)kap, (float)(-kap * 1.4426950408889634),
-        (float)eps, (float)(1.0 / eps), (float)(kap * kap), coef, out);
+    if (adjoint) launch_near_t<float, true>(c, sgm, coef, out);
+    else launch_near_t<float, false>(c, sgm, coef, out);
   } else {
-    near_pack_kernel<double><<<ceil_div(n, 256), 256, 0, s>>>(n, (const double4 *)c.d_tgtP,
-                                                              (const double4 *)c.d_tgtN, c.d_area, sgm,
-                                                              (double4 *)c.d_srcA, (double4 *)c.d_srcB);
-    near_apply_kernel<double><<<grid, kNearWarps * 32, 0, s>>>(
-        c.nWork, c.d_work, c.d_leafStart, c.d_leafCount, c.d_nearOff, c.d_nearSrc, c.d_leafCtr,
-        (const double4 *)c.d_tgtP, (const double4 *)c.d_tgtN, (const double4 *)c.d_srcA,
-        (const double4 *)c.d_srcB, c.d_spOff, c.d_spSrc, c.d_spK, sgm, c.d_area, n, kap, -kap, eps, 1.0 / eps,
-        kap * kap, coef, out);
+    if (adjoint) launch_near_t<double, true>(c, sgm, coef, out);
+    else launch_near_t<double, false>(c, sgm, coef, out);
   }
   c.launches += 2;
   FB_CUDA(cudaGetLastError());

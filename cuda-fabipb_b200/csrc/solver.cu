@@ -150,6 +150,30 @@ pc_apply_kernel(int n, const int2 *__restrict__ tiles, const int *__restrict__ b
   }
 }
 
+// Transposed block-diagonal apply (adjoint solves): output c of a block is
+// column c of its inverse dotted with the block's input, one warp per output,
+// lanes over the (contiguous) column; tiles as for pc_apply_kernel.
+__global__ void __launch_bounds__(kPcRows * kPcSplit)
+pc_apply_t_kernel(int n, const int2 *__restrict__ tiles, const int *__restrict__ bStart, const int *__restrict__ bSize,
+                  const long long *__restrict__ bOff, const double *__restrict__ inv, const double *__restrict__ rhs,
+                  double *x) {
+  const int2 tl = tiles[blockIdx.x];
+  const int b = tl.x, c0 = tl.y;
+  const int hm = bSize[b], st = bStart[b], M = 2 * hm;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const double *Ib = inv + bOff[b];
+  for (int c = c0 + warp; c < min(M, c0 + kPcRows); c += nw) {
+    const double *col = Ib + (size_t)c * M;
+    double y = 0.0;
+    for (int r = lane; r < M; r += 32) y += col[r] * ((r < hm) ? rhs[st + r] : rhs[n + st + r - hm]);
+    for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
+    if (lane == 0) {
+      if (c < hm) x[st + c] = y;
+      else x[n + st + c - hm] = y;
+    }
+  }
+}
+
 __global__ void pc_diag_kernel(int n, const double *__restrict__ area, double s1, double s2,
                                const double *__restrict__ b, double *x) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -270,10 +294,13 @@ bool precond_setup(Context &c, int mode) {
   return true;
 }
 
-bool precond_apply(Context &c, const double *b, double *x) {
+bool precond_apply(Context &c, const double *b, double *x, bool adjoint) {
   FB_CHECK(c.pc != nullptr, "preconditioner not set up");
   PrecondDev &p = *c.pc;
-  if (p.mode == 2) {
+  if (p.mode == 2 && adjoint) {
+    pc_apply_t_kernel<<<p.nTiles, kPcRows * kPcSplit, 0, c.stream>>>(c.n, p.d_tiles, p.d_start, p.d_size, p.d_off,
+                                                                    p.d_inv, b, x);
+  } else if (p.mode == 2) {
     pc_apply_kernel<double><<<p.nTiles, kPcRows * kPcSplit, 0, c.stream>>>(c.n, p.d_tiles, p.d_start, p.d_size,
                                                                            p.d_off, p.d_inv, b, x);
   } else if (p.mode == 3) {
@@ -423,6 +450,18 @@ static bool dot_dev(Context &c, long long n, const double *x, const double *y, d
   return true;
 }
 
+// x . y to the host (fixed-order reduction); needs a preconditioner record
+// for its scratch
+bool dot_to_host(Context &c, long long n, const double *x, const double *y, double *out) {
+  FB_CHECK(c.pc != nullptr, "dot_to_host without a preconditioner record");
+  PrecondDev &p = *c.pc;
+  if (!p.d_part && !p.arena.alloc_n(&p.d_part, 2 * (size_t)kRedBlocks + 2)) return false;
+  if (!dot_dev(c, n, x, y, p.d_part + kRedBlocks, false)) return false;
+  FB_CUDA(cudaMemcpyAsync(out, p.d_part + kRedBlocks, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
+  FB_CUDA(cudaStreamSynchronize(c.stream));
+  return true;
+}
+
 static bool nrm2_host(Context &c, long long n, const double *x, double *out) {
   if (!dot_dev(c, n, x, x, c.pc->d_part + kRedBlocks, true)) return false;
   FB_CUDA(cudaMemcpyAsync(out, c.pc->d_part + kRedBlocks, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
@@ -474,7 +513,7 @@ static bool gmres_update_dev(Context &c, int it, std::vector<double> &H, int ldh
 }
 
 bool gmres_solve(Context &c, const double *b, double *x, int restrt, int maxit, double tol, int *iters, double *resid,
-                 int *info) {
+                 int *info, bool adjoint) {
   FB_CHECK(c.pc != nullptr, "call fabipb_b200_precond_setup before solving (mode -1 for none)");
   PrecondDev &p = *c.pc;
   const long long n2 = 2LL * c.n;
@@ -498,9 +537,9 @@ bool gmres_solve(Context &c, const double *b, double *x, int restrt, int maxit, 
   FB_CUDA(cudaMemcpyAsync(p.d_av, b, n2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
   if (!nrm2_host(c, n2, x, &xn)) return false;
   if (xn != 0.0) {
-    if (!op_matvec(c, -1.0, x, 1.0, p.d_av)) return false;
+    if (!op_matvec(c, -1.0, x, 1.0, p.d_av, adjoint)) return false;
   }
-  if (!precond_apply(c, p.d_av, p.d_r)) return false;
+  if (!precond_apply(c, p.d_av, p.d_r, adjoint)) return false;
   if (!nrm2_host(c, n2, b, &bnrm2)) return false;
   if (bnrm2 == 0.0) bnrm2 = 1.0;
   if (!nrm2_host(c, n2, p.d_r, &rnorm)) return false;
@@ -521,8 +560,8 @@ bool gmres_solve(Context &c, const double *b, double *x, int restrt, int maxit, 
     for (;;) {
       ++i;
       ++(*iters);
-      if (!op_matvec(c, 1.0, p.d_V + (size_t)(i - 1) * n2, 0.0, p.d_av)) return false;
-      if (!precond_apply(c, p.d_av, p.d_w)) return false;
+      if (!op_matvec(c, 1.0, p.d_V + (size_t)(i - 1) * n2, 0.0, p.d_av, adjoint)) return false;
+      if (!precond_apply(c, p.d_av, p.d_w, adjoint)) return false;
       // modified Gram-Schmidt: h[k] = w.v_k; w -= h[k] v_k, one launch per
       // column with the partial sums ping-ponged between two buffers
       double *partA = p.d_part, *partB = p.d_part + kRedBlocks;
@@ -552,8 +591,8 @@ bool gmres_solve(Context &c, const double *b, double *x, int restrt, int maxit, 
     }
     if (!gmres_update_dev(c, i, H, ldh, sv, x)) return false;
     FB_CUDA(cudaMemcpyAsync(p.d_av, b, n2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    if (!op_matvec(c, -1.0, x, 1.0, p.d_av)) return false;
-    if (!precond_apply(c, p.d_av, p.d_r)) return false;
+    if (!op_matvec(c, -1.0, x, 1.0, p.d_av, adjoint)) return false;
+    if (!precond_apply(c, p.d_av, p.d_r, adjoint)) return false;
     if (!nrm2_host(c, n2, p.d_r, &sv[i])) return false;
     *resid = sv[i] / bnrm2;
     if (*resid <= tol) return true;

@@ -63,6 +63,11 @@ def load():
     L.fabipb_b200_cube_data.argtypes = [vp, vp, vp]
     L.fabipb_b200_apply.argtypes = [vp, C.c_int, C.c_double, vp, C.c_double, vp, C.c_int]
     L.fabipb_b200_matvec.argtypes = [vp, C.c_double, vp, C.c_double, vp, C.c_int]
+    L.fabipb_b200_energy_weights.argtypes = [vp, vp, C.c_int]
+    L.fabipb_b200_forward.argtypes = [vp, C.c_int, C.c_int, C.c_double, vp, vp, vp, vp]
+    L.fabipb_b200_backward.argtypes = [vp, C.c_double, C.c_int, C.c_int, C.c_double, vp, vp, vp, vp, vp, C.c_int]
+    L.fabipb_b200_apply_adjoint.argtypes = [vp, C.c_int, C.c_double, vp, C.c_double, vp, C.c_int]
+    L.fabipb_b200_matvec_adjoint.argtypes = [vp, C.c_double, vp, C.c_double, vp, C.c_int]
     for name, args in (("fabipb_b200_rhs", [vp, C.c_int, vp, C.c_int]),
                        ("fabipb_b200_energy", [vp, vp, vp, C.c_int]),
                        ("fabipb_b200_precond_setup", [vp, C.c_int]),
@@ -70,8 +75,6 @@ def load():
                        ("fabipb_b200_solve", [vp, vp, vp, C.c_int, C.c_int, C.c_double, vp, vp, vp, C.c_int])):
         if hasattr(L, name):
             getattr(L, name).argtypes = args
-    for name in dir(L):
-        pass
     _lib = L
     return L
 
@@ -118,6 +121,7 @@ class Surface:
         self.h = h
         self.params = prm
         self.n = int(panels.n)
+        self.n_charges = 0
         if charges is not None:
             self.set_charges(charges)
 
@@ -136,6 +140,7 @@ class Surface:
         pos = np.ascontiguousarray(charges.pos.reshape(-1), dtype=np.float64)
         q = np.ascontiguousarray(charges.q, dtype=np.float64)
         _check(load().fabipb_b200_set_charges(self.h, int(q.shape[0]), _ptr(pos), _ptr(q)), "set_charges")
+        self.n_charges = int(q.shape[0])
 
     def launch_count(self):
         return int(load().fabipb_b200_launch_count(self.h))
@@ -199,6 +204,56 @@ class Surface:
         y = np.zeros(2 * self.n) if y is None else np.array(y, dtype=np.float64)
         _check(load().fabipb_b200_matvec(self.h, alpha, _ptr(x), beta, _ptr(y), 0), "matvec")
         return y
+
+    def apply_adjoint(self, lam, part=ALL, alpha=1.0, beta=0.0, out=None, on_device=0):
+        """out = beta*out + alpha*K_part^T lam (the transposed operator)."""
+        if on_device:
+            _check(load().fabipb_b200_apply_adjoint(self.h, part, alpha, _ptr(lam), beta, _ptr(out), 1),
+                   "apply_adjoint")
+            return out
+        lam = np.ascontiguousarray(lam, dtype=np.float64)
+        out = np.zeros(2 * self.n) if out is None else np.array(out, dtype=np.float64)
+        _check(load().fabipb_b200_apply_adjoint(self.h, part, alpha, _ptr(lam), beta, _ptr(out), 0), "apply_adjoint")
+        return out
+
+    def matvec_adjoint(self, x, alpha=1.0, beta=0.0, y=None, on_device=0):
+        """y = alpha*(D - K)^T x + beta*y."""
+        if on_device:
+            _check(load().fabipb_b200_matvec_adjoint(self.h, alpha, _ptr(x), beta, _ptr(y), 1), "matvec_adjoint")
+            return y
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.zeros(2 * self.n) if y is None else np.array(y, dtype=np.float64)
+        _check(load().fabipb_b200_matvec_adjoint(self.h, alpha, _ptr(x), beta, _ptr(y), 0), "matvec_adjoint")
+        return y
+
+    def energy_weights(self):
+        """Direct energy weights e (2N, tree order): energy_raw = e . sigma."""
+        e = np.zeros(2 * self.n)
+        _check(load().fabipb_b200_energy_weights(self.h, _ptr(e), 0), "energy_weights")
+        return e
+
+    def forward(self, restart=10, maxit=100, tol=1e-6):
+        """Direct RHS, GMRES, direct energy; returns (energy_raw, iters, resid, info)."""
+        e = np.zeros(1)
+        it = np.zeros(1, np.int32)
+        res = np.zeros(1)
+        info = np.zeros(1, np.int32)
+        _check(load().fabipb_b200_forward(self.h, int(restart), int(maxit), float(tol), _ptr(e), _ptr(it), _ptr(res),
+                                          _ptr(info)), "forward")
+        return float(e[0]), int(it[0]), float(res[0]), int(info[0])
+
+    def backward(self, grad_energy=1.0, restart=10, maxit=100, tol=1e-6):
+        """Adjoint solve and charge gradients of grad_energy * energy_raw:
+        returns (dE/dq (M,), dE/dx (M, 3), iters, resid, info)."""
+        m = self.n_charges
+        dq = np.zeros(m)
+        dx = np.zeros(3 * m)
+        it = np.zeros(1, np.int32)
+        res = np.zeros(1)
+        info = np.zeros(1, np.int32)
+        _check(load().fabipb_b200_backward(self.h, float(grad_energy), int(restart), int(maxit), float(tol), _ptr(dq),
+                                           _ptr(dx), _ptr(it), _ptr(res), _ptr(info), 0), "backward")
+        return dq, dx.reshape(m, 3), int(it[0]), float(res[0]), int(info[0])
 
     def rhs(self, use_tree=False, out=None, on_device=0):
         if on_device:

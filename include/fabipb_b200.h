@@ -89,6 +89,16 @@ int fabipb_b200_apply(void *ctx, int part, double alpha, const double *sgm, doub
 /* y = alpha*(D - K)x + beta*y  (MtVmain, src/fabipb.c:1237) */
 int fabipb_b200_matvec(void *ctx, double alpha, const double *x, double beta, double *y,
                        int on_device);
+/* the transposed operators, for adjoint solves (no counterpart in the
+   reference): out = beta*out + alpha*K_part^T*lam, and
+   y = alpha*(D - K)^T x + beta*y.  The transposed far field runs the FMM
+   passes in reverse (Q2M^T = L2P-shaped, M2L over the transposed pair lists,
+   L2L^T/M2M^T as shifts); the near field swaps the roles of the panels of a
+   pair.  The first call builds the transposed lists (allocates). */
+int fabipb_b200_apply_adjoint(void *ctx, int part, double alpha, const double *lam, double beta,
+                              double *out, int on_device);
+int fabipb_b200_matvec_adjoint(void *ctx, double alpha, const double *x, double beta, double *y,
+                               int on_device);
 /* right-hand side, 2N in tree order (setupRHS, src/fabipb.c:744):
    use_tree = 0 direct panel-charge sum, 1 charge-tree walk */
 int fabipb_b200_rhs(void *ctx, int use_tree, double *rhs, int on_device);
@@ -105,6 +115,23 @@ int fabipb_b200_energy(void *ctx, const double *sgm, double *raw, int on_device)
    overlap on one GPU share the array and race.  No counterpart in the
    reference, whose energy path allocates per call. */
 int fabipb_b200_energy_noalloc(void *ctx, const double *sgm, double *raw);
+/* gradients of the solvation energy with respect to the charges, surface
+   fixed (no counterpart in the reference).  The energy here is the direct
+   panel-charge sum E = e . sigma with e the energy weights (2N, pot slot
+   eps dGk/dn - dG0/dn, dpdn slot G0 - Gk, times 2A and the quadrature
+   weights); it equals fabipb_b200_energy with every charge-tree cluster
+   opened.
+   fabipb_b200_forward: direct RHS, GMRES from x0 = b with the current
+   preconditioner (block LU set up when none is), E; keeps sigma.
+   fabipb_b200_backward: the adjoint solve (D - K)^T lambda = e from
+   lambda0 = e with its own Krylov basis, then per charge
+   dE/dq_k = grad_energy * phi_k and dE/dr_k = grad_energy * q_k grad phi_k
+   (dEdq: m values, dEdx: 3m, x y z per charge; either may be NULL). */
+int fabipb_b200_energy_weights(void *ctx, double *e, int on_device);
+int fabipb_b200_forward(void *ctx, int restart, int maxit, double tol, double *energy_raw, int *iters,
+                        double *resid, int *info);
+int fabipb_b200_backward(void *ctx, double grad_energy, int restart, int maxit, double tol, double *dEdq,
+                         double *dEdx, int *iters, double *resid, int *info, int on_device);
 /* preconditioner (src/precond_fmm.c): mode 2 block LU, 3 diagonal, -1 none */
 int fabipb_b200_precond_setup(void *ctx, int mode);
 int fabipb_b200_precond_apply(void *ctx, const double *b, double *x, int on_device);

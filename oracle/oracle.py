@@ -104,6 +104,10 @@ class Oracle:
                              np.ascontiguousarray(charges.pos.reshape(-1)),
                              np.ascontiguousarray(charges.q))
 
+    def set_charges(self, charges):
+        lib().or_set_charges(self.h, int(charges.q.shape[0]), np.ascontiguousarray(charges.pos.reshape(-1)),
+                             np.ascontiguousarray(charges.q))
+
     def __del__(self):
         if getattr(self, "h", None):
             lib().or_destroy(self.h)
