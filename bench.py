@@ -229,6 +229,20 @@ def solve_report(pan, ch, opts, device, st):
         out[tag] = {"gmres_s": ev[1].elapsed_time(ev[2]) / 1000.0, "setup_s": ev[0].elapsed_time(ev[1]) / 1000.0,
                     "energy_s": ev[2].elapsed_time(ev[3]) / 1000.0, "wall_s": wall, "iterations": it,
                     "residual": res, "info": info, "energy_kcal_mol": e}
+        # gradients of the (direct) energy: forward = RHS + GMRES + energy,
+        # backward = adjoint GMRES + dE/dq, dE/dx of every charge
+        ag = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        torch.cuda.synchronize()
+        ag[0].record(st)
+        ef, itf, resf, inff = s.forward(restart=opts["restart"], maxit=100, tol=opts["tol"])
+        ag[1].record(st)
+        dq, dx, itb, resb, infb = s.backward(1.0, restart=opts["restart"], maxit=100, tol=opts["tol"])
+        ag[2].record(st)
+        torch.cuda.synchronize()
+        fs, bs = ag[0].elapsed_time(ag[1]) / 1000.0, ag[1].elapsed_time(ag[2]) / 1000.0
+        out[tag]["adjoint"] = {"forward_s": fs, "backward_s": bs, "backward_over_forward": bs / fs,
+                               "forward_iterations": itf, "backward_iterations": itb, "info": [inff, infb],
+                               "charges": int(len(ch.q)), "energy_direct_kcal_mol": ef * kcal}
         s.close()
     m, f = out["mixed"], out["fp64"]
     out["energy_rel_err_mixed_vs_fp64"] = abs(m["energy_kcal_mol"] - f["energy_kcal_mol"]) / abs(f["energy_kcal_mol"])
