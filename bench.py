@@ -198,6 +198,59 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+def measured_hbm_gbs():
+    """Copy bandwidth measured on this pool (MEASURED_PEAKS.json), else the fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fp:
+            return float(json.load(fp)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def pass_report(surf, info, x_ptr, flush, reps, prec_is_mixed, sm_mhz, n_sm):
+    """Per-pass device times (CUDA events between the passes of one matvec,
+    L2 flushed before every matvec) against each pass's bound: algorithmic
+    FLOPs for the near field and M2L, algorithmic bytes for the rest."""
+    import torch
+    acc = None
+    for _ in range(reps):
+        flush.zero_()
+        t = surf.pass_times(x_ptr, reps=1, on_device=1)
+        acc = t if acc is None else {k: acc[k] + t[k] for k in acc}
+    ms = {k: v / reps for k, v in acc.items()}
+    n, leaves, cubes = info["panels"], info["leaves"], info["cubes"]
+    p, pl = info["max_order"], info["leaf_order"]
+    nmom = lambda q: (q + 1) * (q + 2) * (q + 3) // 6
+    from math import comb
+    hbm, hbm_src = measured_hbm_gbs()
+    fp32 = n_sm * 128 * 2 * sm_mhz * 1e6 / 1e12
+    fp64 = n_sm * 64 * 2 * sm_mhz * 1e6 / 1e12
+    near_peak = fp32 if prec_is_mixed else fp64
+    work = {
+        "near": ("flop", FLOP_PER_PAIR * info["near_panel_pairs"], near_peak),
+        "q2m": ("bytes", 8.0 * (2 * nmom(pl) * n + 2 * n + 2 * nmom(p) * leaves), hbm),
+        "m2m": ("bytes", 8.0 * 2 * nmom(p) * 2 * cubes, hbm),
+        "m2l": ("flop", 8.0 * comb(p + 6, 6) * info["m2l_pairs"], fp64),
+        "l2l": ("bytes", 8.0 * 4 * nmom(p) * 2 * cubes, hbm),
+        "l2p": ("bytes", 8.0 * (2 * nmom(pl) * n + 4 * nmom(p) * leaves + 6 * n), hbm),
+    }
+    out = {}
+    for k, (kind, amount, peak) in work.items():
+        t = ms[k] / 1000.0
+        if kind == "flop":
+            ach = amount / t / 1e12
+            out[k] = {"ms": ms[k], "bound": ("fp32" if (k == "near" and prec_is_mixed) else "fp64"),
+                      "achieved": ach, "unit": "TFLOP/s", "peak": peak, "frac": ach / peak,
+                      "algorithmic": amount}
+        else:
+            ach = amount / t / 1e9
+            out[k] = {"ms": ms[k], "bound": "hbm", "achieved": ach, "unit": "GB/s", "peak": peak,
+                      "frac": ach / peak, "algorithmic": amount, "peak_source": hbm_src}
+    m2l_bytes = 16.0 * nmom(p) * info["m2l_pairs"]   # the (D G0, D Gk) tensors read per launch
+    out["m2l"]["tensor_gbs"] = m2l_bytes / (ms["m2l"] / 1000.0) / 1e9
+    return out
+
+
 def solve_report(pan, ch, opts, device, st):
     """Full solves of the same case in both precisions: direct RHS, block-LU
     preconditioner, device GMRES from x0 = b (as the reference CLI), energy.
@@ -353,6 +406,7 @@ def run_ours(args):
         with open(prof) as fp:
             m = re.search(r"dram_bytes_per_launch \| (\d+)", fp.read())
         traffic = int(m.group(1)) if m else None
+    passes = pass_report(surf, info, x.data_ptr(), flush, args.steps, prec == lib.MIXED, sm_mhz, n_sm)
     solve = None if args.no_solve else solve_report(pan, ch, opts, local, stream)
     cpu = None
     if not args.no_cpu_baseline:
@@ -380,6 +434,7 @@ def run_ours(args):
         "gpu_launches": launches,
         "clocks": clocks,
         "setup_s": info["setup_seconds"],
+        "passes": passes,
         "solve": solve,
     }
     if pg:

@@ -402,6 +402,46 @@ int fabipb_b200_matvec(void *ctx, double alpha, const double *x, double beta, do
   });
 }
 
+int fabipb_b200_pass_times(void *ctx, const double *x, int reps, double *ms, int on_device) {
+  if (!valid_ctx(ctx) || x == nullptr || ms == nullptr || reps < 1) {
+    set_error("fabipb_b200_pass_times: invalid arguments");
+    return 0;
+  }
+  Context *c = (Context *)ctx;
+  cudaEvent_t ev[7];
+  for (int i = 0; i < 7; i++) cudaEventCreate(&ev[i]);
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  cudaSetDevice(c->device);
+  bool ok = true;
+  const double *xd = x;
+  if (ok && !on_device) {
+    ok = cudaMemcpyAsync(c->d_x, x, 2 * (size_t)c->n * sizeof(double), cudaMemcpyHostToDevice, c->stream) ==
+         cudaSuccess;
+    xd = c->d_x;
+  }
+  for (int r = 0; ok && r < reps; r++) {
+    cudaEventRecord(ev[0], c->stream);
+    ok = launch_near(*c, xd, -1.0, c->d_y);
+    cudaEventRecord(ev[1], c->stream);
+    ok = ok && launch_far_upward(*c, xd, false, ev + 2);
+    ok = ok && launch_l2p(*c, -1.0, 1.0, c->d_y, xd, 1.0, 1.0);
+    cudaEventRecord(ev[6], c->stream);
+    if (ok) ok = cudaEventSynchronize(ev[6]) == cudaSuccess;
+    for (int i = 0; ok && i < 6; i++) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
+      acc[i] += t;
+    }
+  }
+  for (int i = 0; i < 7; i++) cudaEventDestroy(ev[i]);
+  if (!ok) {
+    set_error("pass timing failed: %s", get_error());
+    return 0;
+  }
+  for (int i = 0; i < 6; i++) ms[i] = acc[i] / reps;
+  return 1;
+}
+
 int fabipb_b200_apply_adjoint(void *ctx, int part, double alpha, const double *lam, double beta, double *out,
                               int on_device) {
   if (!valid_ctx(ctx) || lam == nullptr || out == nullptr) return 0;

@@ -102,7 +102,8 @@ bool setup_charges(Context &c, int m, const double *pos, const double *q);
 bool launch_near(Context &c, const double *sgm, double coef, double *out, bool adjoint = false);
 // upward pass + interaction + downward pass: leaves local expansions in d_lec
 // (adjoint: the transposed far operator's upward half, see fmm.cu)
-bool launch_far_upward(Context &c, const double *sgm, bool adjoint = false);
+// (marks: 4 events recorded after Q2M, M2M, M2L and L2L, for pass timing)
+bool launch_far_upward(Context &c, const double *sgm, bool adjoint = false, cudaEvent_t *marks = nullptr);
 // L2P: out = beta*out + alpha*far + diag*(area .* x) (diag part optional)
 bool launch_l2p(Context &c, double alpha, double beta, double *out, const double *diagX,
                 double s1, double s2, bool adjoint = false);

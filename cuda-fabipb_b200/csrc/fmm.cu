@@ -877,7 +877,7 @@ static bool setup_m2l_adjoint(Context &c) {
 // the halves exchanged) -> g12, g34 in d_lec planes 0, 1; L2L^T, which is the
 // M2M shift; M2L^T into d_mom planes 0, 1 (adjoint moments pot, dpdn); M2M^T,
 // which is the L2L shift; launch_l2p(adjoint) then applies Q2M^T.
-bool launch_far_upward(Context &c, const double *sgm, bool adjoint) {
+bool launch_far_upward(Context &c, const double *sgm, bool adjoint, cudaEvent_t *marks) {
   const PanelTree &pt = c.pt;
   const int depth = pt.t.depth, height = pt.t.height;
   cudaStream_t s = c.stream;
@@ -890,6 +890,7 @@ bool launch_far_upward(Context &c, const double *sgm, bool adjoint) {
   double *up1 = adjoint ? c.d_lec + plane : c.d_mom, *up2 = adjoint ? c.d_lec : c.d_mom + plane;
   q2m_kernel<<<pt.nLeaves, 256, 0, s>>>(pt.nLeaves, c.n, c.NMleaf, c.NM, c.d_leafStart, c.d_leafCount, c.d_leafFmm,
                                         c.d_Q0, c.d_Q1, sgm, adjoint ? 1 : 0, up1, up2);
+  if (marks) cudaEventRecord(marks[0], s);
   for (int lev = depth - 1; lev >= height; lev--) {
     int ordOut = pt.ordMom[lev], ordIn = pt.ordMom[lev + 1];
     int thr = std::max(32, ((nmom(ordOut) + 31) / 32) * 32);
@@ -898,7 +899,9 @@ bool launch_far_upward(Context &c, const double *sgm, bool adjoint) {
                                                        ordIn, c.d_kidFirst, c.d_kidCount, c.d_cubeCtr, c.d_mOff,
                                                        c.d_mLst, up1, up2);
   }
+  if (marks) cudaEventRecord(marks[1], s);
   if (!launch_m2l_only(c, adjoint)) return false;
+  if (marks) cudaEventRecord(marks[2], s);
   // downward arrays: 4 local planes (forward) or the 2 adjoint moment planes
   // plus 2 scratch planes (adjoint)
   double *d1 = adjoint ? c.d_mom : c.d_lec, *d2 = adjoint ? c.d_mom + plane : c.d_lec + plane;
@@ -911,6 +914,7 @@ bool launch_far_upward(Context &c, const double *sgm, bool adjoint) {
         c.d_lstOff, c.d_lst, d1, d2, c.d_lec + 2 * plane, c.d_lec + 3 * plane);
   }
   if (adjoint) FB_CUDA(cudaMemsetAsync(c.d_lec + 2 * plane, 0, 2 * plane * sizeof(double), s));
+  if (marks) cudaEventRecord(marks[3], s);
   FB_CUDA(cudaGetLastError());
   return true;
 }

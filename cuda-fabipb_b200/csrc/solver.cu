@@ -37,6 +37,7 @@ struct PrecondDev {
   std::vector<long long> hOff;
   int *d_start = nullptr, *d_size = nullptr;
   int2 *d_tiles = nullptr;   // (block, first row) tiles of the apply
+  int *d_colSrc = nullptr;   // per block (offset 2*start): input component of each stored column
   int nTiles = 0;
   long long *d_off = nullptr;
   double *d_inv = nullptr;
@@ -95,15 +96,168 @@ __global__ void pc_assemble_kernel(int nBlocks, const int *__restrict__ bStart, 
   }
 }
 
-__global__ void identity_kernel(int nBlocks, const int *__restrict__ bSize, const long long *__restrict__ bOff,
-                                double *I) {
-  const int b = blockIdx.y;
-  if (b >= nBlocks) return;
+// the listed blocks of I := identity, and their column index the identity
+__global__ void identity_kernel(int nList, const int *__restrict__ list, const int *__restrict__ bStart,
+                                const int *__restrict__ bSize, const long long *__restrict__ bOff, double *I,
+                                int *colSrc) {
+  if ((int)blockIdx.y >= nList) return;
+  const int b = list[blockIdx.y];
   const int M = 2 * bSize[b];
   const long long e = (long long)M * M;
   double *Ib = I + bOff[b];
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < e; p += (long long)gridDim.x * blockDim.x)
     Ib[p] = ((p / M) == (p % M)) ? 1.0 : 0.0;
+  if (blockIdx.x == 0)
+    for (int c = threadIdx.x; c < M; c += blockDim.x) colSrc[2LL * bStart[b] + c] = c;
+}
+
+// In-place inversion of the preconditioner blocks by blocked Gauss-Jordan
+// elimination with partial (row) pivoting, one thread block per diagonal
+// block and everything in one launch (a library LU costs tens of small
+// launches per block).  Per panel of NB columns: the panel is eliminated in
+// shared memory (pivot = first largest |a| at or below the diagonal, as
+// idamax), the other columns receive the panel's row swaps, their panel rows
+// are moved to a scratch Y and zeroed, and A(:, rest) += Panel * Y (the
+// composite elimination of the panel, a rank-NB update).  The column
+// interchanges that end Gauss-Jordan are not carried out: colSrc[c] records
+// which input component stored column c multiplies, and the apply kernels
+// gather through it.  info[b] = k+1 for an exactly zero pivot k.
+constexpr int kGjThreads = 256;
+
+template <int NB>
+__global__ void __launch_bounds__(kGjThreads)
+pc_gj_invert_kernel(const int *__restrict__ list, const int *__restrict__ bStart, const int *__restrict__ bSize,
+                    const long long *__restrict__ bOff, const long long *__restrict__ yOff, double *inv, double *yAll,
+                    int *colSrc, int *info) {
+  extern __shared__ double gjSmem[];
+  __shared__ double redv[kGjThreads];
+  __shared__ int redi[kGjThreads];
+  __shared__ double rowk[NB];
+  const int b = list[blockIdx.x];
+  const int M = 2 * bSize[b];
+  double *A = inv + bOff[b];
+  double *Y = yAll + yOff[b];
+  double *P = gjSmem;                          // panel, [NB][M]
+  double *Yt = gjSmem + (size_t)NB * M;        // Y tile, [64][NB]
+  int *perm = (int *)(Yt + 64 * NB);           // [M]
+  const int t = threadIdx.x;
+  int bad = 0;
+  for (int k0 = 0; k0 < M; k0 += NB) {
+    const int nb = min(NB, M - k0);
+    for (int e = t; e < nb * M; e += kGjThreads) P[e] = A[(size_t)k0 * M + e];   // columns k0.. are contiguous
+    __syncthreads();
+    for (int kk = 0; kk < nb; kk++) {
+      const int k = k0 + kk;
+      double best = -1.0;
+      int bi = M;
+      for (int i = k + t; i < M; i += kGjThreads) {
+        const double v = fabs(P[kk * M + i]);
+        if (v > best) { best = v; bi = i; }
+      }
+      redv[t] = best;
+      redi[t] = bi;
+      __syncthreads();
+      for (int sft = kGjThreads / 2; sft > 0; sft >>= 1) {
+        if (t < sft && (redv[t + sft] > redv[t] || (redv[t + sft] == redv[t] && redi[t + sft] < redi[t]))) {
+          redv[t] = redv[t + sft];
+          redi[t] = redi[t + sft];
+        }
+        __syncthreads();
+      }
+      const int pv = redi[0];
+      if (t == 0) perm[k] = pv;
+      if (pv != k && t < nb) {
+        const double a = P[t * M + k];
+        P[t * M + k] = P[t * M + pv];
+        P[t * M + pv] = a;
+      }
+      __syncthreads();
+      const double piv = P[kk * M + k];
+      if (piv == 0.0) bad = bad ? bad : k + 1;
+      const double d = (piv != 0.0) ? 1.0 / piv : 0.0;
+      if (t < nb) rowk[t] = (t == kk) ? d : P[t * M + k] * d;
+      __syncthreads();
+      for (int i = t; i < M; i += kGjThreads) {
+        if (i == k) {
+          for (int c = 0; c < nb; c++) P[c * M + k] = rowk[c];
+        } else {
+          const double f = P[kk * M + i];
+          for (int c = 0; c < nb; c++) P[c * M + i] = (c == kk) ? -f * d : P[c * M + i] - f * rowk[c];
+        }
+      }
+      __syncthreads();
+    }
+    for (int e = t; e < nb * M; e += kGjThreads) A[(size_t)k0 * M + e] = P[e];
+    // the other columns: the panel's row swaps, then rows k0.. to Y and zero
+    for (int j = t; j < M; j += kGjThreads) {
+      if (j >= k0 && j < k0 + nb) continue;
+      double *col = A + (size_t)j * M;
+      for (int kk = 0; kk < nb; kk++) {
+        const int k = k0 + kk, pv = perm[k];
+        if (pv != k) {
+          const double a = col[k];
+          col[k] = col[pv];
+          col[pv] = a;
+        }
+      }
+      for (int kk = 0; kk < nb; kk++) {
+        Y[(size_t)j * NB + kk] = col[k0 + kk];
+        col[k0 + kk] = 0.0;
+      }
+    }
+    __syncthreads();
+    // A(:, rest) += P * Y, tiles of 64 columns x 64 rows; thread: one row, 16 columns
+    const int rl = t % 64, cg = t / 64;
+    for (int jt = 0; jt < M; jt += 64) {
+      for (int e = t; e < 64 * NB; e += kGjThreads) {
+        const int jl = e / NB, kk = e % NB, j = jt + jl;
+        const bool ok = j < M && (j < k0 || j >= k0 + nb) && kk < nb;
+        Yt[e] = ok ? Y[(size_t)j * NB + kk] : 0.0;
+      }
+      __syncthreads();
+      for (int it = 0; it < M; it += 64) {
+        const int i = it + rl;
+        if (i < M) {
+          double acc[16];
+#pragma unroll
+          for (int c = 0; c < 16; c++) {
+            const int j = jt + cg + 4 * c;
+            acc[c] = (j < M) ? A[(size_t)j * M + i] : 0.0;
+          }
+          for (int kk = 0; kk < nb; kk++) {
+            const double w = P[kk * M + i];
+#pragma unroll
+            for (int c = 0; c < 16; c++) acc[c] += w * Yt[(cg + 4 * c) * NB + kk];
+          }
+#pragma unroll
+          for (int c = 0; c < 16; c++) {
+            const int j = jt + cg + 4 * c;
+            if (j < M && (j < k0 || j >= k0 + nb)) A[(size_t)j * M + i] = acc[c];
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  // the pending column interchanges, as an index: stored column c multiplies input component colSrc[c]
+  __syncthreads();
+  if (t == 0) {
+    // sigma: final column j = stored column sigma[j], built by replaying the swaps in reverse
+    int *cs = colSrc + 2 * bStart[b];
+    for (int c = 0; c < M; c++) cs[c] = c;   // cs temporarily holds sigma
+    for (int k = M - 1; k >= 0; k--) {
+      const int pv = perm[k];
+      if (pv != k) {
+        const int a = cs[k];
+        cs[k] = cs[pv];
+        cs[pv] = a;
+      }
+    }
+    // invert: colSrc[sigma[j]] = j
+    for (int j = 0; j < M; j++) perm[cs[j]] = j;
+    for (int c = 0; c < M; c++) cs[c] = perm[c];
+    info[b] = bad;
+  }
 }
 
 // x = blockdiag(inv) * b, block b gathers its pot/dpdn halves
@@ -123,8 +277,8 @@ constexpr int kPcRows = 64, kPcSplit = 4;
 template <typename TI>
 __global__ void __launch_bounds__(kPcRows * kPcSplit)
 pc_apply_kernel(int n, const int2 *__restrict__ tiles, const int *__restrict__ bStart, const int *__restrict__ bSize,
-                const long long *__restrict__ bOff, const TI *__restrict__ inv, const double *__restrict__ rhs,
-                double *x) {
+                const long long *__restrict__ bOff, const int *__restrict__ colSrc, const TI *__restrict__ inv,
+                const double *__restrict__ rhs, double *x) {
   __shared__ double red[kPcSplit][kPcRows];
   const int2 tl = tiles[blockIdx.x];
   const int b = tl.x, r0 = tl.y;
@@ -132,12 +286,14 @@ pc_apply_kernel(int n, const int2 *__restrict__ tiles, const int *__restrict__ b
   const int rr = threadIdx.x % kPcRows, q = threadIdx.x / kPcRows;
   const int r = r0 + rr;
   const TI *Ib = inv + bOff[b];
+  const int *cs = colSrc + 2 * (size_t)st;
   const int c0 = (int)(((long long)M * q) / kPcSplit), c1 = (int)(((long long)M * (q + 1)) / kPcSplit);
   double y = 0.0;
   if (r < M) {
 #pragma unroll 4
     for (int c = c0; c < c1; c++) {
-      const double xc = (c < hm) ? rhs[st + c] : rhs[n + st + c - hm];
+      const int g = cs[c];
+      const double xc = (g < hm) ? rhs[st + g] : rhs[n + st + g - hm];
       y += (double)Ib[(size_t)c * M + r] * xc;
     }
   }
@@ -155,8 +311,8 @@ pc_apply_kernel(int n, const int2 *__restrict__ tiles, const int *__restrict__ b
 // lanes over the (contiguous) column; tiles as for pc_apply_kernel.
 __global__ void __launch_bounds__(kPcRows * kPcSplit)
 pc_apply_t_kernel(int n, const int2 *__restrict__ tiles, const int *__restrict__ bStart, const int *__restrict__ bSize,
-                  const long long *__restrict__ bOff, const double *__restrict__ inv, const double *__restrict__ rhs,
-                  double *x) {
+                  const long long *__restrict__ bOff, const int *__restrict__ colSrc, const double *__restrict__ inv,
+                  const double *__restrict__ rhs, double *x) {
   const int2 tl = tiles[blockIdx.x];
   const int b = tl.x, c0 = tl.y;
   const int hm = bSize[b], st = bStart[b], M = 2 * hm;
@@ -168,8 +324,9 @@ pc_apply_t_kernel(int n, const int2 *__restrict__ tiles, const int *__restrict__
     for (int r = lane; r < M; r += 32) y += col[r] * ((r < hm) ? rhs[st + r] : rhs[n + st + r - hm]);
     for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
     if (lane == 0) {
-      if (c < hm) x[st + c] = y;
-      else x[n + st + c - hm] = y;
+      const int g = colSrc[2 * (size_t)st + c];   // stored column c is output component g
+      if (g < hm) x[st + g] = y;
+      else x[n + st + g - hm] = y;
     }
   }
 }
@@ -180,6 +337,199 @@ __global__ void pc_diag_kernel(int n, const double *__restrict__ area, double s1
   if (i >= n) return;
   x[i] = b[i] / (s1 * area[i]);
   x[n + i] = b[n + i] / (s2 * area[i]);
+}
+
+// LU and explicit inverse of every block with cuSOLVER (blocks above the
+// Gauss-Jordan kernel's size limit), spread over several streams so that
+// independent blocks run side by side.  Inverts d_A into p.d_inv.
+static bool factor_cusolver(Context &c, PrecondDev &p, const std::vector<int> &blocks) {
+  cudaStream_t s = c.stream;
+  if (blocks.empty()) return true;
+  // copy the assembled blocks out of d_inv, which then starts as the identity
+  std::vector<long long> aOff(p.nBlocks, -1);
+  long long atot = 0;
+  int maxM = 0;
+  for (int b : blocks) {
+    aOff[b] = atot;
+    atot += 4LL * p.hSize[b] * p.hSize[b];
+    maxM = std::max(maxM, 2 * p.hSize[b]);
+  }
+  double *d_A = nullptr;
+  FB_CUDA(cudaMalloc((void **)&d_A, (size_t)atot * sizeof(double)));
+  for (int b : blocks)
+    FB_CUDA(cudaMemcpyAsync(d_A + aOff[b], p.d_inv + p.hOff[b], 4LL * p.hSize[b] * p.hSize[b] * sizeof(double),
+                            cudaMemcpyDeviceToDevice, s));
+  const int ns = std::min(FB_PC_STREAMS, std::max((int)blocks.size(), 1));
+  std::vector<cusolverDnHandle_t> hs(ns, nullptr);
+  std::vector<cudaStream_t> ss(ns, nullptr);
+  std::vector<double *> works(ns, nullptr);
+  std::vector<int *> pivs(ns, nullptr);
+  int lwork = 0, *d_info = nullptr;
+  int *d_list = nullptr;
+  FB_CUDA(cudaMalloc((void **)&d_list, blocks.size() * sizeof(int)));
+  FB_CUDA(cudaMemcpyAsync(d_list, blocks.data(), blocks.size() * sizeof(int), cudaMemcpyHostToDevice, s));
+  dim3 grid(64, (unsigned)blocks.size());
+  identity_kernel<<<grid, 256, 0, s>>>((int)blocks.size(), d_list, p.d_start, p.d_size, p.d_off, p.d_inv, p.d_colSrc);
+  cudaEvent_t evA = nullptr;
+  bool ok = cudaEventCreateWithFlags(&evA, cudaEventDisableTiming) == cudaSuccess;
+  ok = ok && cudaEventRecord(evA, s) == cudaSuccess;
+  for (int k = 0; ok && k < ns; k++) {
+    ok = cudaStreamCreateWithFlags(&ss[k], cudaStreamNonBlocking) == cudaSuccess &&
+         cusolverDnCreate(&hs[k]) == CUSOLVER_STATUS_SUCCESS && cusolverDnSetStream(hs[k], ss[k]) == CUSOLVER_STATUS_SUCCESS &&
+         cudaStreamWaitEvent(ss[k], evA, 0) == cudaSuccess;
+  }
+  if (ok && cusolverDnDgetrf_bufferSize(hs[0], maxM, maxM, d_A, maxM, &lwork) != CUSOLVER_STATUS_SUCCESS) ok = false;
+  for (int k = 0; ok && k < ns; k++)
+    ok = cudaMalloc((void **)&works[k], (size_t)std::max(lwork, 1) * sizeof(double)) == cudaSuccess &&
+         cudaMalloc((void **)&pivs[k], (size_t)maxM * sizeof(int)) == cudaSuccess;
+  ok = ok && cudaMalloc((void **)&d_info, (size_t)p.nBlocks * sizeof(int)) == cudaSuccess;
+  ok = ok && cudaMemsetAsync(d_info, 0, (size_t)p.nBlocks * sizeof(int), s) == cudaSuccess;
+  std::vector<int> order(blocks);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return p.hSize[a] > p.hSize[b]; });
+  for (int q = 0; ok && q < (int)order.size(); q++) {
+    const int b = order[q], k = q % ns;
+    int M = 2 * p.hSize[b];
+    if (M == 0) continue;
+    double *Ab = d_A + aOff[b], *Ib = p.d_inv + p.hOff[b];
+    if (cusolverDnDgetrf(hs[k], M, M, Ab, M, works[k], pivs[k], d_info + b) != CUSOLVER_STATUS_SUCCESS) ok = false;
+    if (ok && cusolverDnDgetrs(hs[k], CUBLAS_OP_N, M, M, Ab, M, pivs[k], Ib, M, d_info + b) != CUSOLVER_STATUS_SUCCESS)
+      ok = false;
+  }
+  for (int k = 0; k < ns; k++) {
+    if (!ss[k]) continue;
+    cudaEvent_t ev = nullptr;
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess) {
+      cudaEventRecord(ev, ss[k]);
+      cudaStreamWaitEvent(s, ev, 0);
+      cudaEventDestroy(ev);
+    } else {
+      ok = false;
+    }
+  }
+  std::vector<int> info(p.nBlocks, 0);
+  if (ok) ok = cudaMemcpyAsync(info.data(), d_info, info.size() * sizeof(int), cudaMemcpyDeviceToHost, s) == cudaSuccess;
+  if (ok) ok = cudaStreamSynchronize(s) == cudaSuccess;
+  for (int k = 0; k < ns; k++) {
+    if (ss[k]) cudaStreamSynchronize(ss[k]);
+    if (hs[k]) cusolverDnDestroy(hs[k]);
+    if (ss[k]) cudaStreamDestroy(ss[k]);
+    cudaFree(works[k]);
+    cudaFree(pivs[k]);
+  }
+  if (evA) cudaEventDestroy(evA);
+  cudaFree(d_info);
+  cudaFree(d_list);
+  cudaFree(d_A);
+  FB_CHECK(ok, "preconditioner factorisation failed: %s", cudaGetErrorString(cudaGetLastError()));
+  for (int b = 0; b < p.nBlocks; b++)
+    FB_CHECK(info[b] == 0, "dgetrf failed in preconditioner block %d (info=%d)", b, info[b]);
+  return true;
+}
+
+// Blocks up to this size go to the Gauss-Jordan kernel, one thread block
+// each; larger ones to cuSOLVER (several streams).  The kernel takes up to
+// kGjMaxM (its panel of NB columns lives in shared memory); measured on the
+// 204,800-panel star surface, sending everything to the kernel is fastest
+// (cuSOLVER launches run slowly beside the kernel's resident blocks).
+#ifndef FB_PC_GJ_MAXM
+#define FB_PC_GJ_MAXM 3200
+#endif
+constexpr int kGjMaxM = 3200;
+
+template <int NB>
+static size_t gj_smem(int maxM) {
+  return (size_t)NB * maxM * sizeof(double) + 64 * NB * sizeof(double) + (size_t)maxM * sizeof(int);
+}
+
+// Gauss-Jordan inversion of every block in p.d_inv (assembled there), size
+// classes on their own streams so the large blocks start at once.
+static bool factor_hybrid(Context &c, PrecondDev &p) {
+  cudaStream_t s = c.stream;
+  struct Cls { int lo, hi, nb; };
+  const int cut = std::min(FB_PC_GJ_MAXM, kGjMaxM);
+  const Cls cls[4] = {{0, std::min(384, cut), 16}, {std::min(384, cut), std::min(768, cut), 16},
+                      {std::min(768, cut), std::min(1600, cut), 16}, {std::min(1600, cut), cut, 8}};
+  std::vector<int> big;
+  for (int b = 0; b < p.nBlocks; b++)
+    if (2 * p.hSize[b] > cut) big.push_back(b);
+  std::vector<long long> yOff(p.nBlocks);
+  long long ytot = 0;
+  for (int b = 0; b < p.nBlocks; b++) {
+    yOff[b] = ytot;
+    ytot += 16LL * 2 * p.hSize[b];
+  }
+  long long *d_yOff = nullptr;
+  double *d_y = nullptr;
+  int *d_info = nullptr;
+  DevArena tmp;
+  if (!tmp.upload(&d_yOff, yOff, s) || !tmp.alloc_n(&d_y, (size_t)std::max(ytot, 1LL)) ||
+      !tmp.alloc_n(&d_info, (size_t)p.nBlocks))
+    return false;
+  FB_CUDA(cudaMemsetAsync(d_info, 0, (size_t)p.nBlocks * sizeof(int), s));
+  cudaEvent_t evA = nullptr;
+  FB_CUDA(cudaEventCreateWithFlags(&evA, cudaEventDisableTiming));
+  FB_CUDA(cudaEventRecord(evA, s));
+  std::vector<cudaStream_t> ss;
+  bool ok = true;
+  for (const Cls &k : cls) {
+    std::vector<int> list;
+    int maxM = 0;
+    for (int b = 0; b < p.nBlocks; b++) {
+      const int M = 2 * p.hSize[b];
+      if (k.hi > k.lo && M > k.lo && M <= k.hi) {
+        list.push_back(b);
+        maxM = std::max(maxM, M);
+      }
+    }
+    if (list.empty()) continue;
+    std::stable_sort(list.begin(), list.end(), [&](int a, int b) { return p.hSize[a] > p.hSize[b]; });
+    int *d_list = nullptr;
+    cudaStream_t st = nullptr;
+    ok = ok && tmp.upload(&d_list, list, s) && cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess;
+    if (!ok) break;
+    ss.push_back(st);
+    cudaEvent_t evL = nullptr;   // the list upload and the assembly on s come first
+    ok = cudaEventCreateWithFlags(&evL, cudaEventDisableTiming) == cudaSuccess && cudaEventRecord(evL, s) == cudaSuccess &&
+         cudaStreamWaitEvent(st, evL, 0) == cudaSuccess;
+    if (evL) cudaEventDestroy(evL);
+    if (!ok) break;
+    if (k.nb == 16) {
+      const size_t shm = gj_smem<16>(maxM);
+      cudaFuncSetAttribute(pc_gj_invert_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+      pc_gj_invert_kernel<16><<<(unsigned)list.size(), kGjThreads, shm, st>>>(
+          d_list, p.d_start, p.d_size, p.d_off, d_yOff, p.d_inv, d_y, p.d_colSrc, d_info);
+    } else {
+      const size_t shm = gj_smem<8>(maxM);
+      cudaFuncSetAttribute(pc_gj_invert_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+      pc_gj_invert_kernel<8><<<(unsigned)list.size(), kGjThreads, shm, st>>>(
+          d_list, p.d_start, p.d_size, p.d_off, d_yOff, p.d_inv, d_y, p.d_colSrc, d_info);
+    }
+    c.launches += 1;
+    ok = cudaGetLastError() == cudaSuccess;
+  }
+  // the large blocks meanwhile, through cuSOLVER on its own streams
+  if (ok) ok = factor_cusolver(c, p, big);
+  for (cudaStream_t st : ss) {
+    cudaEvent_t ev = nullptr;
+    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess) {
+      cudaEventRecord(ev, st);
+      cudaStreamWaitEvent(s, ev, 0);
+      cudaEventDestroy(ev);
+    }
+  }
+  std::vector<int> info(p.nBlocks, 0);
+  if (ok) ok = cudaMemcpyAsync(info.data(), d_info, info.size() * sizeof(int), cudaMemcpyDeviceToHost, s) == cudaSuccess;
+  if (ok) ok = cudaStreamSynchronize(s) == cudaSuccess;
+  for (cudaStream_t st : ss) {
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+  }
+  cudaEventDestroy(evA);
+  tmp.release();
+  FB_CHECK(ok, "preconditioner inversion failed: %s", cudaGetErrorString(cudaGetLastError()));
+  for (int b = 0; b < p.nBlocks; b++)
+    FB_CHECK(info[b] == 0, "zero pivot in preconditioner block %d (step %d)", b, info[b]);
+  return true;
 }
 
 bool precond_setup(Context &c, int mode) {
@@ -208,90 +558,20 @@ bool precond_setup(Context &c, int mode) {
   FB_CHECK(p.maxM <= 46340, "preconditioner block %d too large (increase -t)", p.maxM);
   cudaStream_t s = c.stream;
   StageTimer tm("precond_setup", s);
-  double *d_A = nullptr;
   if (!p.arena.upload(&p.d_start, p.hStart, s) || !p.arena.upload(&p.d_size, p.hSize, s) ||
-      !p.arena.upload(&p.d_tiles, tiles, s) ||
-      !p.arena.upload(&p.d_off, p.hOff, s) || !p.arena.alloc_n(&p.d_inv, (size_t)off))
+      !p.arena.upload(&p.d_tiles, tiles, s) || !p.arena.upload(&p.d_off, p.hOff, s) ||
+      !p.arena.alloc_n(&p.d_inv, (size_t)off) || !p.arena.alloc_n(&p.d_colSrc, 2 * (size_t)c.n))
     return false;
-  FB_CUDA(cudaMalloc((void **)&d_A, (size_t)off * sizeof(double)));
   const double s1 = (1.0 + c.epsilon) / 2.0, s2 = (1.0 + 1.0 / c.epsilon) / 2.0;
   dim3 grid(64, p.nBlocks);
   pc_assemble_kernel<<<grid, 128, 0, s>>>(p.nBlocks, p.d_start, p.d_size, p.d_off, c.d_vtx, c.d_nrm, c.d_area,
-                                          c.prm.quad_order, c.prm.kappa, c.epsilon, s1, s2, d_A);
-  identity_kernel<<<grid, 256, 0, s>>>(p.nBlocks, p.d_size, p.d_off, p.d_inv);
-  c.launches += 2;
-  cudaError_t le = cudaGetLastError();
-  if (le != cudaSuccess) {
-    cudaFree(d_A);
-    set_error("preconditioner assembly launch failed: %s", cudaGetErrorString(le));
-    return false;
-  }
+                                          c.prm.quad_order, c.prm.kappa, c.epsilon, s1, s2, p.d_inv);
+  c.launches += 1;
+  FB_CUDA(cudaGetLastError());
   tm.mark("assemble");
-  // LU and explicit inverse of every block with cuSOLVER, spread over several
-  // streams: a single block of a few hundred rows keeps only a few SMs busy,
-  // so independent blocks run side by side.
-  const int ns = std::min(FB_PC_STREAMS, std::max(p.nBlocks, 1));
-  std::vector<cusolverDnHandle_t> hs(ns, nullptr);
-  std::vector<cudaStream_t> ss(ns, nullptr);
-  std::vector<double *> works(ns, nullptr);
-  std::vector<int *> pivs(ns, nullptr);
-  int lwork = 0, *d_info = nullptr;
-  cudaEvent_t evA = nullptr;
-  bool ok = cudaEventCreateWithFlags(&evA, cudaEventDisableTiming) == cudaSuccess;
-  ok = ok && cudaEventRecord(evA, s) == cudaSuccess;
-  for (int k = 0; ok && k < ns; k++) {
-    ok = cudaStreamCreateWithFlags(&ss[k], cudaStreamNonBlocking) == cudaSuccess &&
-         cusolverDnCreate(&hs[k]) == CUSOLVER_STATUS_SUCCESS && cusolverDnSetStream(hs[k], ss[k]) == CUSOLVER_STATUS_SUCCESS &&
-         cudaStreamWaitEvent(ss[k], evA, 0) == cudaSuccess;
-  }
-  if (ok && cusolverDnDgetrf_bufferSize(hs[0], p.maxM, p.maxM, d_A, p.maxM, &lwork) != CUSOLVER_STATUS_SUCCESS) ok = false;
-  for (int k = 0; ok && k < ns; k++)
-    ok = cudaMalloc((void **)&works[k], (size_t)std::max(lwork, 1) * sizeof(double)) == cudaSuccess &&
-         cudaMalloc((void **)&pivs[k], (size_t)p.maxM * sizeof(int)) == cudaSuccess;
-  ok = ok && cudaMalloc((void **)&d_info, (size_t)p.nBlocks * sizeof(int)) == cudaSuccess;
-  // largest blocks first so the streams finish together
-  std::vector<int> order(p.nBlocks);
-  for (int b = 0; b < p.nBlocks; b++) order[b] = b;
-  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return p.hSize[a] > p.hSize[b]; });
-  for (int q = 0; ok && q < p.nBlocks; q++) {
-    const int b = order[q], k = q % ns;
-    int M = 2 * p.hSize[b];
-    if (M == 0) continue;
-    double *Ab = d_A + p.hOff[b], *Ib = p.d_inv + p.hOff[b];
-    if (cusolverDnDgetrf(hs[k], M, M, Ab, M, works[k], pivs[k], d_info + b) != CUSOLVER_STATUS_SUCCESS) ok = false;
-    if (ok && cusolverDnDgetrs(hs[k], CUBLAS_OP_N, M, M, Ab, M, pivs[k], Ib, M, d_info + b) != CUSOLVER_STATUS_SUCCESS)
-      ok = false;
-  }
-  // join: the main stream waits for every factor stream
-  for (int k = 0; k < ns; k++) {
-    if (!ss[k]) continue;
-    cudaEvent_t ev = nullptr;
-    if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess) {
-      cudaEventRecord(ev, ss[k]);
-      cudaStreamWaitEvent(s, ev, 0);
-      cudaEventDestroy(ev);
-    } else {
-      ok = false;
-    }
-  }
+  const bool ok = factor_hybrid(c, p);
   tm.mark("factor_invert");
-  std::vector<int> info(p.nBlocks, 0);
-  if (ok) ok = cudaMemcpyAsync(info.data(), d_info, info.size() * sizeof(int), cudaMemcpyDeviceToHost, s) == cudaSuccess;
-  if (ok) ok = cudaStreamSynchronize(s) == cudaSuccess;
-  for (int k = 0; k < ns; k++) {
-    if (ss[k]) cudaStreamSynchronize(ss[k]);
-    if (hs[k]) cusolverDnDestroy(hs[k]);
-    if (ss[k]) cudaStreamDestroy(ss[k]);
-    cudaFree(works[k]);
-    cudaFree(pivs[k]);
-  }
-  if (evA) cudaEventDestroy(evA);
-  cudaFree(d_info);
-  cudaFree(d_A);
-  FB_CHECK(ok, "preconditioner factorisation failed: %s", cudaGetErrorString(cudaGetLastError()));
-  for (int b = 0; b < p.nBlocks; b++)
-    FB_CHECK(info[b] == 0, "dgetrf failed in preconditioner block %d (info=%d)", b, info[b]);
-  return true;
+  return ok;
 }
 
 bool precond_apply(Context &c, const double *b, double *x, bool adjoint) {
@@ -299,10 +579,10 @@ bool precond_apply(Context &c, const double *b, double *x, bool adjoint) {
   PrecondDev &p = *c.pc;
   if (p.mode == 2 && adjoint) {
     pc_apply_t_kernel<<<p.nTiles, kPcRows * kPcSplit, 0, c.stream>>>(c.n, p.d_tiles, p.d_start, p.d_size, p.d_off,
-                                                                    p.d_inv, b, x);
+                                                                    p.d_colSrc, p.d_inv, b, x);
   } else if (p.mode == 2) {
     pc_apply_kernel<double><<<p.nTiles, kPcRows * kPcSplit, 0, c.stream>>>(c.n, p.d_tiles, p.d_start, p.d_size,
-                                                                           p.d_off, p.d_inv, b, x);
+                                                                           p.d_off, p.d_colSrc, p.d_inv, b, x);
   } else if (p.mode == 3) {
     pc_diag_kernel<<<ceil_div(c.n, 256), 256, 0, c.stream>>>(c.n, c.d_area, (1.0 + c.epsilon) / 2.0,
                                                             (1.0 + 1.0 / c.epsilon) / 2.0, b, x);

@@ -64,6 +64,7 @@ def load():
     L.fabipb_b200_apply.argtypes = [vp, C.c_int, C.c_double, vp, C.c_double, vp, C.c_int]
     L.fabipb_b200_matvec.argtypes = [vp, C.c_double, vp, C.c_double, vp, C.c_int]
     L.fabipb_b200_energy_weights.argtypes = [vp, vp, C.c_int]
+    L.fabipb_b200_pass_times.argtypes = [vp, vp, C.c_int, vp, C.c_int]
     L.fabipb_b200_forward.argtypes = [vp, C.c_int, C.c_int, C.c_double, vp, vp, vp, vp]
     L.fabipb_b200_backward.argtypes = [vp, C.c_double, C.c_int, C.c_int, C.c_double, vp, vp, vp, vp, vp, C.c_int]
     L.fabipb_b200_apply_adjoint.argtypes = [vp, C.c_int, C.c_double, vp, C.c_double, vp, C.c_int]
@@ -225,6 +226,16 @@ class Surface:
         y = np.zeros(2 * self.n) if y is None else np.array(y, dtype=np.float64)
         _check(load().fabipb_b200_matvec_adjoint(self.h, alpha, _ptr(x), beta, _ptr(y), 0), "matvec_adjoint")
         return y
+
+    PASSES = ("near", "q2m", "m2m", "m2l", "l2l", "l2p")
+
+    def pass_times(self, x, reps=5, on_device=0):
+        """Mean milliseconds per matvec pass (near, q2m, m2m, m2l, l2l, l2p)."""
+        ms = np.zeros(6)
+        if not on_device:
+            x = np.ascontiguousarray(x, dtype=np.float64)
+        _check(load().fabipb_b200_pass_times(self.h, _ptr(x), int(reps), _ptr(ms), int(on_device)), "pass_times")
+        return dict(zip(self.PASSES, ms.tolist()))
 
     def energy_weights(self):
         """Direct energy weights e (2N, tree order): energy_raw = e . sigma."""

@@ -89,6 +89,12 @@ int fabipb_b200_apply(void *ctx, int part, double alpha, const double *sgm, doub
 /* y = alpha*(D - K)x + beta*y  (MtVmain, src/fabipb.c:1237) */
 int fabipb_b200_matvec(void *ctx, double alpha, const double *x, double beta, double *y,
                        int on_device);
+/* stage report (the counterpart of the reference's -B=1 stage times, no
+   counterpart in its ABI): runs the matvec passes reps times with CUDA events
+   between them and returns the mean milliseconds per pass in ms[6]:
+   near field (pack + P2P + FP64 corrections), Q2M, M2M (all levels), M2L,
+   L2L (all levels), L2P (with the diagonal term). */
+int fabipb_b200_pass_times(void *ctx, const double *x, int reps, double *ms, int on_device);
 /* the transposed operators, for adjoint solves (no counterpart in the
    reference): out = beta*out + alpha*K_part^T*lam, and
    y = alpha*(D - K)^T x + beta*y.  The transposed far field runs the FMM
