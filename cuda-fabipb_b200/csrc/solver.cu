@@ -24,6 +24,8 @@
 #include <cmath>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "context.cuh"
 #include "quad.cuh"
 
@@ -112,136 +114,224 @@ __global__ void identity_kernel(int nList, const int *__restrict__ list, const i
 }
 
 // In-place inversion of the preconditioner blocks by blocked Gauss-Jordan
-// elimination with partial (row) pivoting, one thread block per diagonal
-// block and everything in one launch (a library LU costs tens of small
-// launches per block).  Per panel of NB columns: the panel is eliminated in
-// shared memory (pivot = first largest |a| at or below the diagonal, as
-// idamax), the other columns receive the panel's row swaps, their panel rows
-// are moved to a scratch Y and zeroed, and A(:, rest) += Panel * Y (the
-// composite elimination of the panel, a rank-NB update).  The column
-// interchanges that end Gauss-Jordan are not carried out: colSrc[c] records
-// which input component stored column c multiplies, and the apply kernels
-// gather through it.  info[b] = k+1 for an exactly zero pivot k.
+// elimination with partial (row) pivoting, all blocks in one launch per size
+// class (a library LU costs tens of small launches per block).  A block is
+// inverted by a cluster of CS thread blocks (CS = 1 for small blocks).  Per
+// panel of NB columns:
+//   * every CTA of the cluster eliminates the panel in its shared memory (the
+//     same data, so the same result; pivot = first largest |a| at or below
+//     the diagonal, as idamax) and rank 0 writes it back;
+//   * each CTA takes its share of the other columns (64-column tiles dealt
+//     round-robin): the panel's row interchanges, the panel rows moved to a
+//     scratch Y and zeroed, then A(:, j) += Panel * Y(:, j), the composite
+//     elimination of the panel as a rank-NB update (4x4 outputs per thread);
+//   * a cluster barrier before the next panel, whose columns some CTA owns.
+// The column interchanges that end Gauss-Jordan are not carried out:
+// colSrc[c] records which input component stored column c multiplies, and
+// the apply kernels gather through it.  info[b] = k+1 for an exactly zero
+// pivot k.
 constexpr int kGjThreads = 256;
 
 template <int NB>
-__global__ void __launch_bounds__(kGjThreads)
+__host__ __device__ constexpr size_t gj_smem_bytes(int maxM) {
+  return (size_t)NB * maxM * sizeof(double) + 64 * NB * sizeof(double) + (size_t)maxM * sizeof(int);
+}
+
+template <int NB, int CS>
+__global__ void __launch_bounds__(kGjThreads, 1)
 pc_gj_invert_kernel(const int *__restrict__ list, const int *__restrict__ bStart, const int *__restrict__ bSize,
                     const long long *__restrict__ bOff, const long long *__restrict__ yOff, double *inv, double *yAll,
                     int *colSrc, int *info) {
   extern __shared__ double gjSmem[];
-  __shared__ double redv[kGjThreads];
-  __shared__ int redi[kGjThreads];
-  __shared__ double rowk[NB];
-  const int b = list[blockIdx.x];
+  __shared__ double wbest[kGjThreads / 32];
+  __shared__ int wbi[kGjThreads / 32];
+  __shared__ int sPos[2 * NB], sSrc[2 * NB], sCnt;
+  __shared__ double sRk[NB], sOk[NB];
+  const int rank = (CS > 1) ? (int)(blockIdx.x % CS) : 0;
+  const int b = list[blockIdx.x / CS];
   const int M = 2 * bSize[b];
   double *A = inv + bOff[b];
   double *Y = yAll + yOff[b];
   double *P = gjSmem;                          // panel, [NB][M]
   double *Yt = gjSmem + (size_t)NB * M;        // Y tile, [64][NB]
   int *perm = (int *)(Yt + 64 * NB);           // [M]
-  const int t = threadIdx.x;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   int bad = 0;
   for (int k0 = 0; k0 < M; k0 += NB) {
     const int nb = min(NB, M - k0);
+    if (CS > 1) {   // the owners' updates of these columns are complete and visible
+      __threadfence();
+      cooperative_groups::this_cluster().sync();
+    }
     for (int e = t; e < nb * M; e += kGjThreads) P[e] = A[(size_t)k0 * M + e];   // columns k0.. are contiguous
     __syncthreads();
+    // Row i of the panel belongs to thread i mod kGjThreads throughout, so a
+    // step's pivot search reads only rows its thread wrote in the previous
+    // step: two barriers per step.
     for (int kk = 0; kk < nb; kk++) {
       const int k = k0 + kk;
       double best = -1.0;
       int bi = M;
-      for (int i = k + t; i < M; i += kGjThreads) {
+      for (int i = t; i < M; i += kGjThreads) {
+        if (i < k) continue;
         const double v = fabs(P[kk * M + i]);
         if (v > best) { best = v; bi = i; }
       }
-      redv[t] = best;
-      redi[t] = bi;
-      __syncthreads();
-      for (int sft = kGjThreads / 2; sft > 0; sft >>= 1) {
-        if (t < sft && (redv[t + sft] > redv[t] || (redv[t + sft] == redv[t] && redi[t + sft] < redi[t]))) {
-          redv[t] = redv[t + sft];
-          redi[t] = redi[t + sft];
-        }
-        __syncthreads();
+      for (int o = 16; o > 0; o >>= 1) {   // first largest within the warp
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
       }
-      const int pv = redi[0];
+      if (lane == 0) { wbest[warp] = best; wbi[warp] = bi; }
+      __syncthreads();
+      int pv = wbi[0];
+      double pb = wbest[0];
+      for (int w = 1; w < kGjThreads / 32; w++)
+        if (wbest[w] > pb || (wbest[w] == pb && wbi[w] < pv)) { pb = wbest[w]; pv = wbi[w]; }
       if (t == 0) perm[k] = pv;
-      if (pv != k && t < nb) {
-        const double a = P[t * M + k];
-        P[t * M + k] = P[t * M + pv];
-        P[t * M + pv] = a;
-      }
-      __syncthreads();
-      const double piv = P[kk * M + k];
+      // read phase: the pivot row (old row pv, scaled) to sRk, and the old row
+      // k, which moves to row pv, to sOk
+      const double piv = P[kk * M + pv];
       if (piv == 0.0) bad = bad ? bad : k + 1;
       const double d = (piv != 0.0) ? 1.0 / piv : 0.0;
-      if (t < nb) rowk[t] = (t == kk) ? d : P[t * M + k] * d;
+      if (t < nb) {
+        sRk[t] = (t == kk) ? d : P[t * M + pv] * d;
+        sOk[t] = P[t * M + k];
+      }
       __syncthreads();
+      // write phase
       for (int i = t; i < M; i += kGjThreads) {
         if (i == k) {
-          for (int c = 0; c < nb; c++) P[c * M + k] = rowk[c];
+          for (int c = 0; c < nb; c++) P[c * M + k] = sRk[c];
+        } else if (i == pv) {   // (only reached when pv != k) the old row k, eliminated
+          const double f = sOk[kk];
+          for (int c = 0; c < nb; c++) P[c * M + i] = (c == kk) ? -f * d : sOk[c] - f * sRk[c];
         } else {
           const double f = P[kk * M + i];
-          for (int c = 0; c < nb; c++) P[c * M + i] = (c == kk) ? -f * d : P[c * M + i] - f * rowk[c];
+          for (int c = 0; c < nb; c++) P[c * M + i] = (c == kk) ? -f * d : P[c * M + i] - f * sRk[c];
         }
       }
-      __syncthreads();
-    }
-    for (int e = t; e < nb * M; e += kGjThreads) A[(size_t)k0 * M + e] = P[e];
-    // the other columns: the panel's row swaps, then rows k0.. to Y and zero
-    for (int j = t; j < M; j += kGjThreads) {
-      if (j >= k0 && j < k0 + nb) continue;
-      double *col = A + (size_t)j * M;
-      for (int kk = 0; kk < nb; kk++) {
-        const int k = k0 + kk, pv = perm[k];
-        if (pv != k) {
-          const double a = col[k];
-          col[k] = col[pv];
-          col[pv] = a;
-        }
-      }
-      for (int kk = 0; kk < nb; kk++) {
-        Y[(size_t)j * NB + kk] = col[k0 + kk];
-        col[k0 + kk] = 0.0;
-      }
+      __syncthreads();   // sRk/sOk are rewritten by the next step; its search reads own rows only
     }
     __syncthreads();
-    // A(:, rest) += P * Y, tiles of 64 columns x 64 rows; thread: one row, 16 columns
-    const int rl = t % 64, cg = t / 64;
-    for (int jt = 0; jt < M; jt += 64) {
+    if (rank == 0)
+      for (int e = t; e < nb * M; e += kGjThreads) A[(size_t)k0 * M + e] = P[e];
+    // the panel's row interchanges as one gather: row r takes the value of row sSrc of the same column
+    if (t == 0) {
+      int cnt = 0;
+      auto add = [&](int r) {
+        for (int q = 0; q < cnt; q++)
+          if (sPos[q] == r) return;
+        sPos[cnt] = r;
+        sSrc[cnt] = r;
+        cnt++;
+      };
+      for (int kk = 0; kk < nb; kk++) {
+        add(k0 + kk);
+        add(perm[k0 + kk]);
+      }
+      for (int kk = 0; kk < nb; kk++) {   // replay the swaps on the source indices
+        const int k = k0 + kk, pv = perm[k];
+        int qa = 0, qb = 0;
+        for (int q = 0; q < cnt; q++) {
+          if (sPos[q] == k) qa = q;
+          if (sPos[q] == pv) qb = q;
+        }
+        const int tmp = sSrc[qa];
+        sSrc[qa] = sSrc[qb];
+        sSrc[qb] = tmp;
+      }
+      sCnt = cnt;
+    }
+    __syncthreads();
+    // this CTA's columns: gather the interchanged rows, rows k0.. to Y, zero them (a warp per column)
+    const int cnt = sCnt;
+    for (int jt = 64 * rank; jt < M; jt += 64 * CS)
+      for (int j = jt + warp; j < min(M, jt + 64); j += kGjThreads / 32) {
+        if (j >= k0 && j < k0 + nb) continue;
+        double *col = A + (size_t)j * M;
+        double v = 0.0;
+        int r = -1;
+        if (lane < cnt) {
+          r = sPos[lane];
+          v = col[sSrc[lane]];
+        }
+        __syncwarp();
+        if (lane < cnt) {
+          if (r >= k0 && r < k0 + nb) {
+            Y[(size_t)j * NB + (r - k0)] = v;
+            col[r] = 0.0;
+          } else {
+            col[r] = v;
+          }
+        }
+      }
+    __syncthreads();
+    // A(:, j) += P * Y(:, j) over this CTA's 64-column tiles; thread: 4 rows x 4 columns
+    const int tr = t % 16, tc = t / 16;
+    for (int jt = 64 * rank; jt < M; jt += 64 * CS) {
       for (int e = t; e < 64 * NB; e += kGjThreads) {
         const int jl = e / NB, kk = e % NB, j = jt + jl;
         const bool ok = j < M && (j < k0 || j >= k0 + nb) && kk < nb;
         Yt[e] = ok ? Y[(size_t)j * NB + kk] : 0.0;
       }
       __syncthreads();
-      for (int it = 0; it < M; it += 64) {
-        const int i = it + rl;
-        if (i < M) {
-          double acc[16];
+      // row tiles, the next tile's A values loaded while the current one is computed
+      auto load_tile = [&](int it, double (&v)[4][4]) {
+        const int i0 = it + 4 * tr;
+        const bool in = i0 < M, full = i0 + 4 <= M;   // M is even: a row quad is full or holds two rows
 #pragma unroll
-          for (int c = 0; c < 16; c++) {
-            const int j = jt + cg + 4 * c;
-            acc[c] = (j < M) ? A[(size_t)j * M + i] : 0.0;
-          }
-          for (int kk = 0; kk < nb; kk++) {
-            const double w = P[kk * M + i];
-#pragma unroll
-            for (int c = 0; c < 16; c++) acc[c] += w * Yt[(cg + 4 * c) * NB + kk];
-          }
-#pragma unroll
-          for (int c = 0; c < 16; c++) {
-            const int j = jt + cg + 4 * c;
-            if (j < M && (j < k0 || j >= k0 + nb)) A[(size_t)j * M + i] = acc[c];
+        for (int c = 0; c < 4; c++) {
+          const int j = jt + 4 * tc + c;
+          if (in && j < M) {
+            const double2 *src = reinterpret_cast<const double2 *>(A + (size_t)j * M + i0);
+            const double2 lo = src[0], hi = full ? src[1] : make_double2(0.0, 0.0);
+            v[c][0] = lo.x; v[c][1] = lo.y; v[c][2] = hi.x; v[c][3] = hi.y;
+          } else {
+            v[c][0] = v[c][1] = v[c][2] = v[c][3] = 0.0;
           }
         }
+      };
+      double acc[4][4], nxt[4][4];
+      load_tile(0, acc);
+      for (int it = 0; it < M; it += 64) {
+        const int i0 = it + 4 * tr;
+        if (it + 64 < M) load_tile(it + 64, nxt);
+        if (i0 < M) {
+          const bool full = i0 + 4 <= M;
+          for (int kk = 0; kk < nb; kk++) {
+            const double2 *pw = reinterpret_cast<const double2 *>(P + (size_t)kk * M + i0);
+            const double2 wlo = pw[0], whi = full ? pw[1] : make_double2(0.0, 0.0);
+            const double w[4] = {wlo.x, wlo.y, whi.x, whi.y};
+            double y[4];
+#pragma unroll
+            for (int c = 0; c < 4; c++) y[c] = Yt[(4 * tc + c) * NB + kk];
+#pragma unroll
+            for (int c = 0; c < 4; c++)
+#pragma unroll
+              for (int r = 0; r < 4; r++) acc[c][r] += w[r] * y[c];
+          }
+#pragma unroll
+          for (int c = 0; c < 4; c++) {
+            const int j = jt + 4 * tc + c;
+            if (j < M && (j < k0 || j >= k0 + nb)) {
+              double2 *dst = reinterpret_cast<double2 *>(A + (size_t)j * M + i0);
+              dst[0] = make_double2(acc[c][0], acc[c][1]);
+              if (full) dst[1] = make_double2(acc[c][2], acc[c][3]);
+            }
+          }
+        }
+#pragma unroll
+        for (int c = 0; c < 4; c++)
+#pragma unroll
+          for (int r = 0; r < 4; r++) acc[c][r] = nxt[c][r];
       }
       __syncthreads();
     }
   }
   // the pending column interchanges, as an index: stored column c multiplies input component colSrc[c]
   __syncthreads();
-  if (t == 0) {
+  if (rank == 0 && t == 0) {
     // sigma: final column j = stored column sigma[j], built by replaying the swaps in reverse
     int *cs = colSrc + 2 * bStart[b];
     for (int c = 0; c < M; c++) cs[c] = c;   // cs temporarily holds sigma
@@ -258,6 +348,7 @@ pc_gj_invert_kernel(const int *__restrict__ list, const int *__restrict__ bStart
     for (int c = 0; c < M; c++) cs[c] = perm[c];
     info[b] = bad;
   }
+  if (CS > 1) cooperative_groups::this_cluster().sync();   // no CTA leaves while others may still read
 }
 
 // x = blockdiag(inv) * b, block b gathers its pot/dpdn halves
@@ -434,21 +525,51 @@ static bool factor_cusolver(Context &c, PrecondDev &p, const std::vector<int> &b
 #ifndef FB_PC_GJ_MAXM
 #define FB_PC_GJ_MAXM 3200
 #endif
+// CTAs per block for blocks of 385-768 rows (1 or 2; 1600+ rows use 8)
+#ifndef FB_PC_GJ_MIDCS
+#define FB_PC_GJ_MIDCS 2
+#endif
 constexpr int kGjMaxM = 3200;
 
-template <int NB>
-static size_t gj_smem(int maxM) {
-  return (size_t)NB * maxM * sizeof(double) + 64 * NB * sizeof(double) + (size_t)maxM * sizeof(int);
+template <int NB, int CS>
+static bool launch_gj_t(int nList, int maxM, cudaStream_t st, const int *d_list, PrecondDev &p, const long long *d_yOff,
+                        double *d_y, int *d_info) {
+  const size_t shm = gj_smem_bytes<NB>(maxM);
+  FB_CUDA(cudaFuncSetAttribute(pc_gj_invert_kernel<NB, CS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(nList * CS));
+  cfg.blockDim = dim3(kGjThreads);
+  cfg.dynamicSmemBytes = shm;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = CS;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  FB_CUDA(cudaLaunchKernelEx(&cfg, pc_gj_invert_kernel<NB, CS>, d_list, (const int *)p.d_start,
+                             (const int *)p.d_size, (const long long *)p.d_off, d_yOff, p.d_inv, d_y, p.d_colSrc,
+                             d_info));
+  return true;
+}
+
+static bool launch_gj(int nb, int cs, int nList, int maxM, cudaStream_t st, const int *d_list, PrecondDev &p,
+                      const long long *d_yOff, double *d_y, int *d_info) {
+  if (nb == 16 && cs == 1) return launch_gj_t<16, 1>(nList, maxM, st, d_list, p, d_yOff, d_y, d_info);
+  if (nb == 16 && cs == 2) return launch_gj_t<16, 2>(nList, maxM, st, d_list, p, d_yOff, d_y, d_info);
+  if (nb == 16 && cs == 8) return launch_gj_t<16, 8>(nList, maxM, st, d_list, p, d_yOff, d_y, d_info);
+  return launch_gj_t<8, 8>(nList, maxM, st, d_list, p, d_yOff, d_y, d_info);
 }
 
 // Gauss-Jordan inversion of every block in p.d_inv (assembled there), size
 // classes on their own streams so the large blocks start at once.
 static bool factor_hybrid(Context &c, PrecondDev &p) {
   cudaStream_t s = c.stream;
-  struct Cls { int lo, hi, nb; };
+  struct Cls { int lo, hi, nb, cs; };   // rows, panel width, CTAs per block
   const int cut = std::min(FB_PC_GJ_MAXM, kGjMaxM);
-  const Cls cls[4] = {{0, std::min(384, cut), 16}, {std::min(384, cut), std::min(768, cut), 16},
-                      {std::min(768, cut), std::min(1600, cut), 16}, {std::min(1600, cut), cut, 8}};
+  const Cls cls[4] = {{0, std::min(384, cut), 16, 1}, {std::min(384, cut), std::min(768, cut), 16, FB_PC_GJ_MIDCS},
+                      {std::min(768, cut), std::min(1600, cut), 16, 8}, {std::min(1600, cut), cut, 8, 8}};
   std::vector<int> big;
   for (int b = 0; b < p.nBlocks; b++)
     if (2 * p.hSize[b] > cut) big.push_back(b);
@@ -493,16 +614,9 @@ static bool factor_hybrid(Context &c, PrecondDev &p) {
          cudaStreamWaitEvent(st, evL, 0) == cudaSuccess;
     if (evL) cudaEventDestroy(evL);
     if (!ok) break;
-    if (k.nb == 16) {
-      const size_t shm = gj_smem<16>(maxM);
-      cudaFuncSetAttribute(pc_gj_invert_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-      pc_gj_invert_kernel<16><<<(unsigned)list.size(), kGjThreads, shm, st>>>(
-          d_list, p.d_start, p.d_size, p.d_off, d_yOff, p.d_inv, d_y, p.d_colSrc, d_info);
-    } else {
-      const size_t shm = gj_smem<8>(maxM);
-      cudaFuncSetAttribute(pc_gj_invert_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-      pc_gj_invert_kernel<8><<<(unsigned)list.size(), kGjThreads, shm, st>>>(
-          d_list, p.d_start, p.d_size, p.d_off, d_yOff, p.d_inv, d_y, p.d_colSrc, d_info);
+    if (!launch_gj(k.nb, k.cs, (int)list.size(), maxM, st, d_list, p, d_yOff, d_y, d_info)) {
+      ok = false;
+      break;
     }
     c.launches += 1;
     ok = cudaGetLastError() == cudaSuccess;
