@@ -155,12 +155,12 @@ bool op_apply(Context &c, int part, double alpha, const double *sgm, double beta
 }
 
 // y = alpha*(D - K)x + beta*y, D = diag(s1*A, s2*A) (MtVmain); adjoint: (D - K^T)
-bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y, bool adjoint) {
+bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y, bool adjoint, bool fp64) {
   double s1 = (1.0 + c.epsilon) / 2.0 * alpha;
   double s2 = (1.0 + 1.0 / c.epsilon) / 2.0 * alpha;
   if (!launch_far_upward(c, x, adjoint)) return false;
   if (!launch_l2p(c, -alpha, beta, y, x, s1, s2, adjoint)) return false;
-  if (!launch_near(c, x, -alpha, y, adjoint)) return false;
+  if (!launch_near(c, x, -alpha, y, adjoint, fp64)) return false;
   return true;
 }
 
@@ -440,6 +440,28 @@ int fabipb_b200_pass_times(void *ctx, const double *x, int reps, double *ms, int
   }
   for (int i = 0; i < 6; i++) ms[i] = acc[i] / reps;
   return 1;
+}
+
+int fabipb_b200_solve_refined(void *ctx, const double *b, double *x, int restart, int maxit, double tol_inner,
+                              double tol, int max_outer, int *outer, int *iters, double *resid, int *info,
+                              int on_device) {
+  if (!valid_ctx(ctx) || b == nullptr || x == nullptr || restart < 1 || maxit < 1 || max_outer < 0) {
+    set_error("fabipb_b200_solve_refined: invalid arguments");
+    return 0;
+  }
+  Context *c = (Context *)ctx;
+  int ou = 0, it = 0, inf = 0;
+  double res = 0.0;
+  StageTimer tm("solve", c->stream);
+  int ok = with_vectors(c, b, x, true, on_device, [&](const double *bd, double *xd) {
+    return refined_solve(*c, bd, xd, restart, maxit, tol_inner, tol, max_outer, &ou, &it, &res, &inf);
+  });
+  tm.mark("refined");
+  if (outer) *outer = ou;
+  if (iters) *iters = it;
+  if (resid) *resid = res;
+  if (info) *info = inf;
+  return ok;
 }
 
 int fabipb_b200_apply_adjoint(void *ctx, int part, double alpha, const double *lam, double beta, double *out,

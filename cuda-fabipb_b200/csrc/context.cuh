@@ -45,6 +45,8 @@ struct Context {
   int *d_spOff = nullptr, *d_spSrc = nullptr;  // CSR by destination panel
   double4 *d_spK = nullptr;                    // exact minus one-point coefficient
   double4 *d_spKT = nullptr;                   // the same for the transposed operator (built on first use)
+  void *d_tgtP64 = nullptr, *d_tgtN64 = nullptr;   // FP64 records of a mixed context (refinement residuals)
+  void *d_srcA64 = nullptr, *d_srcB64 = nullptr;
 
   // ---- FMM ----------------------------------------------------------
   int P = 0, NM = 0;                       // max order, nmom(max order)
@@ -72,6 +74,7 @@ struct Context {
 
   // ---- scratch vectors for host-pointer calls ------------------------
   double *d_x = nullptr, *d_y = nullptr, *d_w = nullptr;
+  double *d_refR = nullptr, *d_refD = nullptr, *d_refZ = nullptr;   // iterative refinement (first use)
 
   // ---- charges, RHS, energy -------------------------------------------
   std::vector<int> chargeOrders;           // per-level charge-tree order (host policy)
@@ -99,7 +102,8 @@ bool setup_charges(Context &c, int m, const double *pos, const double *q);
 
 // device operators on device vectors (stream-ordered, no synchronisation)
 // near:  out += coef * K_near * sgm
-bool launch_near(Context &c, const double *sgm, double coef, double *out, bool adjoint = false);
+// (fp64: the FP64 P2P in a mixed context, for refinement residuals)
+bool launch_near(Context &c, const double *sgm, double coef, double *out, bool adjoint = false, bool fp64 = false);
 // upward pass + interaction + downward pass: leaves local expansions in d_lec
 // (adjoint: the transposed far operator's upward half, see fmm.cu)
 // (marks: 4 events recorded after Q2M, M2M, M2L and L2L, for pass timing)
@@ -115,6 +119,9 @@ bool precond_setup(Context &c, int mode);
 bool precond_apply(Context &c, const double *b, double *x, bool adjoint = false);
 bool gmres_solve(Context &c, const double *b, double *x, int restart, int maxit, double tol,
                  int *iters, double *resid, int *info, bool adjoint = false);
+// iterative refinement: FP64 residuals, corrections by GMRES on the context's operator
+bool refined_solve(Context &c, const double *b, double *x, int restart, int maxit, double tolInner, double tol,
+                   int maxOuter, int *outer, int *iters, double *resid, int *info);
 void free_charges(Context &c);
 void free_precond(Context &c);
 void free_adjoint(Context &c);
@@ -127,6 +134,7 @@ int create_context(const fabipb_b200_params *p, int n, const double *vtx, const 
 // composite operators (device vectors)
 // (adjoint: the transposed operator K^T, and (D - K)^T)
 bool op_apply(Context &c, int part, double alpha, const double *sgm, double beta, double *pot, bool adjoint = false);
-bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y, bool adjoint = false);
+bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y, bool adjoint = false,
+               bool fp64 = false);
 
 }  // namespace fb

@@ -431,19 +431,36 @@ bool setup_near(Context &c) {
 }
 
 template <typename T, bool ADJ>
-static void launch_near_t(Context &c, const double *sgm, double coef, double *out) {
+static void launch_near_t(Context &c, const void *tgtP, const void *tgtN, void *srcA, void *srcB, const double *sgm,
+                          double coef, double *out) {
   typedef typename Vec4<T>::t V;
   const int n = c.n;
   cudaStream_t s = c.stream;
   const double kap = c.prm.kappa, eps = c.epsilon;
   const unsigned grid = ceil_div(c.nWork, kNearWarps);
   const double kexp = sizeof(T) == 4 ? -kap * 1.4426950408889634 : -kap;   // float: exp2 argument
-  near_pack_kernel<T><<<ceil_div(n, 256), 256, 0, s>>>(n, (const V *)c.d_tgtP, (const V *)c.d_tgtN, c.d_area, sgm,
-                                                       (V *)c.d_srcA, (V *)c.d_srcB);
+  near_pack_kernel<T><<<ceil_div(n, 256), 256, 0, s>>>(n, (const V *)tgtP, (const V *)tgtN, c.d_area, sgm, (V *)srcA,
+                                                       (V *)srcB);
   near_apply_kernel<T, ADJ><<<grid, kNearWarps * 32, 0, s>>>(
-      c.nWork, c.d_work, c.d_leafStart, c.d_leafCount, c.d_nearOff, c.d_nearSrc, c.d_leafCtr, (const V *)c.d_tgtP,
-      (const V *)c.d_tgtN, (const V *)c.d_srcA, (const V *)c.d_srcB, c.d_spOff, c.d_spSrc,
-      ADJ ? c.d_spKT : c.d_spK, sgm, c.d_area, n, (T)kap, (T)kexp, (T)eps, (T)(1.0 / eps), (T)(kap * kap), coef, out);
+      c.nWork, c.d_work, c.d_leafStart, c.d_leafCount, c.d_nearOff, c.d_nearSrc, c.d_leafCtr, (const V *)tgtP,
+      (const V *)tgtN, (const V *)srcA, (const V *)srcB, c.d_spOff, c.d_spSrc, ADJ ? c.d_spKT : c.d_spK, sgm,
+      c.d_area, n, (T)kap, (T)kexp, (T)eps, (T)(1.0 / eps), (T)(kap * kap), coef, out);
+}
+
+// FP64 records in a mixed context, for the FP64 residuals of iterative
+// refinement (built on first use)
+static bool setup_near_fp64(Context &c) {
+  if (c.d_tgtP64) return true;
+  const int n = c.n;
+  const size_t vb = sizeof(double4) * (size_t)n;
+  if (!c.arena.alloc(&c.d_tgtP64, vb) || !c.arena.alloc(&c.d_tgtN64, vb) || !c.arena.alloc(&c.d_srcA64, vb) ||
+      !c.arena.alloc(&c.d_srcB64, vb))
+    return false;
+  near_targets_kernel<double><<<ceil_div(n, 256), 256, 0, c.stream>>>(n, c.d_vtx, c.d_nrm, c.d_area, c.d_leafOfPanel,
+                                                                      c.d_leafCtr, (double4 *)c.d_tgtP64,
+                                                                      (double4 *)c.d_tgtN64);
+  FB_CUDA(cudaGetLastError());
+  return true;
 }
 
 // Transposed special-pair table: entry (X, Y) of row X holds the correction
@@ -485,14 +502,18 @@ static bool setup_near_adjoint(Context &c) {
   return true;
 }
 
-bool launch_near(Context &c, const double *sgm, double coef, double *out, bool adjoint) {
+bool launch_near(Context &c, const double *sgm, double coef, double *out, bool adjoint, bool fp64) {
   if (adjoint && !setup_near_adjoint(c)) return false;
-  if (c.mixed) {
-    if (adjoint) launch_near_t<float, true>(c, sgm, coef, out);
-    else launch_near_t<float, false>(c, sgm, coef, out);
+  if (c.mixed && fp64) {
+    if (!setup_near_fp64(c)) return false;
+    if (adjoint) launch_near_t<double, true>(c, c.d_tgtP64, c.d_tgtN64, c.d_srcA64, c.d_srcB64, sgm, coef, out);
+    else launch_near_t<double, false>(c, c.d_tgtP64, c.d_tgtN64, c.d_srcA64, c.d_srcB64, sgm, coef, out);
+  } else if (c.mixed) {
+    if (adjoint) launch_near_t<float, true>(c, c.d_tgtP, c.d_tgtN, c.d_srcA, c.d_srcB, sgm, coef, out);
+    else launch_near_t<float, false>(c, c.d_tgtP, c.d_tgtN, c.d_srcA, c.d_srcB, sgm, coef, out);
   } else {
-    if (adjoint) launch_near_t<double, true>(c, sgm, coef, out);
-    else launch_near_t<double, false>(c, sgm, coef, out);
+    if (adjoint) launch_near_t<double, true>(c, c.d_tgtP, c.d_tgtN, c.d_srcA, c.d_srcB, sgm, coef, out);
+    else launch_near_t<double, false>(c, c.d_tgtP, c.d_tgtN, c.d_srcA, c.d_srcB, sgm, coef, out);
   }
   c.launches += 2;
   FB_CUDA(cudaGetLastError());

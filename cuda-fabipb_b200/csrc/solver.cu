@@ -998,3 +998,59 @@ bool gmres_solve(Context &c, const double *b, double *x, int restrt, int maxit, 
 }
 
 }  // namespace fb
+
+namespace fb {
+
+__global__ void add_kernel(long long n, const double *__restrict__ d, double *x) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    x[i] += d[i];
+}
+
+// Mixed-precision iterative refinement: the residual r = b - A x is formed
+// with the FP64 operator (in a mixed context the FP64 near-field P2P), the
+// correction A d = r is solved by GMRES with the context's own operator (the
+// FP32 P2P in a mixed context) to the relative tolerance tolInner from d = 0,
+// and x += d, until ||P^-1 r|| / ||b|| <= tol (the reference GMRES measure,
+// src/gmres.c:225-232).  The outer residuals and updates are FP64 vectors.
+bool refined_solve(Context &c, const double *b, double *x, int restart, int maxit, double tolInner, double tol,
+                   int maxOuter, int *outer, int *iters, double *resid, int *info) {
+  FB_CHECK(c.pc != nullptr, "call fabipb_b200_precond_setup before solving (mode -1 for none)");
+  const long long n2 = 2LL * c.n;
+  if (!c.d_refR && (!c.arena.alloc_n(&c.d_refR, (size_t)n2) || !c.arena.alloc_n(&c.d_refD, (size_t)n2) ||
+                    !c.arena.alloc_n(&c.d_refZ, (size_t)n2)))
+    return false;
+  double bn = 0.0;
+  if (!dot_to_host(c, n2, b, b, &bn)) return false;
+  bn = sqrt(bn);
+  if (bn == 0.0) bn = 1.0;
+  *outer = 0;
+  *iters = 0;
+  *info = 0;
+  for (;;) {
+    FB_CUDA(cudaMemcpyAsync(c.d_refR, b, n2 * sizeof(double), cudaMemcpyDeviceToDevice, c.stream));
+    if (!op_matvec(c, -1.0, x, 1.0, c.d_refR, false, true)) return false;
+    if (!precond_apply(c, c.d_refR, c.d_refZ)) return false;
+    double zn = 0.0;
+    if (!dot_to_host(c, n2, c.d_refZ, c.d_refZ, &zn)) return false;
+    *resid = sqrt(zn) / bn;
+    if (*resid <= tol || !(*resid == *resid)) {
+      if (!(*resid == *resid)) *info = 2;
+      return true;
+    }
+    if (*outer >= maxOuter || *iters >= maxit) {
+      *info = 1;
+      return true;
+    }
+    ++(*outer);
+    FB_CUDA(cudaMemsetAsync(c.d_refD, 0, n2 * sizeof(double), c.stream));
+    int it = 0, inf = 0;
+    double res = 0.0;
+    if (!gmres_solve(c, c.d_refR, c.d_refD, restart, maxit - *iters, tolInner, &it, &res, &inf)) return false;
+    *iters += it;
+    add_kernel<<<kRedBlocks * 4, 256, 0, c.stream>>>(n2, c.d_refD, x);
+    c.launches += 1;
+    FB_CUDA(cudaGetLastError());
+  }
+}
+
+}  // namespace fb

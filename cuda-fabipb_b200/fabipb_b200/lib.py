@@ -64,6 +64,8 @@ def load():
     L.fabipb_b200_apply.argtypes = [vp, C.c_int, C.c_double, vp, C.c_double, vp, C.c_int]
     L.fabipb_b200_matvec.argtypes = [vp, C.c_double, vp, C.c_double, vp, C.c_int]
     L.fabipb_b200_energy_weights.argtypes = [vp, vp, C.c_int]
+    L.fabipb_b200_solve_refined.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int, vp, vp,
+                                            vp, vp, C.c_int]
     L.fabipb_b200_pass_times.argtypes = [vp, vp, C.c_int, vp, C.c_int]
     L.fabipb_b200_forward.argtypes = [vp, C.c_int, C.c_int, C.c_double, vp, vp, vp, vp]
     L.fabipb_b200_backward.argtypes = [vp, C.c_double, C.c_int, C.c_int, C.c_double, vp, vp, vp, vp, vp, C.c_int]
@@ -236,6 +238,20 @@ class Surface:
             x = np.ascontiguousarray(x, dtype=np.float64)
         _check(load().fabipb_b200_pass_times(self.h, _ptr(x), int(reps), _ptr(ms), int(on_device)), "pass_times")
         return dict(zip(self.PASSES, ms.tolist()))
+
+    def solve_refined(self, b, x0, restart=10, maxit=200, tol_inner=1e-5, tol=1e-10, max_outer=20):
+        """Iterative refinement (FP64 residuals, corrections by GMRES on this
+        context's operator); returns (x, outer, iters, resid, info)."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.array(x0, dtype=np.float64)
+        ou = np.zeros(1, np.int32)
+        it = np.zeros(1, np.int32)
+        res = np.zeros(1)
+        info = np.zeros(1, np.int32)
+        _check(load().fabipb_b200_solve_refined(self.h, _ptr(b), _ptr(x), int(restart), int(maxit), float(tol_inner),
+                                                float(tol), int(max_outer), _ptr(ou), _ptr(it), _ptr(res), _ptr(info),
+                                                0), "solve_refined")
+        return x, int(ou[0]), int(it[0]), float(res[0]), int(info[0])
 
     def energy_weights(self):
         """Direct energy weights e (2N, tree order): energy_raw = e . sigma."""

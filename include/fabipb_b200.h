@@ -89,6 +89,16 @@ int fabipb_b200_apply(void *ctx, int part, double alpha, const double *sgm, doub
 /* y = alpha*(D - K)x + beta*y  (MtVmain, src/fabipb.c:1237) */
 int fabipb_b200_matvec(void *ctx, double alpha, const double *x, double beta, double *y,
                        int on_device);
+/* iterative refinement (no counterpart in the reference): FP64 residuals
+   r = b - A x (in a mixed context through the FP64 near-field P2P), each
+   correction solved by GMRES with the context's operator (the FP32 P2P in a
+   mixed context) to the relative tolerance tol_inner from zero, x += d,
+   until ||P^-1 r|| / ||b|| <= tol.  x holds the initial guess.  *outer =
+   corrections made, *iters = inner GMRES iterations in total (at most
+   maxit), *info = 0 converged, 1 out of iterations, 2 NaN. */
+int fabipb_b200_solve_refined(void *ctx, const double *b, double *x, int restart, int maxit, double tol_inner,
+                              double tol, int max_outer, int *outer, int *iters, double *resid, int *info,
+                              int on_device);
 /* stage report (the counterpart of the reference's -B=1 stage times, no
    counterpart in its ABI): runs the matvec passes reps times with CUDA events
    between them and returns the mean milliseconds per pass in ms[6]:
