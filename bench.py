@@ -261,7 +261,9 @@ def solve_report(pan, ch, opts, device, st):
     from fabipb_b200 import lib
     out = {}
     kcal = 2.0 * np.pi * 332.0716
-    for tag, prec in (("mixed", lib.MIXED), ("fp64", lib.FP64)):
+    # each precision runs twice and the second run is reported: the first
+    # pays the one-time loading of the kernels it is the first to use
+    for tag, prec in (("mixed", lib.MIXED), ("mixed", lib.MIXED), ("fp64", lib.FP64), ("fp64", lib.FP64)):
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         torch.cuda.synchronize()
         w0 = time.perf_counter()
@@ -279,9 +281,19 @@ def solve_report(pan, ch, opts, device, st):
         ev[3].record(st)
         torch.cuda.synchronize()
         wall = time.perf_counter() - w0
+        # iterative refinement to the same tolerance (FP64 residuals; in the
+        # mixed context the corrections use the FP32 near field)
+        rf = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        rf[0].record(st)
+        xr, outer, itr, resr, infr = s.solve_refined(b, b.copy(), restart=opts["restart"], maxit=200,
+                                                     tol_inner=opts["tol"], tol=opts["tol"], max_outer=10)
+        rf[1].record(st)
+        torch.cuda.synchronize()
+        refined = {"gmres_s": rf[0].elapsed_time(rf[1]) / 1000.0, "outer": outer, "iterations": itr,
+                   "residual_fp64": resr, "info": infr, "energy_kcal_mol": s.energy_raw(xr) * kcal}
         out[tag] = {"gmres_s": ev[1].elapsed_time(ev[2]) / 1000.0, "setup_s": ev[0].elapsed_time(ev[1]) / 1000.0,
                     "energy_s": ev[2].elapsed_time(ev[3]) / 1000.0, "wall_s": wall, "iterations": it,
-                    "residual": res, "info": info, "energy_kcal_mol": e}
+                    "residual": res, "info": info, "energy_kcal_mol": e, "refined": refined}
         # gradients of the (direct) energy: forward = RHS + GMRES + energy,
         # backward = adjoint GMRES + dE/dq, dE/dx of every charge
         ag = [torch.cuda.Event(enable_timing=True) for _ in range(3)]

@@ -43,6 +43,7 @@ struct PrecondDev {
   int nTiles = 0;
   long long *d_off = nullptr;
   double *d_inv = nullptr;
+  float *d_invF = nullptr;   // mixed contexts: the inverses stored in FP32 (applied with FP64 sums)
   int maxM = 0;
   // GMRES workspace
   int restart = 0;
@@ -400,19 +401,20 @@ pc_apply_kernel(int n, const int2 *__restrict__ tiles, const int *__restrict__ b
 // Transposed block-diagonal apply (adjoint solves): output c of a block is
 // column c of its inverse dotted with the block's input, one warp per output,
 // lanes over the (contiguous) column; tiles as for pc_apply_kernel.
+template <typename TI>
 __global__ void __launch_bounds__(kPcRows * kPcSplit)
 pc_apply_t_kernel(int n, const int2 *__restrict__ tiles, const int *__restrict__ bStart, const int *__restrict__ bSize,
-                  const long long *__restrict__ bOff, const int *__restrict__ colSrc, const double *__restrict__ inv,
+                  const long long *__restrict__ bOff, const int *__restrict__ colSrc, const TI *__restrict__ inv,
                   const double *__restrict__ rhs, double *x) {
   const int2 tl = tiles[blockIdx.x];
   const int b = tl.x, c0 = tl.y;
   const int hm = bSize[b], st = bStart[b], M = 2 * hm;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  const double *Ib = inv + bOff[b];
+  const TI *Ib = inv + bOff[b];
   for (int c = c0 + warp; c < min(M, c0 + kPcRows); c += nw) {
-    const double *col = Ib + (size_t)c * M;
+    const TI *col = Ib + (size_t)c * M;
     double y = 0.0;
-    for (int r = lane; r < M; r += 32) y += col[r] * ((r < hm) ? rhs[st + r] : rhs[n + st + r - hm]);
+    for (int r = lane; r < M; r += 32) y += (double)col[r] * ((r < hm) ? rhs[st + r] : rhs[n + st + r - hm]);
     for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
     if (lane == 0) {
       const int g = colSrc[2 * (size_t)st + c];   // stored column c is output component g
@@ -646,6 +648,11 @@ static bool factor_hybrid(Context &c, PrecondDev &p) {
   return true;
 }
 
+__global__ void to_float_kernel(long long n, const double *__restrict__ a, float *b) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
 bool precond_setup(Context &c, int mode) {
   free_precond(c);
   c.pc = new PrecondDev();
@@ -674,8 +681,11 @@ bool precond_setup(Context &c, int mode) {
   StageTimer tm("precond_setup", s);
   if (!p.arena.upload(&p.d_start, p.hStart, s) || !p.arena.upload(&p.d_size, p.hSize, s) ||
       !p.arena.upload(&p.d_tiles, tiles, s) || !p.arena.upload(&p.d_off, p.hOff, s) ||
-      !p.arena.alloc_n(&p.d_inv, (size_t)off) || !p.arena.alloc_n(&p.d_colSrc, 2 * (size_t)c.n))
+      !p.arena.alloc_n(&p.d_colSrc, 2 * (size_t)c.n))
     return false;
+  // the inversion works in FP64; a mixed context keeps an FP32 copy only
+  if (c.mixed) FB_CUDA(cudaMalloc((void **)&p.d_inv, (size_t)off * sizeof(double)));
+  else if (!p.arena.alloc_n(&p.d_inv, (size_t)off)) return false;
   const double s1 = (1.0 + c.epsilon) / 2.0, s2 = (1.0 + 1.0 / c.epsilon) / 2.0;
   dim3 grid(64, p.nBlocks);
   pc_assemble_kernel<<<grid, 128, 0, s>>>(p.nBlocks, p.d_start, p.d_size, p.d_off, c.d_vtx, c.d_nrm, c.d_area,
@@ -683,8 +693,18 @@ bool precond_setup(Context &c, int mode) {
   c.launches += 1;
   FB_CUDA(cudaGetLastError());
   tm.mark("assemble");
-  const bool ok = factor_hybrid(c, p);
+  bool ok = factor_hybrid(c, p);
   tm.mark("factor_invert");
+  if (c.mixed) {
+    if (ok) ok = p.arena.alloc_n(&p.d_invF, (size_t)off);
+    if (ok) {
+      to_float_kernel<<<1184, 256, 0, s>>>(off, p.d_inv, p.d_invF);
+      ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(s) == cudaSuccess;
+    }
+    cudaFree(p.d_inv);
+    p.d_inv = nullptr;
+    FB_CHECK(ok, "preconditioner FP32 copy failed: %s", get_error());
+  }
   return ok;
 }
 
@@ -692,11 +712,19 @@ bool precond_apply(Context &c, const double *b, double *x, bool adjoint) {
   FB_CHECK(c.pc != nullptr, "preconditioner not set up");
   PrecondDev &p = *c.pc;
   if (p.mode == 2 && adjoint) {
-    pc_apply_t_kernel<<<p.nTiles, kPcRows * kPcSplit, 0, c.stream>>>(c.n, p.d_tiles, p.d_start, p.d_size, p.d_off,
-                                                                    p.d_colSrc, p.d_inv, b, x);
+    if (p.d_invF)
+      pc_apply_t_kernel<float><<<p.nTiles, kPcRows * kPcSplit, 0, c.stream>>>(c.n, p.d_tiles, p.d_start, p.d_size,
+                                                                             p.d_off, p.d_colSrc, p.d_invF, b, x);
+    else
+      pc_apply_t_kernel<double><<<p.nTiles, kPcRows * kPcSplit, 0, c.stream>>>(c.n, p.d_tiles, p.d_start, p.d_size,
+                                                                              p.d_off, p.d_colSrc, p.d_inv, b, x);
   } else if (p.mode == 2) {
-    pc_apply_kernel<double><<<p.nTiles, kPcRows * kPcSplit, 0, c.stream>>>(c.n, p.d_tiles, p.d_start, p.d_size,
-                                                                           p.d_off, p.d_colSrc, p.d_inv, b, x);
+    if (p.d_invF)
+      pc_apply_kernel<float><<<p.nTiles, kPcRows * kPcSplit, 0, c.stream>>>(c.n, p.d_tiles, p.d_start, p.d_size,
+                                                                           p.d_off, p.d_colSrc, p.d_invF, b, x);
+    else
+      pc_apply_kernel<double><<<p.nTiles, kPcRows * kPcSplit, 0, c.stream>>>(c.n, p.d_tiles, p.d_start, p.d_size,
+                                                                             p.d_off, p.d_colSrc, p.d_inv, b, x);
   } else if (p.mode == 3) {
     pc_diag_kernel<<<ceil_div(c.n, 256), 256, 0, c.stream>>>(c.n, c.d_area, (1.0 + c.epsilon) / 2.0,
                                                             (1.0 + 1.0 / c.epsilon) / 2.0, b, x);
