@@ -94,6 +94,9 @@ Context::~Context() {
   free_precond(*this);
   free_adjoint(*this);
   arena.release();
+  if (sideStream) cudaStreamDestroy(sideStream);
+  if (evFork) cudaEventDestroy(evFork);
+  if (evJoin) cudaEventDestroy(evJoin);
   if (ownStream && stream) cudaStreamDestroy(stream);
 }
 
@@ -128,7 +131,7 @@ bool setup_geometry(Context &c, const double *vtx, const double *nrm, const doub
       !c.arena.upload(&c.d_leafCtr, leafCtr, s))
     return false;
   if (!c.arena.alloc_n(&c.d_x, 2 * (size_t)n) || !c.arena.alloc_n(&c.d_y, 2 * (size_t)n) ||
-      !c.arena.alloc_n(&c.d_w, 2 * (size_t)n))
+      !c.arena.alloc_n(&c.d_w, 2 * (size_t)n) || !c.arena.alloc_n(&c.d_nearOut, 2 * (size_t)n))
     return false;
   return true;
 }
@@ -158,9 +161,14 @@ bool op_apply(Context &c, int part, double alpha, const double *sgm, double beta
 bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y, bool adjoint, bool fp64) {
   double s1 = (1.0 + c.epsilon) / 2.0 * alpha;
   double s2 = (1.0 + 1.0 / c.epsilon) / 2.0 * alpha;
+  // the near field on the side stream, into d_nearOut, beside the far passes
+  FB_CUDA(cudaEventRecord(c.evFork, c.stream));
+  FB_CUDA(cudaStreamWaitEvent(c.sideStream, c.evFork, 0));
+  if (!launch_near(c, x, -alpha, c.d_nearOut, adjoint, fp64, c.sideStream, false)) return false;
+  FB_CUDA(cudaEventRecord(c.evJoin, c.sideStream));
   if (!launch_far_upward(c, x, adjoint)) return false;
-  if (!launch_l2p(c, -alpha, beta, y, x, s1, s2, adjoint)) return false;
-  if (!launch_near(c, x, -alpha, y, adjoint, fp64)) return false;
+  FB_CUDA(cudaStreamWaitEvent(c.stream, c.evJoin, 0));
+  if (!launch_l2p(c, -alpha, beta, y, x, s1, s2, adjoint, c.d_nearOut)) return false;
   return true;
 }
 
@@ -201,6 +209,12 @@ int create_context(const fabipb_b200_params *p, int n, const double *vtx, const 
     ok = false;
   }
   c->ownStream = ok;
+  if (ok && (cudaStreamCreateWithFlags(&c->sideStream, cudaStreamNonBlocking) != cudaSuccess ||
+             cudaEventCreateWithFlags(&c->evFork, cudaEventDisableTiming) != cudaSuccess ||
+             cudaEventCreateWithFlags(&c->evJoin, cudaEventDisableTiming) != cudaSuccess)) {
+    set_error("stream/event creation failed");
+    ok = false;
+  }
   StageTimer tm("create", c->stream);
   ok = ok && init_quad_tables();
   ok = ok && setup_geometry(*c, vtx, normal, area);

@@ -75,6 +75,10 @@ struct Context {
   // ---- scratch vectors for host-pointer calls ------------------------
   double *d_x = nullptr, *d_y = nullptr, *d_w = nullptr;
   double *d_refR = nullptr, *d_refD = nullptr, *d_refZ = nullptr;   // iterative refinement (first use)
+  // the matvec runs the near field on a second stream beside the far passes
+  cudaStream_t sideStream = nullptr;
+  cudaEvent_t evFork = nullptr, evJoin = nullptr;
+  double *d_nearOut = nullptr;             // 2N: the near-field term of the current matvec
 
   // ---- charges, RHS, energy -------------------------------------------
   std::vector<int> chargeOrders;           // per-level charge-tree order (host policy)
@@ -102,15 +106,19 @@ bool setup_charges(Context &c, int m, const double *pos, const double *q);
 
 // device operators on device vectors (stream-ordered, no synchronisation)
 // near:  out += coef * K_near * sgm
-// (fp64: the FP64 P2P in a mixed context, for refinement residuals)
-bool launch_near(Context &c, const double *sgm, double coef, double *out, bool adjoint = false, bool fp64 = false);
+// (fp64: the FP64 P2P in a mixed context, for refinement residuals; stream:
+// the stream to launch on, default the context's; accumulate = false writes
+// out = coef * K_near * sgm)
+bool launch_near(Context &c, const double *sgm, double coef, double *out, bool adjoint = false, bool fp64 = false,
+                 cudaStream_t stream = nullptr, bool accumulate = true);
 // upward pass + interaction + downward pass: leaves local expansions in d_lec
 // (adjoint: the transposed far operator's upward half, see fmm.cu)
 // (marks: 4 events recorded after Q2M, M2M, M2L and L2L, for pass timing)
 bool launch_far_upward(Context &c, const double *sgm, bool adjoint = false, cudaEvent_t *marks = nullptr);
 // L2P: out = beta*out + alpha*far + diag*(area .* x) (diag part optional)
+// (addend: a vector added to out, the near field computed beside the far passes)
 bool launch_l2p(Context &c, double alpha, double beta, double *out, const double *diagX,
-                double s1, double s2, bool adjoint = false);
+                double s1, double s2, bool adjoint = false, const double *addend = nullptr);
 bool launch_m2l_only(Context &c, bool adjoint = false);
 bool launch_rhs(Context &c, int useTree, double *rhs);
 bool launch_energy(Context &c, const double *sgm, double *raw_host);

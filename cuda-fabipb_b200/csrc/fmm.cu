@@ -655,7 +655,8 @@ __global__ void l2p_kernel(int n, int NMleaf, int NM, const int *__restrict__ le
                            const double *__restrict__ Q1, const double *__restrict__ lec1,
                            const double *__restrict__ lec2, const double *__restrict__ lec3,
                            const double *__restrict__ lec4, double alpha, double beta, const double *__restrict__ area,
-                           const double *__restrict__ diagX, double s1, double s2, int swap, double *out) {
+                           const double *__restrict__ diagX, double s1, double s2, int swap,
+                           const double *__restrict__ addend, double *out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const size_t f = (size_t)leafFmm[leafOfPanel[i]] * NM;
@@ -676,6 +677,10 @@ __global__ void l2p_kernel(int n, int NMleaf, int NM, const int *__restrict__ le
   if (diagX) {
     o0 += s1 * area[i] * diagX[i];
     o1 += s2 * area[i] * diagX[n + i];
+  }
+  if (addend) {
+    o0 += addend[i];
+    o1 += addend[n + i];
   }
   out[i] = o0;
   out[n + i] = o1;
@@ -928,7 +933,7 @@ bool launch_m2l_only(Context &c, bool adjoint) {
 }
 
 bool launch_l2p(Context &c, double alpha, double beta, double *out, const double *diagX, double s1, double s2,
-                bool adjoint) {
+                bool adjoint, const double *addend) {
   const size_t plane = (size_t)c.pt.nFmm * c.NM;
   c.launches += 1;
   // adjoint: Q0 . (adjoint dpdn moments + 0) -> dpdn half, Q1 . (adjoint pot moments + 0) -> pot half
@@ -936,7 +941,7 @@ bool launch_l2p(Context &c, double alpha, double beta, double *out, const double
   const double *l3 = adjoint ? c.d_mom : c.d_lec + 2 * plane, *l4 = c.d_lec + 3 * plane;
   l2p_kernel<<<ceil_div(c.n, 256), 256, 0, c.stream>>>(c.n, c.NMleaf, c.NM, c.d_leafOfPanel, c.d_leafFmm, c.d_Q0,
                                                        c.d_Q1, l1, l2, l3, l4, alpha, beta, c.d_area, diagX, s1, s2,
-                                                       adjoint ? 1 : 0, out);
+                                                       adjoint ? 1 : 0, addend, out);
   FB_CUDA(cudaGetLastError());
   return true;
 }

@@ -154,7 +154,7 @@ near_apply_kernel(int nWork, const int2 *__restrict__ work, const int *__restric
                   const int *__restrict__ spOff, const int *__restrict__ spSrc,
                   const double4 *__restrict__ spK, const double *__restrict__ sgm,
                   const double *__restrict__ area, int n, T kappa, T kexp, T eps, T ieps, T kap2,
-                  double coef, double *out) {
+                  double coef, int accumulate, double *out) {
   typedef typename Vec4<T>::t V;
   __shared__ V sA[kNearWarps][32];
   __shared__ V sB[kNearWarps][32];
@@ -221,8 +221,9 @@ near_apply_kernel(int nWork, const int2 *__restrict__ work, const int *__restric
     e1 += d.z * sd + d.w * sp;
   }
   const double AX = area[X] * kFourPiI;
-  out[X] += coef * (AX * (double)acc0 + e0);
-  out[X + n] += coef * (AX * (double)acc1 + e1);
+  const double v0 = coef * (AX * (double)acc0 + e0), v1 = coef * (AX * (double)acc1 + e1);
+  out[X] = accumulate ? out[X] + v0 : v0;   // each output has exactly one writer
+  out[X + n] = accumulate ? out[X + n] + v1 : v1;
 }
 
 // FP64 correction for every special pair: exact panelIA0 minus the
@@ -432,10 +433,9 @@ bool setup_near(Context &c) {
 
 template <typename T, bool ADJ>
 static void launch_near_t(Context &c, const void *tgtP, const void *tgtN, void *srcA, void *srcB, const double *sgm,
-                          double coef, double *out) {
+                          double coef, double *out, cudaStream_t s, bool accumulate) {
   typedef typename Vec4<T>::t V;
   const int n = c.n;
-  cudaStream_t s = c.stream;
   const double kap = c.prm.kappa, eps = c.epsilon;
   const unsigned grid = ceil_div(c.nWork, kNearWarps);
   const double kexp = sizeof(T) == 4 ? -kap * 1.4426950408889634 : -kap;   // float: exp2 argument
@@ -444,7 +444,7 @@ static void launch_near_t(Context &c, const void *tgtP, const void *tgtN, void *
   near_apply_kernel<T, ADJ><<<grid, kNearWarps * 32, 0, s>>>(
       c.nWork, c.d_work, c.d_leafStart, c.d_leafCount, c.d_nearOff, c.d_nearSrc, c.d_leafCtr, (const V *)tgtP,
       (const V *)tgtN, (const V *)srcA, (const V *)srcB, c.d_spOff, c.d_spSrc, ADJ ? c.d_spKT : c.d_spK, sgm,
-      c.d_area, n, (T)kap, (T)kexp, (T)eps, (T)(1.0 / eps), (T)(kap * kap), coef, out);
+      c.d_area, n, (T)kap, (T)kexp, (T)eps, (T)(1.0 / eps), (T)(kap * kap), coef, accumulate ? 1 : 0, out);
 }
 
 // FP64 records in a mixed context, for the FP64 residuals of iterative
@@ -502,18 +502,21 @@ static bool setup_near_adjoint(Context &c) {
   return true;
 }
 
-bool launch_near(Context &c, const double *sgm, double coef, double *out, bool adjoint, bool fp64) {
+bool launch_near(Context &c, const double *sgm, double coef, double *out, bool adjoint, bool fp64,
+                 cudaStream_t stream, bool accumulate) {
   if (adjoint && !setup_near_adjoint(c)) return false;
+  cudaStream_t s = stream ? stream : c.stream;
+  const bool acc = accumulate;
   if (c.mixed && fp64) {
     if (!setup_near_fp64(c)) return false;
-    if (adjoint) launch_near_t<double, true>(c, c.d_tgtP64, c.d_tgtN64, c.d_srcA64, c.d_srcB64, sgm, coef, out);
-    else launch_near_t<double, false>(c, c.d_tgtP64, c.d_tgtN64, c.d_srcA64, c.d_srcB64, sgm, coef, out);
+    if (adjoint) launch_near_t<double, true>(c, c.d_tgtP64, c.d_tgtN64, c.d_srcA64, c.d_srcB64, sgm, coef, out, s, acc);
+    else launch_near_t<double, false>(c, c.d_tgtP64, c.d_tgtN64, c.d_srcA64, c.d_srcB64, sgm, coef, out, s, acc);
   } else if (c.mixed) {
-    if (adjoint) launch_near_t<float, true>(c, c.d_tgtP, c.d_tgtN, c.d_srcA, c.d_srcB, sgm, coef, out);
-    else launch_near_t<float, false>(c, c.d_tgtP, c.d_tgtN, c.d_srcA, c.d_srcB, sgm, coef, out);
+    if (adjoint) launch_near_t<float, true>(c, c.d_tgtP, c.d_tgtN, c.d_srcA, c.d_srcB, sgm, coef, out, s, acc);
+    else launch_near_t<float, false>(c, c.d_tgtP, c.d_tgtN, c.d_srcA, c.d_srcB, sgm, coef, out, s, acc);
   } else {
-    if (adjoint) launch_near_t<double, true>(c, c.d_tgtP, c.d_tgtN, c.d_srcA, c.d_srcB, sgm, coef, out);
-    else launch_near_t<double, false>(c, c.d_tgtP, c.d_tgtN, c.d_srcA, c.d_srcB, sgm, coef, out);
+    if (adjoint) launch_near_t<double, true>(c, c.d_tgtP, c.d_tgtN, c.d_srcA, c.d_srcB, sgm, coef, out, s, acc);
+    else launch_near_t<double, false>(c, c.d_tgtP, c.d_tgtN, c.d_srcA, c.d_srcB, sgm, coef, out, s, acc);
   }
   c.launches += 2;
   FB_CUDA(cudaGetLastError());
