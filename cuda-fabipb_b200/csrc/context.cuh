@@ -67,6 +67,7 @@ struct Context {
   int nConvList = 0;                           // entries of d_lst
   long long nM2LPairs = 0;
   double2 *d_m2lTens = nullptr;                // [nMom][pairs] (D G0, D Gk) per M2L pair
+  float2 *d_m2lTensF = nullptr;                // the same in FP32 (mixed contexts, orders <= 4)
   // transposed M2L lists (adjoint operator, built on first use)
   bool m2lAdjReady = false;
   std::vector<int> h_m2lDstT;
@@ -114,12 +115,14 @@ bool launch_near(Context &c, const double *sgm, double coef, double *out, bool a
 // upward pass + interaction + downward pass: leaves local expansions in d_lec
 // (adjoint: the transposed far operator's upward half, see fmm.cu)
 // (marks: 4 events recorded after Q2M, M2M, M2L and L2L, for pass timing)
-bool launch_far_upward(Context &c, const double *sgm, bool adjoint = false, cudaEvent_t *marks = nullptr);
+// (fp64: the FP64 interaction also in a mixed context, for refinement residuals)
+bool launch_far_upward(Context &c, const double *sgm, bool adjoint = false, cudaEvent_t *marks = nullptr,
+                       bool fp64 = false);
 // L2P: out = beta*out + alpha*far + diag*(area .* x) (diag part optional)
 // (addend: a vector added to out, the near field computed beside the far passes)
 bool launch_l2p(Context &c, double alpha, double beta, double *out, const double *diagX,
                 double s1, double s2, bool adjoint = false, const double *addend = nullptr);
-bool launch_m2l_only(Context &c, bool adjoint = false);
+bool launch_m2l_only(Context &c, bool adjoint = false, bool fp64 = false);
 bool launch_rhs(Context &c, int useTree, double *rhs);
 bool launch_energy(Context &c, const double *sgm, double *raw_host);
 bool precond_setup(Context &c, int mode);

@@ -328,14 +328,15 @@ __global__ void m2l_tensor_kernel(long long nPairs, const int *__restrict__ pair
 
 // Sum four values over the 32 lanes with six shuffles: after the call lane 0
 // holds the total of v[0], lane 8 of v[1], lane 16 of v[2], lane 24 of v[3].
-__device__ __forceinline__ double warp_sum4(double a, double b, double c, double d, int lane) {
+template <typename TV>
+__device__ __forceinline__ TV warp_sum4(TV a, TV b, TV c, TV d, int lane) {
   const bool hi16 = lane & 16;
-  double s0 = hi16 ? a : c, s1 = hi16 ? b : d;      // sent away
-  double k0 = hi16 ? c : a, k1 = hi16 ? d : b;      // kept
+  TV s0 = hi16 ? a : c, s1 = hi16 ? b : d;      // sent away
+  TV k0 = hi16 ? c : a, k1 = hi16 ? d : b;      // kept
   k0 += __shfl_xor_sync(0xffffffffu, s0, 16);
   k1 += __shfl_xor_sync(0xffffffffu, s1, 16);
   const bool hi8 = lane & 8;
-  double k = hi8 ? k1 : k0;
+  TV k = hi8 ? k1 : k0;
   k += __shfl_xor_sync(0xffffffffu, hi8 ? k0 : k1, 8);
   k += __shfl_xor_sync(0xffffffffu, k, 4);
   k += __shfl_xor_sync(0xffffffffu, k, 2);
@@ -495,13 +496,33 @@ __host__ __device__ constexpr int m2l_entries() {
 #ifndef FB_M2L_MIN_BLOCKS
 #define FB_M2L_MIN_BLOCKS 3
 #endif
+#ifndef FB_M2L_MIN_BLOCKS_F32
+#define FB_M2L_MIN_BLOCKS_F32 4
+#endif
 
-template <int PM>
+template <typename TV>
+struct Vec2;
+template <>
+struct Vec2<double> {
+  typedef double2 t;
+  __device__ static double2 make(double a, double b) { return make_double2(a, b); }
+};
+template <>
+struct Vec2<float> {
+  typedef float2 t;
+  __device__ static float2 make(double a, double b) { return make_float2((float)a, (float)b); }
+};
+
+// TV: the arithmetic type of the conv (double, or float in mixed contexts);
+// the per-coefficient sums across batches are always FP64.
+template <int PM, typename TV = double>
 struct M2LUnrolledShape {
+  typedef typename Vec2<TV>::t V2;
   static constexpr int NMP = nmom_c(PM);
   static constexpr int W = 4;                         // warps per block
-  static constexpr size_t warpElems = (size_t)NMP * 32 + 2 * NMP;   // moment columns + [4][NMP] sums
-  static constexpr size_t bytes = W * warpElems * sizeof(double2);
+  static constexpr size_t colBytes = (size_t)NMP * 32 * sizeof(V2);   // moment columns
+  static constexpr size_t warpBytes = colBytes + 4 * NMP * sizeof(double);   // + [4][NMP] sums
+  static constexpr size_t bytes = W * warpBytes;
 };
 
 // Moment column of source j, coefficient e: XOR-swizzled so that both the
@@ -509,21 +530,23 @@ struct M2LUnrolledShape {
 // bank conflicts.
 __device__ __forceinline__ int m2l_slot(int e, int j) { return e * 32 + (j ^ (e & 31)); }
 
-struct M2LSums {
-  double s1, s2, s3, s4;
-};
-
 // One (alpha, beta) entry.  FULL: the cube's order is PM, every entry counts.
 // The four sums of a coefficient are reduced over the lanes (component v's
 // total lands in lane 8v) and added to the warp's shared sums sAcc[v][alpha].
-template <int PM, int Q, bool FULL, bool ADJ>
-__device__ __forceinline__ void m2l_step(M2LSums &S, const double2 *sC, const double2 (&T)[nmom_c(PM)], int lane,
-                                         int order, double *sAcc) {
+template <typename TV>
+struct M2LSumsT {
+  TV s1, s2, s3, s4;
+};
+
+template <int PM, int Q, bool FULL, bool ADJ, typename TV>
+__device__ __forceinline__ void m2l_step(M2LSumsT<TV> &S, const typename Vec2<TV>::t *sC,
+                                         const typename Vec2<TV>::t (&T)[nmom_c(PM)], int lane, int order,
+                                         double *sAcc) {
   constexpr M2LEntry E = m2l_entry<PM>(Q);
-  if (E.first) S.s1 = S.s2 = S.s3 = S.s4 = 0.0;
+  if (E.first) S.s1 = S.s2 = S.s3 = S.s4 = (TV)0;
   if (FULL || E.dsum <= order) {
-    const double2 mo = sC[m2l_slot(E.ib, lane)];
-    const double2 d = T[E.ig];
+    const typename Vec2<TV>::t mo = sC[m2l_slot(E.ib, lane)];
+    const typename Vec2<TV>::t d = T[E.ig];
     if ((ADJ ? E.dal : E.dsum - E.dal) & 1) {   // (-1)^|input|, or (-1)^|output| transposed
       S.s1 -= mo.y * d.x; S.s2 -= mo.y * d.y; S.s3 -= mo.x * d.x; S.s4 -= mo.x * d.y;
     } else {
@@ -531,31 +554,38 @@ __device__ __forceinline__ void m2l_step(M2LSums &S, const double2 *sC, const do
     }
   }
   if (E.last && (FULL || E.dal <= order)) {
-    const double t = warp_sum4(S.s1, S.s2, S.s3, S.s4, lane);
-    if ((lane & 7) == 0) sAcc[(lane >> 3) * nmom_c(PM) + E.al] += t;
+    const TV t = warp_sum4<TV>(S.s1, S.s2, S.s3, S.s4, lane);
+    if ((lane & 7) == 0) sAcc[(lane >> 3) * nmom_c(PM) + E.al] += (double)t;
   }
 }
 
-template <int PM, bool FULL, bool ADJ, int... Q>
-__device__ __forceinline__ void m2l_steps(std::integer_sequence<int, Q...>, M2LSums &S, const double2 *sC,
-                                          const double2 (&T)[nmom_c(PM)], int lane, int order, double *sAcc) {
-  (m2l_step<PM, Q, FULL, ADJ>(S, sC, T, lane, order, sAcc), ...);
+template <int PM, bool FULL, bool ADJ, typename TV, int... Q>
+__device__ __forceinline__ void m2l_steps(std::integer_sequence<int, Q...>, M2LSumsT<TV> &S,
+                                          const typename Vec2<TV>::t *sC,
+                                          const typename Vec2<TV>::t (&T)[nmom_c(PM)], int lane, int order,
+                                          double *sAcc) {
+  (m2l_step<PM, Q, FULL, ADJ, TV>(S, sC, T, lane, order, sAcc), ...);
 }
 
-// ADJ: the transposed interaction, as for m2l_kernel.
-template <int PM, bool ADJ>
-__global__ void __launch_bounds__(128, FB_M2L_MIN_BLOCKS)
+// ADJ: the transposed interaction, as for m2l_kernel.  TV = float: tensors
+// (float2) and staged moments in FP32, each batch's per-coefficient sums in
+// FP32, accumulated over the batches in FP64.
+template <int PM, bool ADJ, typename TV>
+__global__ void __launch_bounds__(128, sizeof(TV) == 4 ? FB_M2L_MIN_BLOCKS_F32 : FB_M2L_MIN_BLOCKS)
 m2l_unrolled_kernel(int nDst, const int *__restrict__ dstList, const int *__restrict__ m2lOff,
                     const int *__restrict__ m2lSrc, const int *__restrict__ pairIdx,
                     const int *__restrict__ ordOfCube, long long nPairs,
-                    const double2 *__restrict__ tens, int NM, double eps, const double *__restrict__ momPot,
-                    const double *__restrict__ momDpdn, double *lec1, double *lec2, double *lec3, double *lec4) {
-  typedef M2LUnrolledShape<PM> Sh;
+                    const typename Vec2<TV>::t *__restrict__ tens, int NM, double eps,
+                    const double *__restrict__ momPot, const double *__restrict__ momDpdn, double *lec1,
+                    double *lec2, double *lec3, double *lec4) {
+  typedef M2LUnrolledShape<PM, TV> Sh;
+  typedef typename Vec2<TV>::t V2;
   constexpr int NMP = Sh::NMP;
   extern __shared__ double2 m2luSmem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double2 *sC = m2luSmem + (size_t)warp * Sh::warpElems;
-  double *sAcc = reinterpret_cast<double *>(sC + NMP * 32);   // [4][NMP]
+  char *wbase = reinterpret_cast<char *>(m2luSmem) + (size_t)warp * Sh::warpBytes;
+  V2 *sC = reinterpret_cast<V2 *>(wbase);
+  double *sAcc = reinterpret_cast<double *>(wbase + Sh::colBytes);   // [4][NMP]
   const int bi = blockIdx.x * Sh::W + warp;
   if (bi >= nDst) return;  // warp-uniform
   const int f = dstList[bi];
@@ -576,20 +606,22 @@ m2l_unrolled_kernel(int nDst, const int *__restrict__ dstList, const int *__rest
       for (int e0 = 0; e0 < NMP; e0 += 32) {
         const int e = e0 + lane;
         if (e < NMP)
-          sC[m2l_slot(e, j)] = j < nb ? make_double2(momPot[(size_t)sj * NM + e], momDpdn[(size_t)sj * NM + e])
-                                      : make_double2(0.0, 0.0);
+          sC[m2l_slot(e, j)] = j < nb ? Vec2<TV>::make(momPot[(size_t)sj * NM + e], momDpdn[(size_t)sj * NM + e])
+                                      : Vec2<TV>::make(0.0, 0.0);
       }
     }
-    double2 T[NMP];
-    const double2 *tp = tens + (ADJ ? pairIdx[live ? k : o0] : (live ? k : o0));
+    V2 T[NMP];
+    const V2 *tp = tens + (ADJ ? pairIdx[live ? k : o0] : (live ? k : o0));
 #pragma unroll
     for (int e = 0; e < NMP; e++) T[e] = tp[(size_t)e * nPairs];
     __syncwarp();
-    M2LSums S{0.0, 0.0, 0.0, 0.0};
+    M2LSumsT<TV> S{(TV)0, (TV)0, (TV)0, (TV)0};
     if (order == PM)
-      m2l_steps<PM, true, ADJ>(std::make_integer_sequence<int, m2l_entries<PM>()>{}, S, sC, T, lane, order, sAcc);
+      m2l_steps<PM, true, ADJ, TV>(std::make_integer_sequence<int, m2l_entries<PM>()>{}, S, sC, T, lane, order,
+                                   sAcc);
     else
-      m2l_steps<PM, false, ADJ>(std::make_integer_sequence<int, m2l_entries<PM>()>{}, S, sC, T, lane, order, sAcc);
+      m2l_steps<PM, false, ADJ, TV>(std::make_integer_sequence<int, m2l_entries<PM>()>{}, S, sC, T, lane, order,
+                                    sAcc);
   }
   __syncwarp();
   const int nm = ((order + 1) * (order + 2) * (order + 3)) / 6;
@@ -607,6 +639,11 @@ m2l_unrolled_kernel(int nDst, const int *__restrict__ dstList, const int *__rest
       lec4[o] += S4 - S3;
     }
   }
+}
+
+__global__ void tensors_to_float_kernel(long long n, const double2 *__restrict__ a, float2 *b) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    b[i] = make_float2((float)a[i].x, (float)a[i].y);
 }
 
 // L2L: one block per child cube of one level (parents one level up)
@@ -700,8 +737,29 @@ static void launch_leaf_moments(Context &c, int order) {
 // Forward: moments (d_mom) -> local expansions (4 planes of d_lec).
 // Adjoint: adjoint locals g12, g34 (planes 0, 1 of d_lec) -> adjoint moments
 // (pot, dpdn: planes 0, 1 of d_mom) over the transposed pair lists.
+template <int PU, bool ADJ, typename TV>
+static void launch_m2l_unrolled(Context &c, int nDst, const int *dst, const int *off, const int *src,
+                                const int *pairIdx, const void *tens, const double *inPot, const double *inDpdn,
+                                double *o1, double *o2, double *o3, double *o4) {
+  typedef M2LUnrolledShape<PU, TV> Sh;
+  static bool attrDone = false;
+  if (!attrDone) {
+    cudaFuncSetAttribute(m2l_unrolled_kernel<PU, ADJ, TV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)Sh::bytes);
+    attrDone = true;
+  }
+  const unsigned grid = ceil_div((long long)nDst, Sh::W);
+  m2l_unrolled_kernel<PU, ADJ, TV><<<grid, Sh::W * 32, Sh::bytes, c.stream>>>(
+      nDst, dst, off, src, pairIdx, c.d_ordM2L, c.nM2LPairs, (const typename Vec2<TV>::t *)tens, c.NM, c.epsilon,
+      inPot, inDpdn, o1, o2, o3, o4);
+}
+
+// Forward: moments (d_mom) -> local expansions (4 planes of d_lec).
+// Adjoint: adjoint locals g12, g34 (planes 0, 1 of d_lec) -> adjoint moments
+// (pot, dpdn: planes 0, 1 of d_mom) over the transposed pair lists.
+// fp32: the FP32 conv of a mixed context (orders up to 4).
 template <int PM>
-static void launch_m2l_t(Context &c, bool adj) {
+static void launch_m2l_t(Context &c, bool adj, bool fp32) {
   const size_t plane = (size_t)c.pt.nFmm * c.NM;
   const int nDst = adj ? (int)c.h_m2lDstT.size() : (int)c.h_m2lDst.size();
   const int *dst = adj ? c.d_m2lDstT : c.d_m2lDst, *off = adj ? c.d_m2lOffT : c.d_m2lOff;
@@ -709,31 +767,23 @@ static void launch_m2l_t(Context &c, bool adj) {
   const double *inPot = adj ? c.d_lec + plane : c.d_mom, *inDpdn = adj ? c.d_lec : c.d_mom + plane;
   double *o1 = adj ? c.d_mom : c.d_lec, *o2 = adj ? c.d_mom + plane : c.d_lec + plane;
   double *o3 = c.d_lec + 2 * plane, *o4 = c.d_lec + 3 * plane;
-  static int attrDone[2][kMaxOrder + 1] = {{0}};
   if (PM <= 4) {
     constexpr int PU = PM <= 4 ? PM : 4;
-    typedef M2LUnrolledShape<PU> Sh;
-    if (!attrDone[adj][PM]) {
-      cudaFuncSetAttribute(adj ? m2l_unrolled_kernel<PU, true> : m2l_unrolled_kernel<PU, false>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::bytes);
-      attrDone[adj][PM] = 1;
+    if (fp32 && c.d_m2lTensF) {
+      if (adj) launch_m2l_unrolled<PU, true, float>(c, nDst, dst, off, src, pairIdx, c.d_m2lTensF, inPot, inDpdn, o1, o2, o3, o4);
+      else launch_m2l_unrolled<PU, false, float>(c, nDst, dst, off, src, pairIdx, c.d_m2lTensF, inPot, inDpdn, o1, o2, o3, o4);
+    } else {
+      if (adj) launch_m2l_unrolled<PU, true, double>(c, nDst, dst, off, src, pairIdx, c.d_m2lTens, inPot, inDpdn, o1, o2, o3, o4);
+      else launch_m2l_unrolled<PU, false, double>(c, nDst, dst, off, src, pairIdx, c.d_m2lTens, inPot, inDpdn, o1, o2, o3, o4);
     }
-    const unsigned grid = ceil_div((long long)nDst, Sh::W);
-    if (adj)
-      m2l_unrolled_kernel<PU, true><<<grid, Sh::W * 32, Sh::bytes, c.stream>>>(
-          nDst, dst, off, src, pairIdx, c.d_ordM2L, c.nM2LPairs, c.d_m2lTens, c.NM, c.epsilon, inPot, inDpdn, o1, o2,
-          o3, o4);
-    else
-      m2l_unrolled_kernel<PU, false><<<grid, Sh::W * 32, Sh::bytes, c.stream>>>(
-          nDst, dst, off, src, pairIdx, c.d_ordM2L, c.nM2LPairs, c.d_m2lTens, c.NM, c.epsilon, inPot, inDpdn, o1, o2,
-          o3, o4);
     return;
   }
   typedef M2LShape<PM> Sh;
-  if (!attrDone[adj][PM]) {
+  static int attrDone[2] = {0, 0};
+  if (!attrDone[adj]) {
     cudaFuncSetAttribute(adj ? m2l_kernel<PM, true> : m2l_kernel<PM, false>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::bytes);
-    attrDone[adj][PM] = 1;
+    attrDone[adj] = 1;
   }
   const unsigned grid = ceil_div((long long)nDst, Sh::W);
   if (adj)
@@ -839,6 +889,11 @@ bool setup_fmm(Context &c) {
     if (!c.arena.alloc_n(&c.d_m2lTens, (size_t)c.NM * c.nM2LPairs)) return false;
     FB_DISPATCH_ORDER(c.P, launch_m2l_tensors, c, d_pairDst);
     FB_CUDA(cudaGetLastError());
+    if (c.mixed && c.P <= 4) {   // the FP32 copy the mixed conv reads
+      if (!c.arena.alloc_n(&c.d_m2lTensF, (size_t)c.NM * c.nM2LPairs)) return false;
+      tensors_to_float_kernel<<<1184, 256, 0, s>>>((long long)c.NM * c.nM2LPairs, c.d_m2lTens, c.d_m2lTensF);
+      FB_CUDA(cudaGetLastError());
+    }
   }
   // leaf matrices
   if (!c.arena.alloc_n(&c.d_Q0, (size_t)c.NMleaf * c.n) || !c.arena.alloc_n(&c.d_Q1, (size_t)c.NMleaf * c.n))
@@ -882,7 +937,7 @@ static bool setup_m2l_adjoint(Context &c) {
 // the halves exchanged) -> g12, g34 in d_lec planes 0, 1; L2L^T, which is the
 // M2M shift; M2L^T into d_mom planes 0, 1 (adjoint moments pot, dpdn); M2M^T,
 // which is the L2L shift; launch_l2p(adjoint) then applies Q2M^T.
-bool launch_far_upward(Context &c, const double *sgm, bool adjoint, cudaEvent_t *marks) {
+bool launch_far_upward(Context &c, const double *sgm, bool adjoint, cudaEvent_t *marks, bool fp64) {
   const PanelTree &pt = c.pt;
   const int depth = pt.t.depth, height = pt.t.height;
   cudaStream_t s = c.stream;
@@ -905,7 +960,7 @@ bool launch_far_upward(Context &c, const double *sgm, bool adjoint, cudaEvent_t 
                                                        c.d_mLst, up1, up2);
   }
   if (marks) cudaEventRecord(marks[1], s);
-  if (!launch_m2l_only(c, adjoint)) return false;
+  if (!launch_m2l_only(c, adjoint, fp64)) return false;
   if (marks) cudaEventRecord(marks[2], s);
   // downward arrays: 4 local planes (forward) or the 2 adjoint moment planes
   // plus 2 scratch planes (adjoint)
@@ -924,9 +979,9 @@ bool launch_far_upward(Context &c, const double *sgm, bool adjoint, cudaEvent_t 
   return true;
 }
 
-bool launch_m2l_only(Context &c, bool adjoint) {
+bool launch_m2l_only(Context &c, bool adjoint, bool fp64) {
   if ((adjoint ? c.h_m2lDstT : c.h_m2lDst).empty()) return true;
-  FB_DISPATCH_ORDER(c.P, launch_m2l_t, c, adjoint);
+  FB_DISPATCH_ORDER(c.P, launch_m2l_t, c, adjoint, c.mixed && !fp64);
   c.launches += 1;
   FB_CUDA(cudaGetLastError());
   return true;
