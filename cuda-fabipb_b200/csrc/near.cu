@@ -98,6 +98,10 @@ constexpr int kNearWarps = 4;
 #ifndef FB_NEAR_MIN_BLOCKS
 #define FB_NEAR_MIN_BLOCKS 8
 #endif
+// FP32 near field with packed f32x2 arithmetic (near_apply_f2_kernel)
+#ifndef FB_NEAR_PACKED
+#define FB_NEAR_PACKED 1
+#endif
 
 // One disjoint pair, one-point rule: the four KER4 kernels (src/kernel.c:109-147)
 // at d = target - source, times the source weights a.w = A*sigma_dpdn and
@@ -222,6 +226,152 @@ near_apply_kernel(int nWork, const int2 *__restrict__ work, const int *__restric
   }
   const double AX = area[X] * kFourPiI;
   const double v0 = coef * (AX * (double)acc0 + e0), v1 = coef * (AX * (double)acc1 + e1);
+  out[X] = accumulate ? out[X] + v0 : v0;   // each output has exactly one writer
+  out[X + n] = accumulate ? out[X + n] + v1 : v1;
+}
+
+// ---------------------------------------------------------------------------
+// FP32 near field with packed f32x2 arithmetic (sm_100 FFMA2/FMUL2/FADD2):
+// every lane evaluates two sources per step, so the issue slots per pair
+// drop by about half while the FP32 work stays the same.  A tile of 32
+// sources is staged as 16 source pairs, each as four float4
+// (-x0 -x1 -y0 -y1 | -z0 -z1 wa0 wa1 | nx0 nx1 ny0 ny1 | nz0 nz1 wb0 wb1),
+// so the packed operands come straight from the loads; an odd source count
+// is padded with a zero-weight source far away.  Same tasks, lane split,
+// pair formula (near_pair) and FP64 epilogue as near_apply_kernel.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+
+template <bool ADJ>
+__device__ __forceinline__ void near_pair2(const float4 A, const float4 B, const float4 C, const float4 D, float2 tx,
+                                           float2 ty, float2 tz, float2 tnx, float2 tny, float2 tnz, float kappa,
+                                           float kexp, float eps, float ieps, float kap2, float2 &acc0,
+                                           float2 &acc1) {
+  const float2 one = f2(1.f), m1 = f2(-1.f);
+  const float2 dx = __fadd2_rn(tx, make_float2(A.x, A.y));
+  const float2 dy = __fadd2_rn(ty, make_float2(A.z, A.w));
+  const float2 dz = __fadd2_rn(tz, make_float2(B.x, B.y));
+  const float2 wa = make_float2(B.z, B.w), wb = make_float2(D.z, D.w);
+  const float2 snx = make_float2(C.x, C.y), sny = make_float2(C.z, C.w), snz = make_float2(D.x, D.y);
+  const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+  float2 g;
+  g.x = r2.x > 0.f ? rsqrt_t(r2.x) : 0.f;   // 1/r, 0 for the coincident pair
+  g.y = r2.y > 0.f ? rsqrt_t(r2.y) : 0.f;
+  const float2 r = __fmul2_rn(r2, g);
+  const float2 ea = __fmul2_rn(f2(kexp), r);
+  float2 e;
+  e.x = expneg_t(1.f, ea.x);
+  e.y = expneg_t(1.f, ea.y);
+  const float2 c = __fmul2_rn(__ffma2_rn(f2(kappa), r, one), e);    // (kappa r + 1) e^{-kappa r}
+  const float2 g2 = __fmul2_rn(g, g), h = __fmul2_rn(g2, g);
+  const float2 ipX = __ffma2_rn(tnz, dz, __ffma2_rn(tny, dy, __fmul2_rn(tnx, dx)));
+  const float2 ipY = __ffma2_rn(snz, dz, __ffma2_rn(sny, dy, __fmul2_rn(snx, dx)));
+  const float2 ip0 = __ffma2_rn(tnz, snz, __ffma2_rn(tny, sny, __fmul2_rn(tnx, snx)));
+  const float2 t1 = __fmul2_rn(ipY, h), t2 = __fmul2_rn(ipX, h), u = __fmul2_rn(ipX, t1);
+  const float2 y0 = __fmul2_rn(g, __ffma2_rn(e, m1, one));                                   // G0 - Gk
+  const float2 dd = __fmul2_rn(__ffma2_rn(u, f2(-3.f), __fmul2_rn(ip0, g)), g2);             // d2 G0
+  const float2 y3 = __ffma2_rn(dd, __fadd2_rn(c, m1), __fmul2_rn(__fmul2_rn(f2(-kap2), e), u));
+  if (ADJ) {
+    const float2 q1 = __fmul2_rn(t2, __ffma2_rn(f2(-eps), c, one));    // -t2 (eps c - 1)
+    const float2 q2 = __fmul2_rn(t1, __ffma2_rn(f2(-ieps), c, one));   // -t1 (c/eps - 1)
+    acc0 = __ffma2_rn(y3, wa, acc0);
+    acc0 = __ffma2_rn(q1, wb, acc0);
+    acc1 = __ffma2_rn(y0, wb, acc1);
+    acc1 = __ffma2_rn(q2, wa, acc1);
+  } else {
+    const float2 y1 = __fmul2_rn(t1, __ffma2_rn(f2(eps), c, m1));      // eps dGk/dn_y - dG0/dn_y
+    const float2 y2 = __fmul2_rn(t2, __ffma2_rn(f2(ieps), c, m1));     // dGk/dn_x / eps - dG0/dn_x
+    acc0 = __ffma2_rn(y0, wa, acc0);
+    acc0 = __ffma2_rn(y1, wb, acc0);
+    acc1 = __ffma2_rn(y2, wa, acc1);
+    acc1 = __ffma2_rn(y3, wb, acc1);
+  }
+}
+
+template <bool ADJ>
+__global__ void __launch_bounds__(kNearWarps * 32, FB_NEAR_MIN_BLOCKS)
+near_apply_f2_kernel(int nWork, const int2 *__restrict__ work, const int *__restrict__ leafStart,
+                     const int *__restrict__ leafCount, const int *__restrict__ nearOff,
+                     const int *__restrict__ nearSrc, const double *__restrict__ leafCtr,
+                     const float4 *__restrict__ tgtP, const float4 *__restrict__ tgtN,
+                     const float4 *__restrict__ srcA, const float4 *__restrict__ srcB,
+                     const int *__restrict__ spOff, const int *__restrict__ spSrc, const double4 *__restrict__ spK,
+                     const double *__restrict__ sgm, const double *__restrict__ area, int n, float kappa, float kexp,
+                     float eps, float ieps, float kap2, double coef, int accumulate, double *out) {
+  __shared__ float4 sP[kNearWarps][16][4];
+  __shared__ float sR[kNearWarps][2][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int task = blockIdx.x * kNearWarps + warp;
+  if (task >= nWork) return;  // warp-uniform
+  const int2 wk = work[task];
+  const int L = wk.x;
+  const int base = leafStart[L], cnt = leafCount[L];
+  const int g0 = 32 * wk.y;
+  const int mt = min(32, cnt - g0);   // targets in this group
+  const int k = 32 / mt;              // lanes per target
+  const int t = lane / k, sub = lane - t * k;
+  const bool valid = t < mt;
+  const int X = base + g0 + (valid ? t : 0);
+  const float4 tp = tgtP[X], tn = tgtN[X];
+  const float2 tnx = f2(tn.x), tny = f2(tn.y), tnz = f2(tn.z);
+  const double cx = leafCtr[3 * L], cy = leafCtr[3 * L + 1], cz = leafCtr[3 * L + 2];
+  float2 acc0 = f2(0.f), acc1 = f2(0.f);
+  float *pf = reinterpret_cast<float *>(&sP[warp][lane >> 1][0]) + (lane & 1);
+  const int p1 = nearOff[L + 1];
+  for (int p = nearOff[L]; p < p1; p++) {
+    const int S = nearSrc[p];
+    const int sb = leafStart[S], sc = leafCount[S];
+    const float2 tx = f2(tp.x + (float)(cx - leafCtr[3 * S]));
+    const float2 ty = f2(tp.y + (float)(cy - leafCtr[3 * S + 1]));
+    const float2 tz = f2(tp.z + (float)(cz - leafCtr[3 * S + 2]));
+    for (int j0 = 0; j0 < sc; j0 += 32) {
+      const int m = min(32, sc - j0);
+      float4 a = make_float4(-1e4f, -1e4f, -1e4f, 0.f), b = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (lane < m) {
+        a = srcA[sb + j0 + lane];
+        b = srcB[sb + j0 + lane];
+      }
+      pf[0] = -a.x; pf[2] = -a.y; pf[4] = -a.z; pf[6] = a.w;
+      pf[8] = b.x; pf[10] = b.y; pf[12] = b.z; pf[14] = b.w;
+      __syncwarp();
+      const int np = (m + 1) >> 1;
+      if (k == 1) {   // warp-uniform: a full group
+#pragma unroll 2
+        for (int q = 0; q < np; q++)
+          near_pair2<ADJ>(sP[warp][q][0], sP[warp][q][1], sP[warp][q][2], sP[warp][q][3], tx, ty, tz, tnx, tny,
+                          tnz, kappa, kexp, eps, ieps, kap2, acc0, acc1);
+      } else {
+#pragma unroll 2
+        for (int q = sub; q < np; q += k)
+          near_pair2<ADJ>(sP[warp][q][0], sP[warp][q][1], sP[warp][q][2], sP[warp][q][3], tx, ty, tz, tnx, tny,
+                          tnz, kappa, kexp, eps, ieps, kap2, acc0, acc1);
+      }
+      __syncwarp();
+    }
+  }
+  float s0 = acc0.x + acc0.y, s1 = acc1.x + acc1.y;
+  if (k > 1) {   // warp-uniform: add the k partial sums of each target
+    sR[warp][0][lane] = s0;
+    sR[warp][1][lane] = s1;
+    __syncwarp();
+    if (valid && sub == 0)
+      for (int i = 1; i < k; i++) {
+        s0 += sR[warp][0][lane + i];
+        s1 += sR[warp][1][lane + i];
+      }
+  }
+  if (!valid || sub != 0) return;
+  double e0 = 0.0, e1 = 0.0;
+  const int sp1 = spOff[X + 1];
+  for (int e = spOff[X]; e < sp1; e++) {
+    const int Y = spSrc[e];
+    const double4 d = spK[e];
+    const double sp = sgm[Y], sd = sgm[n + Y];
+    e0 += d.x * sd + d.y * sp;
+    e1 += d.z * sd + d.w * sp;
+  }
+  const double AX = area[X] * kFourPiI;
+  const double v0 = coef * (AX * (double)s0 + e0), v1 = coef * (AX * (double)s1 + e1);
   out[X] = accumulate ? out[X] + v0 : v0;   // each output has exactly one writer
   out[X + n] = accumulate ? out[X + n] + v1 : v1;
 }
@@ -441,6 +591,14 @@ static void launch_near_t(Context &c, const void *tgtP, const void *tgtN, void *
   const double kexp = sizeof(T) == 4 ? -kap * 1.4426950408889634 : -kap;   // float: exp2 argument
   near_pack_kernel<T><<<ceil_div(n, 256), 256, 0, s>>>(n, (const V *)tgtP, (const V *)tgtN, c.d_area, sgm, (V *)srcA,
                                                        (V *)srcB);
+  if (sizeof(T) == 4 && FB_NEAR_PACKED) {
+    near_apply_f2_kernel<ADJ><<<grid, kNearWarps * 32, 0, s>>>(
+        c.nWork, c.d_work, c.d_leafStart, c.d_leafCount, c.d_nearOff, c.d_nearSrc, c.d_leafCtr,
+        (const float4 *)tgtP, (const float4 *)tgtN, (const float4 *)srcA, (const float4 *)srcB, c.d_spOff, c.d_spSrc,
+        ADJ ? c.d_spKT : c.d_spK, sgm, c.d_area, n, (float)kap, (float)kexp, (float)eps, (float)(1.0 / eps),
+        (float)(kap * kap), coef, accumulate ? 1 : 0, out);
+    return;
+  }
   near_apply_kernel<T, ADJ><<<grid, kNearWarps * 32, 0, s>>>(
       c.nWork, c.d_work, c.d_leafStart, c.d_leafCount, c.d_nearOff, c.d_nearSrc, c.d_leafCtr, (const V *)tgtP,
       (const V *)tgtN, (const V *)srcA, (const V *)srcB, c.d_spOff, c.d_spSrc, ADJ ? c.d_spKT : c.d_spK, sgm,
