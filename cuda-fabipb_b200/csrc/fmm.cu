@@ -515,14 +515,31 @@ struct Vec2<float> {
 
 // TV: the arithmetic type of the conv (double, or float in mixed contexts);
 // the per-coefficient sums across batches are always FP64.
+// TSMEM (order 5): the tensors of the batch's 32 pairs are staged in shared
+// memory next to the moments instead of being held in registers.
 template <int PM, typename TV = double>
 struct M2LUnrolledShape {
   typedef typename Vec2<TV>::t V2;
   static constexpr int NMP = nmom_c(PM);
-  static constexpr int W = 4;                         // warps per block
-  static constexpr size_t colBytes = (size_t)NMP * 32 * sizeof(V2);   // moment columns
-  static constexpr size_t warpBytes = colBytes + 4 * NMP * sizeof(double);   // + [4][NMP] sums
+  static constexpr bool TSMEM = PM >= 5;
+  static constexpr int W = TSMEM ? (sizeof(TV) == 8 ? 1 : 2) : 4;   // warps per block
+  static constexpr size_t colBytes = (size_t)NMP * 32 * sizeof(V2);   // moment columns (and tensor columns)
+  static constexpr size_t warpBytes = (TSMEM ? 2 : 1) * colBytes + 4 * NMP * sizeof(double);   // + [4][NMP] sums
   static constexpr size_t bytes = W * warpBytes;
+};
+
+// the tensor entry ig of this lane's pair: registers or the shared column
+template <int PM, typename TV, bool TSMEM>
+struct M2LTensors;
+template <int PM, typename TV>
+struct M2LTensors<PM, TV, false> {
+  typename Vec2<TV>::t v[nmom_c(PM)];
+  __device__ __forceinline__ typename Vec2<TV>::t get(int ig, int) const { return v[ig]; }
+};
+template <int PM, typename TV>
+struct M2LTensors<PM, TV, true> {
+  const typename Vec2<TV>::t *col;
+  __device__ __forceinline__ typename Vec2<TV>::t get(int ig, int lane) const { return col[ig * 32 + lane]; }
 };
 
 // Moment column of source j, coefficient e: XOR-swizzled so that both the
@@ -538,15 +555,14 @@ struct M2LSumsT {
   TV s1, s2, s3, s4;
 };
 
-template <int PM, int Q, bool FULL, bool ADJ, typename TV>
-__device__ __forceinline__ void m2l_step(M2LSumsT<TV> &S, const typename Vec2<TV>::t *sC,
-                                         const typename Vec2<TV>::t (&T)[nmom_c(PM)], int lane, int order,
-                                         double *sAcc) {
+template <int PM, int Q, bool FULL, bool ADJ, typename TV, typename TT>
+__device__ __forceinline__ void m2l_step(M2LSumsT<TV> &S, const typename Vec2<TV>::t *sC, const TT &T, int lane,
+                                         int order, double *sAcc) {
   constexpr M2LEntry E = m2l_entry<PM>(Q);
   if (E.first) S.s1 = S.s2 = S.s3 = S.s4 = (TV)0;
   if (FULL || E.dsum <= order) {
     const typename Vec2<TV>::t mo = sC[m2l_slot(E.ib, lane)];
-    const typename Vec2<TV>::t d = T[E.ig];
+    const typename Vec2<TV>::t d = T.get(E.ig, lane);
     if ((ADJ ? E.dal : E.dsum - E.dal) & 1) {   // (-1)^|input|, or (-1)^|output| transposed
       S.s1 -= mo.y * d.x; S.s2 -= mo.y * d.y; S.s3 -= mo.x * d.x; S.s4 -= mo.x * d.y;
     } else {
@@ -559,19 +575,19 @@ __device__ __forceinline__ void m2l_step(M2LSumsT<TV> &S, const typename Vec2<TV
   }
 }
 
-template <int PM, bool FULL, bool ADJ, typename TV, int... Q>
+template <int PM, bool FULL, bool ADJ, typename TV, typename TT, int... Q>
 __device__ __forceinline__ void m2l_steps(std::integer_sequence<int, Q...>, M2LSumsT<TV> &S,
-                                          const typename Vec2<TV>::t *sC,
-                                          const typename Vec2<TV>::t (&T)[nmom_c(PM)], int lane, int order,
+                                          const typename Vec2<TV>::t *sC, const TT &T, int lane, int order,
                                           double *sAcc) {
-  (m2l_step<PM, Q, FULL, ADJ, TV>(S, sC, T, lane, order, sAcc), ...);
+  (m2l_step<PM, Q, FULL, ADJ, TV, TT>(S, sC, T, lane, order, sAcc), ...);
 }
 
 // ADJ: the transposed interaction, as for m2l_kernel.  TV = float: tensors
 // (float2) and staged moments in FP32, each batch's per-coefficient sums in
 // FP32, accumulated over the batches in FP64.
 template <int PM, bool ADJ, typename TV>
-__global__ void __launch_bounds__(128, sizeof(TV) == 4 ? FB_M2L_MIN_BLOCKS_F32 : FB_M2L_MIN_BLOCKS)
+__global__ void __launch_bounds__(M2LUnrolledShape<PM, TV>::W * 32,
+                                  PM >= 5 ? 1 : (sizeof(TV) == 4 ? FB_M2L_MIN_BLOCKS_F32 : FB_M2L_MIN_BLOCKS))
 m2l_unrolled_kernel(int nDst, const int *__restrict__ dstList, const int *__restrict__ m2lOff,
                     const int *__restrict__ m2lSrc, const int *__restrict__ pairIdx,
                     const int *__restrict__ ordOfCube, long long nPairs,
@@ -610,10 +626,16 @@ m2l_unrolled_kernel(int nDst, const int *__restrict__ dstList, const int *__rest
                                       : Vec2<TV>::make(0.0, 0.0);
       }
     }
-    V2 T[NMP];
+    M2LTensors<PM, TV, Sh::TSMEM> T;
     const V2 *tp = tens + (ADJ ? pairIdx[live ? k : o0] : (live ? k : o0));
+    if constexpr (Sh::TSMEM) {
+      V2 *sT = reinterpret_cast<V2 *>(wbase + Sh::colBytes + 4 * NMP * sizeof(double));
+      for (int e = 0; e < NMP; e++) sT[e * 32 + lane] = tp[(size_t)e * nPairs];
+      T.col = sT;
+    } else {
 #pragma unroll
-    for (int e = 0; e < NMP; e++) T[e] = tp[(size_t)e * nPairs];
+      for (int e = 0; e < NMP; e++) T.v[e] = tp[(size_t)e * nPairs];
+    }
     __syncwarp();
     M2LSumsT<TV> S{(TV)0, (TV)0, (TV)0, (TV)0};
     if (order == PM)
@@ -767,8 +789,8 @@ static void launch_m2l_t(Context &c, bool adj, bool fp32) {
   const double *inPot = adj ? c.d_lec + plane : c.d_mom, *inDpdn = adj ? c.d_lec : c.d_mom + plane;
   double *o1 = adj ? c.d_mom : c.d_lec, *o2 = adj ? c.d_mom + plane : c.d_lec + plane;
   double *o3 = c.d_lec + 2 * plane, *o4 = c.d_lec + 3 * plane;
-  if (PM <= 4) {
-    constexpr int PU = PM <= 4 ? PM : 4;
+  if (PM <= 5) {
+    constexpr int PU = PM <= 5 ? PM : 5;
     if (fp32 && c.d_m2lTensF) {
       if (adj) launch_m2l_unrolled<PU, true, float>(c, nDst, dst, off, src, pairIdx, c.d_m2lTensF, inPot, inDpdn, o1, o2, o3, o4);
       else launch_m2l_unrolled<PU, false, float>(c, nDst, dst, off, src, pairIdx, c.d_m2lTensF, inPot, inDpdn, o1, o2, o3, o4);
@@ -889,7 +911,7 @@ bool setup_fmm(Context &c) {
     if (!c.arena.alloc_n(&c.d_m2lTens, (size_t)c.NM * c.nM2LPairs)) return false;
     FB_DISPATCH_ORDER(c.P, launch_m2l_tensors, c, d_pairDst);
     FB_CUDA(cudaGetLastError());
-    if (c.mixed && c.P <= 4) {   // the FP32 copy the mixed conv reads
+    if (c.mixed && c.P <= 5) {   // the FP32 copy the mixed conv reads
       if (!c.arena.alloc_n(&c.d_m2lTensF, (size_t)c.NM * c.nM2LPairs)) return false;
       tensors_to_float_kernel<<<1184, 256, 0, s>>>((long long)c.NM * c.nM2LPairs, c.d_m2lTens, c.d_m2lTensF);
       FB_CUDA(cudaGetLastError());
