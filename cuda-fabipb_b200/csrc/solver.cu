@@ -63,15 +63,16 @@ void free_precond(Context &c) {
 // ---------------------------------------------------------------------------
 // block assembly: A(j, i) = -K1(X=j,Y=i) etc. in column-major M x M
 // ---------------------------------------------------------------------------
+template <typename TO>
 __global__ void pc_assemble_kernel(int nBlocks, const int *__restrict__ bStart, const int *__restrict__ bSize,
                                    const long long *__restrict__ bOff, const double *__restrict__ vtx,
                                    const double *__restrict__ nrm, const double *__restrict__ area, int q,
-                                   double kappa, double eps, double s1, double s2, double *A) {
+                                   double kappa, double eps, double s1, double s2, TO *A) {
   const int b = blockIdx.y;
   if (b >= nBlocks) return;
   const int hm = bSize[b], st = bStart[b], M = 2 * hm;
   const long long pairs = (long long)hm * hm;
-  double *Ab = A + bOff[b];
+  TO *Ab = A + bOff[b];
   for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < pairs;
        p += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(p / hm), j = (int)(p % hm);  // i: pnlY (column), j: pnlX (row)
@@ -92,10 +93,10 @@ __global__ void pc_assemble_kernel(int nBlocks, const int *__restrict__ bStart, 
     panel_ia0_d(q, kappa, eps, X, Y, Xi == Yi, K, nullptr);
     double d0 = (i == j) ? s1 * area[Yi] : 0.0;
     double d1 = (i == j) ? s2 * area[Yi] : 0.0;
-    Ab[(size_t)i * M + j] = -K[1] + d0;
-    Ab[(size_t)i * M + j + hm] = -K[0];
-    Ab[(size_t)(i + hm) * M + j] = -K[3];
-    Ab[(size_t)(i + hm) * M + j + hm] = -K[2] + d1;
+    Ab[(size_t)i * M + j] = (TO)(-K[1] + d0);
+    Ab[(size_t)i * M + j + hm] = (TO)(-K[0]);
+    Ab[(size_t)(i + hm) * M + j] = (TO)(-K[3]);
+    Ab[(size_t)(i + hm) * M + j + hm] = (TO)(-K[2] + d1);
   }
 }
 
@@ -133,28 +134,30 @@ __global__ void identity_kernel(int nList, const int *__restrict__ list, const i
 // pivot k.
 constexpr int kGjThreads = 256;
 
-template <int NB>
+template <typename TV, int NB>
 __host__ __device__ constexpr size_t gj_smem_bytes(int maxM) {
-  return (size_t)NB * maxM * sizeof(double) + 64 * NB * sizeof(double) + (size_t)maxM * sizeof(int);
+  return (size_t)NB * maxM * sizeof(TV) + 64 * NB * sizeof(TV) + (size_t)maxM * sizeof(int);
 }
 
-template <int NB, int CS>
+template <typename TV, int NB, int CS>
 __global__ void __launch_bounds__(kGjThreads, 1)
 pc_gj_invert_kernel(const int *__restrict__ list, const int *__restrict__ bStart, const int *__restrict__ bSize,
-                    const long long *__restrict__ bOff, const long long *__restrict__ yOff, double *inv, double *yAll,
+                    const long long *__restrict__ bOff, const long long *__restrict__ yOff, TV *inv, TV *yAll,
                     int *colSrc, int *info) {
-  extern __shared__ double gjSmem[];
-  __shared__ double wbest[kGjThreads / 32];
+  typedef typename Vec2<TV>::t V2;
+  extern __shared__ double gjSmemD[];
+  TV *gjSmem = reinterpret_cast<TV *>(gjSmemD);
+  __shared__ TV wbest[kGjThreads / 32];
   __shared__ int wbi[kGjThreads / 32];
   __shared__ int sPos[2 * NB], sSrc[2 * NB], sCnt;
-  __shared__ double sRk[NB], sOk[NB];
+  __shared__ TV sRk[NB], sOk[NB];
   const int rank = (CS > 1) ? (int)(blockIdx.x % CS) : 0;
   const int b = list[blockIdx.x / CS];
   const int M = 2 * bSize[b];
-  double *A = inv + bOff[b];
-  double *Y = yAll + yOff[b];
-  double *P = gjSmem;                          // panel, [NB][M]
-  double *Yt = gjSmem + (size_t)NB * M;        // Y tile, [64][NB]
+  TV *A = inv + bOff[b];
+  TV *Y = yAll + yOff[b];
+  TV *P = gjSmem;                          // panel, [NB][M]
+  TV *Yt = gjSmem + (size_t)NB * M;        // Y tile, [64][NB]
   int *perm = (int *)(Yt + 64 * NB);           // [M]
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   int bad = 0;
@@ -171,30 +174,30 @@ pc_gj_invert_kernel(const int *__restrict__ list, const int *__restrict__ bStart
     // step: two barriers per step.
     for (int kk = 0; kk < nb; kk++) {
       const int k = k0 + kk;
-      double best = -1.0;
+      TV best = (TV)-1;
       int bi = M;
       for (int i = t; i < M; i += kGjThreads) {
         if (i < k) continue;
-        const double v = fabs(P[kk * M + i]);
+        const TV v = fabs(P[kk * M + i]);
         if (v > best) { best = v; bi = i; }
       }
       for (int o = 16; o > 0; o >>= 1) {   // first largest within the warp
-        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const TV ob = __shfl_xor_sync(0xffffffffu, best, o);
         const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
         if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
       }
       if (lane == 0) { wbest[warp] = best; wbi[warp] = bi; }
       __syncthreads();
       int pv = wbi[0];
-      double pb = wbest[0];
+      TV pb = wbest[0];
       for (int w = 1; w < kGjThreads / 32; w++)
         if (wbest[w] > pb || (wbest[w] == pb && wbi[w] < pv)) { pb = wbest[w]; pv = wbi[w]; }
       if (t == 0) perm[k] = pv;
       // read phase: the pivot row (old row pv, scaled) to sRk, and the old row
       // k, which moves to row pv, to sOk
-      const double piv = P[kk * M + pv];
-      if (piv == 0.0) bad = bad ? bad : k + 1;
-      const double d = (piv != 0.0) ? 1.0 / piv : 0.0;
+      const TV piv = P[kk * M + pv];
+      if (piv == (TV)0) bad = bad ? bad : k + 1;
+      const TV d = (piv != (TV)0) ? (TV)1 / piv : (TV)0;
       if (t < nb) {
         sRk[t] = (t == kk) ? d : P[t * M + pv] * d;
         sOk[t] = P[t * M + k];
@@ -205,10 +208,10 @@ pc_gj_invert_kernel(const int *__restrict__ list, const int *__restrict__ bStart
         if (i == k) {
           for (int c = 0; c < nb; c++) P[c * M + k] = sRk[c];
         } else if (i == pv) {   // (only reached when pv != k) the old row k, eliminated
-          const double f = sOk[kk];
+          const TV f = sOk[kk];
           for (int c = 0; c < nb; c++) P[c * M + i] = (c == kk) ? -f * d : sOk[c] - f * sRk[c];
         } else {
-          const double f = P[kk * M + i];
+          const TV f = P[kk * M + i];
           for (int c = 0; c < nb; c++) P[c * M + i] = (c == kk) ? -f * d : P[c * M + i] - f * sRk[c];
         }
       }
@@ -250,8 +253,8 @@ pc_gj_invert_kernel(const int *__restrict__ list, const int *__restrict__ bStart
     for (int jt = 64 * rank; jt < M; jt += 64 * CS)
       for (int j = jt + warp; j < min(M, jt + 64); j += kGjThreads / 32) {
         if (j >= k0 && j < k0 + nb) continue;
-        double *col = A + (size_t)j * M;
-        double v = 0.0;
+        TV *col = A + (size_t)j * M;
+        TV v = (TV)0;
         int r = -1;
         if (lane < cnt) {
           r = sPos[lane];
@@ -261,7 +264,7 @@ pc_gj_invert_kernel(const int *__restrict__ list, const int *__restrict__ bStart
         if (lane < cnt) {
           if (r >= k0 && r < k0 + nb) {
             Y[(size_t)j * NB + (r - k0)] = v;
-            col[r] = 0.0;
+            col[r] = (TV)0;
           } else {
             col[r] = v;
           }
@@ -274,26 +277,26 @@ pc_gj_invert_kernel(const int *__restrict__ list, const int *__restrict__ bStart
       for (int e = t; e < 64 * NB; e += kGjThreads) {
         const int jl = e / NB, kk = e % NB, j = jt + jl;
         const bool ok = j < M && (j < k0 || j >= k0 + nb) && kk < nb;
-        Yt[e] = ok ? Y[(size_t)j * NB + kk] : 0.0;
+        Yt[e] = ok ? Y[(size_t)j * NB + kk] : (TV)0;
       }
       __syncthreads();
       // row tiles, the next tile's A values loaded while the current one is computed
-      auto load_tile = [&](int it, double (&v)[4][4]) {
+      auto load_tile = [&](int it, TV (&v)[4][4]) {
         const int i0 = it + 4 * tr;
         const bool in = i0 < M, full = i0 + 4 <= M;   // M is even: a row quad is full or holds two rows
 #pragma unroll
         for (int c = 0; c < 4; c++) {
           const int j = jt + 4 * tc + c;
           if (in && j < M) {
-            const double2 *src = reinterpret_cast<const double2 *>(A + (size_t)j * M + i0);
-            const double2 lo = src[0], hi = full ? src[1] : make_double2(0.0, 0.0);
+            const V2 *src = reinterpret_cast<const V2 *>(A + (size_t)j * M + i0);
+            const V2 lo = src[0], hi = full ? src[1] : V2{(TV)0, (TV)0};
             v[c][0] = lo.x; v[c][1] = lo.y; v[c][2] = hi.x; v[c][3] = hi.y;
           } else {
-            v[c][0] = v[c][1] = v[c][2] = v[c][3] = 0.0;
+            v[c][0] = v[c][1] = v[c][2] = v[c][3] = (TV)0;
           }
         }
       };
-      double acc[4][4], nxt[4][4];
+      TV acc[4][4], nxt[4][4];
       load_tile(0, acc);
       for (int it = 0; it < M; it += 64) {
         const int i0 = it + 4 * tr;
@@ -301,10 +304,10 @@ pc_gj_invert_kernel(const int *__restrict__ list, const int *__restrict__ bStart
         if (i0 < M) {
           const bool full = i0 + 4 <= M;
           for (int kk = 0; kk < nb; kk++) {
-            const double2 *pw = reinterpret_cast<const double2 *>(P + (size_t)kk * M + i0);
-            const double2 wlo = pw[0], whi = full ? pw[1] : make_double2(0.0, 0.0);
-            const double w[4] = {wlo.x, wlo.y, whi.x, whi.y};
-            double y[4];
+            const V2 *pw = reinterpret_cast<const V2 *>(P + (size_t)kk * M + i0);
+            const V2 wlo = pw[0], whi = full ? pw[1] : V2{(TV)0, (TV)0};
+            const TV w[4] = {wlo.x, wlo.y, whi.x, whi.y};
+            TV y[4];
 #pragma unroll
             for (int c = 0; c < 4; c++) y[c] = Yt[(4 * tc + c) * NB + kk];
 #pragma unroll
@@ -316,9 +319,9 @@ pc_gj_invert_kernel(const int *__restrict__ list, const int *__restrict__ bStart
           for (int c = 0; c < 4; c++) {
             const int j = jt + 4 * tc + c;
             if (j < M && (j < k0 || j >= k0 + nb)) {
-              double2 *dst = reinterpret_cast<double2 *>(A + (size_t)j * M + i0);
-              dst[0] = make_double2(acc[c][0], acc[c][1]);
-              if (full) dst[1] = make_double2(acc[c][2], acc[c][3]);
+              V2 *dst = reinterpret_cast<V2 *>(A + (size_t)j * M + i0);
+              dst[0] = V2{acc[c][0], acc[c][1]};
+              if (full) dst[1] = V2{acc[c][2], acc[c][3]};
             }
           }
         }
@@ -519,25 +522,25 @@ static bool factor_cusolver(Context &c, PrecondDev &p, const std::vector<int> &b
   return true;
 }
 
-// Blocks up to this size go to the Gauss-Jordan kernel, one thread block
-// each; larger ones to cuSOLVER (several streams).  The kernel takes up to
-// kGjMaxM (its panel of NB columns lives in shared memory); measured on the
-// 204,800-panel star surface, sending everything to the kernel is fastest
-// (cuSOLVER launches run slowly beside the kernel's resident blocks).
+// Blocks up to this many rows (and up to the size classes below) go to the
+// Gauss-Jordan kernel; larger ones to cuSOLVER (several streams, FP64 only).
+// Measured on the 204,800-panel star surface, sending everything to the
+// kernel is fastest (cuSOLVER launches run slowly beside the kernel's
+// resident blocks).
 #ifndef FB_PC_GJ_MAXM
-#define FB_PC_GJ_MAXM 3200
+#define FB_PC_GJ_MAXM 11000
 #endif
 // CTAs per block for blocks of 385-768 rows (1 or 2; 1600+ rows use 8)
 #ifndef FB_PC_GJ_MIDCS
 #define FB_PC_GJ_MIDCS 2
 #endif
-constexpr int kGjMaxM = 3200;
 
-template <int NB, int CS>
+template <typename TV, int NB, int CS>
 static bool launch_gj_t(int nList, int maxM, cudaStream_t st, const int *d_list, PrecondDev &p, const long long *d_yOff,
-                        double *d_y, int *d_info) {
-  const size_t shm = gj_smem_bytes<NB>(maxM);
-  FB_CUDA(cudaFuncSetAttribute(pc_gj_invert_kernel<NB, CS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+                        TV *inv, TV *d_y, int *d_info) {
+  const size_t shm = gj_smem_bytes<TV, NB>(maxM);
+  FB_CUDA(cudaFuncSetAttribute(pc_gj_invert_kernel<TV, NB, CS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)shm));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(nList * CS));
   cfg.blockDim = dim3(kGjThreads);
@@ -550,31 +553,59 @@ static bool launch_gj_t(int nList, int maxM, cudaStream_t st, const int *d_list,
   attr[0].val.clusterDim.z = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  FB_CUDA(cudaLaunchKernelEx(&cfg, pc_gj_invert_kernel<NB, CS>, d_list, (const int *)p.d_start,
-                             (const int *)p.d_size, (const long long *)p.d_off, d_yOff, p.d_inv, d_y, p.d_colSrc,
+  FB_CUDA(cudaLaunchKernelEx(&cfg, pc_gj_invert_kernel<TV, NB, CS>, d_list, (const int *)p.d_start,
+                             (const int *)p.d_size, (const long long *)p.d_off, d_yOff, inv, d_y, p.d_colSrc,
                              d_info));
   return true;
 }
 
+template <typename TV>
 static bool launch_gj(int nb, int cs, int nList, int maxM, cudaStream_t st, const int *d_list, PrecondDev &p,
-                      const long long *d_yOff, double *d_y, int *d_info) {
-  if (nb == 16 && cs == 1) return launch_gj_t<16, 1>(nList, maxM, st, d_list, p, d_yOff, d_y, d_info);
-  if (nb == 16 && cs == 2) return launch_gj_t<16, 2>(nList, maxM, st, d_list, p, d_yOff, d_y, d_info);
-  if (nb == 16 && cs == 8) return launch_gj_t<16, 8>(nList, maxM, st, d_list, p, d_yOff, d_y, d_info);
-  return launch_gj_t<8, 8>(nList, maxM, st, d_list, p, d_yOff, d_y, d_info);
+                      const long long *d_yOff, TV *inv, TV *d_y, int *d_info) {
+  if (nb == 16 && cs == 1) return launch_gj_t<TV, 16, 1>(nList, maxM, st, d_list, p, d_yOff, inv, d_y, d_info);
+  if (nb == 16 && cs == 2) return launch_gj_t<TV, 16, 2>(nList, maxM, st, d_list, p, d_yOff, inv, d_y, d_info);
+  if (nb == 16 && cs == 8) return launch_gj_t<TV, 16, 8>(nList, maxM, st, d_list, p, d_yOff, inv, d_y, d_info);
+  if (nb == 8 && cs == 8) return launch_gj_t<TV, 8, 8>(nList, maxM, st, d_list, p, d_yOff, inv, d_y, d_info);
+  if constexpr (sizeof(TV) == 4) return launch_gj_t<TV, 4, 8>(nList, maxM, st, d_list, p, d_yOff, inv, d_y, d_info);
+  set_error("no Gauss-Jordan class with panel width %d", nb);
+  return false;
 }
 
-// Gauss-Jordan inversion of every block in p.d_inv (assembled there), size
-// classes on their own streams so the large blocks start at once.
-static bool factor_hybrid(Context &c, PrecondDev &p) {
+// Size classes of the Gauss-Jordan kernel per precision: rows up to, panel
+// width NB, CTAs per block (the panel of NB columns and the pivot record fit
+// in shared memory).  Blocks above the last class go to cuSOLVER (FP64).
+struct GjCls { int hi, nb, cs; };
+template <typename TV>
+static const GjCls *gj_classes(int *count) {
+  // FP64 stops at 3200 rows: above it cuSOLVER's factorisation of a single
+  // large block (all SMs) beats the kernel's narrow panels (measured on a
+  // 2.1M-panel surface: 7.9 s against 9.8 s for the whole inversion)
+  static const GjCls d64[4] = {{384, 16, 1}, {768, 16, FB_PC_GJ_MIDCS}, {1600, 16, 8}, {3200, 8, 8}};
+  static const GjCls d32[5] = {{384, 16, 1}, {768, 16, FB_PC_GJ_MIDCS}, {3200, 16, 8}, {6000, 8, 8}, {11000, 4, 8}};
+  *count = sizeof(TV) == 8 ? 4 : 5;
+  return sizeof(TV) == 8 ? d64 : d32;
+}
+
+template <typename TV>
+static int gj_max_rows() {
+  int n = 0;
+  const GjCls *c = gj_classes<TV>(&n);
+  return std::min(c[n - 1].hi, FB_PC_GJ_MAXM);
+}
+
+// Gauss-Jordan inversion of every block of inv (assembled there), size
+// classes on their own streams so the large blocks start at once; blocks
+// above the kernel's size limit (FP64 only) go to cuSOLVER meanwhile.
+template <typename TV>
+static bool factor_gauss_jordan(Context &c, PrecondDev &p, TV *inv) {
   cudaStream_t s = c.stream;
-  struct Cls { int lo, hi, nb, cs; };   // rows, panel width, CTAs per block
-  const int cut = std::min(FB_PC_GJ_MAXM, kGjMaxM);
-  const Cls cls[4] = {{0, std::min(384, cut), 16, 1}, {std::min(384, cut), std::min(768, cut), 16, FB_PC_GJ_MIDCS},
-                      {std::min(768, cut), std::min(1600, cut), 16, 8}, {std::min(1600, cut), cut, 8, 8}};
+  const int cut = gj_max_rows<TV>();
+  int ncls = 0;
+  const GjCls *cls = gj_classes<TV>(&ncls);
   std::vector<int> big;
   for (int b = 0; b < p.nBlocks; b++)
     if (2 * p.hSize[b] > cut) big.push_back(b);
+  FB_CHECK(big.empty() || sizeof(TV) == 8, "preconditioner block of %d rows above the FP32 limit %d", p.maxM, cut);
   std::vector<long long> yOff(p.nBlocks);
   long long ytot = 0;
   for (int b = 0; b < p.nBlocks; b++) {
@@ -582,7 +613,7 @@ static bool factor_hybrid(Context &c, PrecondDev &p) {
     ytot += 16LL * 2 * p.hSize[b];
   }
   long long *d_yOff = nullptr;
-  double *d_y = nullptr;
+  TV *d_y = nullptr;
   int *d_info = nullptr;
   DevArena tmp;
   if (!tmp.upload(&d_yOff, yOff, s) || !tmp.alloc_n(&d_y, (size_t)std::max(ytot, 1LL)) ||
@@ -594,12 +625,14 @@ static bool factor_hybrid(Context &c, PrecondDev &p) {
   FB_CUDA(cudaEventRecord(evA, s));
   std::vector<cudaStream_t> ss;
   bool ok = true;
-  for (const Cls &k : cls) {
+  for (int ci = 0; ci < ncls; ci++) {
+    const GjCls &k = cls[ci];
+    const int lo = ci ? cls[ci - 1].hi : 0, hi = std::min(k.hi, cut);
     std::vector<int> list;
     int maxM = 0;
     for (int b = 0; b < p.nBlocks; b++) {
       const int M = 2 * p.hSize[b];
-      if (k.hi > k.lo && M > k.lo && M <= k.hi) {
+      if (hi > lo && M > lo && M <= hi) {
         list.push_back(b);
         maxM = std::max(maxM, M);
       }
@@ -616,7 +649,7 @@ static bool factor_hybrid(Context &c, PrecondDev &p) {
          cudaStreamWaitEvent(st, evL, 0) == cudaSuccess;
     if (evL) cudaEventDestroy(evL);
     if (!ok) break;
-    if (!launch_gj(k.nb, k.cs, (int)list.size(), maxM, st, d_list, p, d_yOff, d_y, d_info)) {
+    if (!launch_gj<TV>(k.nb, k.cs, (int)list.size(), maxM, st, d_list, p, d_yOff, inv, d_y, d_info)) {
       ok = false;
       break;
     }
@@ -624,7 +657,9 @@ static bool factor_hybrid(Context &c, PrecondDev &p) {
     ok = cudaGetLastError() == cudaSuccess;
   }
   // the large blocks meanwhile, through cuSOLVER on its own streams
-  if (ok) ok = factor_cusolver(c, p, big);
+  if (ok && !big.empty()) {
+    if constexpr (sizeof(TV) == 8) ok = factor_cusolver(c, p, big);
+  }
   for (cudaStream_t st : ss) {
     cudaEvent_t ev = nullptr;
     if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) == cudaSuccess) {
@@ -646,11 +681,6 @@ static bool factor_hybrid(Context &c, PrecondDev &p) {
   for (int b = 0; b < p.nBlocks; b++)
     FB_CHECK(info[b] == 0, "zero pivot in preconditioner block %d (step %d)", b, info[b]);
   return true;
-}
-
-__global__ void to_float_kernel(long long n, const double *__restrict__ a, float *b) {
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-    b[i] = (float)a[i];
 }
 
 bool precond_setup(Context &c, int mode) {
@@ -683,28 +713,32 @@ bool precond_setup(Context &c, int mode) {
       !p.arena.upload(&p.d_tiles, tiles, s) || !p.arena.upload(&p.d_off, p.hOff, s) ||
       !p.arena.alloc_n(&p.d_colSrc, 2 * (size_t)c.n))
     return false;
-  // the inversion works in FP64; a mixed context keeps an FP32 copy only
-  if (c.mixed) FB_CUDA(cudaMalloc((void **)&p.d_inv, (size_t)off * sizeof(double)));
-  else if (!p.arena.alloc_n(&p.d_inv, (size_t)off)) return false;
+  // FP64 contexts invert in FP64; mixed contexts assemble and invert in FP32
+  // (the preconditioner only steers GMRES; its inverse is stored in FP32)
   const double s1 = (1.0 + c.epsilon) / 2.0, s2 = (1.0 + 1.0 / c.epsilon) / 2.0;
   dim3 grid(64, p.nBlocks);
-  pc_assemble_kernel<<<grid, 128, 0, s>>>(p.nBlocks, p.d_start, p.d_size, p.d_off, c.d_vtx, c.d_nrm, c.d_area,
-                                          c.prm.quad_order, c.prm.kappa, c.epsilon, s1, s2, p.d_inv);
-  c.launches += 1;
-  FB_CUDA(cudaGetLastError());
-  tm.mark("assemble");
-  bool ok = factor_hybrid(c, p);
-  tm.mark("factor_invert");
+  bool ok;
   if (c.mixed) {
-    if (ok) ok = p.arena.alloc_n(&p.d_invF, (size_t)off);
-    if (ok) {
-      to_float_kernel<<<1184, 256, 0, s>>>(off, p.d_inv, p.d_invF);
-      ok = cudaGetLastError() == cudaSuccess && cudaStreamSynchronize(s) == cudaSuccess;
-    }
-    cudaFree(p.d_inv);
-    p.d_inv = nullptr;
-    FB_CHECK(ok, "preconditioner FP32 copy failed: %s", get_error());
+    FB_CHECK(p.maxM <= gj_max_rows<float>(), "preconditioner block of %d rows above the FP32 limit %d", p.maxM,
+             gj_max_rows<float>());
+    if (!p.arena.alloc_n(&p.d_invF, (size_t)off)) return false;
+    pc_assemble_kernel<float><<<grid, 128, 0, s>>>(p.nBlocks, p.d_start, p.d_size, p.d_off, c.d_vtx, c.d_nrm, c.d_area,
+                                                   c.prm.quad_order, c.prm.kappa, c.epsilon, s1, s2, p.d_invF);
+    c.launches += 1;
+    FB_CUDA(cudaGetLastError());
+    tm.mark("assemble");
+    ok = factor_gauss_jordan<float>(c, p, p.d_invF);
+  } else {
+    if (!p.arena.alloc_n(&p.d_inv, (size_t)off)) return false;
+    pc_assemble_kernel<double><<<grid, 128, 0, s>>>(p.nBlocks, p.d_start, p.d_size, p.d_off, c.d_vtx, c.d_nrm,
+                                                    c.d_area, c.prm.quad_order, c.prm.kappa, c.epsilon, s1, s2,
+                                                    p.d_inv);
+    c.launches += 1;
+    FB_CUDA(cudaGetLastError());
+    tm.mark("assemble");
+    ok = factor_gauss_jordan<double>(c, p, p.d_inv);
   }
+  tm.mark("factor_invert");
   return ok;
 }
 
