@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 #include <unordered_map>
 
 #include "context.cuh"
@@ -528,28 +529,49 @@ bool setup_near(Context &c) {
     nearSorted[L].assign(pt.nearSrc.begin() + pt.nearOff[L], pt.nearSrc.begin() + pt.nearOff[L + 1]);
     std::sort(nearSorted[L].begin(), nearSorted[L].end());
   }
+  // per panel: itself and the panels sharing a vertex with it, ascending,
+  // kept when their leaves are near; chunks of panels on host threads, merged
+  // in panel order
   std::vector<int> spOff(n + 1, 0), spDst, spSrc;
-  spDst.reserve(16 * (size_t)n);
-  spSrc.reserve(16 * (size_t)n);
-  std::vector<int> cand;
-  for (int X = 0; X < n; X++) {
-    cand.clear();
-    cand.push_back(X);
-    for (int k = 0; k < 3; k++) {
-      int v = pv[3 * (size_t)X + k];
-      for (int e = vOff[v]; e < vOff[v + 1]; e++) cand.push_back(vPan[e]);
-    }
-    std::sort(cand.begin(), cand.end());
-    cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
-    const std::vector<int> &ns = nearSorted[leafOf[X]];
-    for (int Y : cand) {
-      if (std::binary_search(ns.begin(), ns.end(), leafOf[Y])) {
-        spDst.push_back(X);
-        spSrc.push_back(Y);
+  const int nth = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+  std::vector<std::vector<int>> partSrc(nth);
+  std::vector<int> cntOf(n, 0);
+  auto work_range = [&](int th) {
+    const int x0 = (int)((long long)n * th / nth), x1 = (int)((long long)n * (th + 1) / nth);
+    std::vector<int> cand;
+    std::vector<int> &out = partSrc[th];
+    out.reserve(16 * (size_t)(x1 - x0));
+    for (int X = x0; X < x1; X++) {
+      cand.clear();
+      cand.push_back(X);
+      for (int k = 0; k < 3; k++) {
+        int v = pv[3 * (size_t)X + k];
+        for (int e = vOff[v]; e < vOff[v + 1]; e++) cand.push_back(vPan[e]);
       }
+      std::sort(cand.begin(), cand.end());
+      cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+      const std::vector<int> &ns = nearSorted[leafOf[X]];
+      int cnt = 0;
+      for (int Y : cand)
+        if (std::binary_search(ns.begin(), ns.end(), leafOf[Y])) {
+          out.push_back(Y);
+          cnt++;
+        }
+      cntOf[X] = cnt;
     }
-    spOff[X + 1] = (int)spSrc.size();
+  };
+  {
+    std::vector<std::thread> pool;
+    for (int th = 1; th < nth; th++) pool.emplace_back(work_range, th);
+    work_range(0);
+    for (auto &th : pool) th.join();
   }
+  for (int X = 0; X < n; X++) spOff[X + 1] = spOff[X] + cntOf[X];
+  spSrc.reserve(spOff[n]);
+  for (int th = 0; th < nth; th++) spSrc.insert(spSrc.end(), partSrc[th].begin(), partSrc[th].end());
+  spDst.resize(spSrc.size());
+  for (int X = 0; X < n; X++)
+    for (int e = spOff[X]; e < spOff[X + 1]; e++) spDst[e] = X;
   c.nSpecial = (long long)spSrc.size();
   tm.mark("special_pairs_host");
   int *d_spDst = nullptr;
