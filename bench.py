@@ -381,7 +381,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            surf.matvec(xh_np, 1.0, 0.0, yh_np)
+            surf.matvec(xh_np, 1.0, 0.0, out=yh_np)
         e2e_s = time.perf_counter() - t0
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     near_ms = [s.elapsed_time(e) for s, e in zip(nstarts, nends)]

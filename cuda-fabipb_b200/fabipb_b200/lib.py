@@ -199,12 +199,25 @@ class Surface:
         _check(load().fabipb_b200_apply(self.h, part, alpha, _ptr(sgm), beta, _ptr(pot), 0), "apply")
         return pot
 
-    def matvec(self, x, alpha=1.0, beta=0.0, y=None, on_device=0):
+    def _host_out(self, y, out, beta):
+        """The host array the library writes: `out` itself when it is a
+        writeable C-contiguous float64 array of 2N (no copy: a pinned buffer
+        stays pinned), else a fresh array; holds y on entry when beta != 0."""
+        if (out is not None and isinstance(out, np.ndarray) and out.dtype == np.float64 and out.flags.c_contiguous
+                and out.flags.writeable and out.size == 2 * self.n):
+            if beta != 0.0 and y is not None and y is not out:
+                out[:] = y
+            return out
+        return np.zeros(2 * self.n) if y is None else np.array(y, dtype=np.float64)
+
+    def matvec(self, x, alpha=1.0, beta=0.0, y=None, on_device=0, out=None):
+        """y_new = alpha*(D - K)x + beta*y; host arrays are not modified
+        unless `out` is given, which receives the result in place."""
         if on_device:
             _check(load().fabipb_b200_matvec(self.h, alpha, _ptr(x), beta, _ptr(y), 1), "matvec")
             return y
         x = np.ascontiguousarray(x, dtype=np.float64)
-        y = np.zeros(2 * self.n) if y is None else np.array(y, dtype=np.float64)
+        y = self._host_out(y, out, beta)
         _check(load().fabipb_b200_matvec(self.h, alpha, _ptr(x), beta, _ptr(y), 0), "matvec")
         return y
 
