@@ -169,18 +169,18 @@ pc_gj_invert_kernel(const int *__restrict__ list, const int *__restrict__ bStart
     }
     for (int e = t; e < nb * M; e += kGjThreads) P[e] = A[(size_t)k0 * M + e];   // columns k0.. are contiguous
     __syncthreads();
-    // Row i of the panel belongs to thread i mod kGjThreads throughout, so a
-    // step's pivot search reads only rows its thread wrote in the previous
-    // step: two barriers per step.
+    // Row i of the panel belongs to thread i mod kGjThreads throughout: each
+    // step's write phase also finds the thread's candidate pivot of the next
+    // column among its own rows, so a step needs two barriers.
+    TV best = (TV)-1;
+    int bi = M;
+    for (int i = t; i < M; i += kGjThreads) {
+      if (i < k0) continue;
+      const TV v = fabs(P[i]);
+      if (v > best) { best = v; bi = i; }
+    }
     for (int kk = 0; kk < nb; kk++) {
       const int k = k0 + kk;
-      TV best = (TV)-1;
-      int bi = M;
-      for (int i = t; i < M; i += kGjThreads) {
-        if (i < k) continue;
-        const TV v = fabs(P[kk * M + i]);
-        if (v > best) { best = v; bi = i; }
-      }
       for (int o = 16; o > 0; o >>= 1) {   // first largest within the warp
         const TV ob = __shfl_xor_sync(0xffffffffu, best, o);
         const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
@@ -193,29 +193,39 @@ pc_gj_invert_kernel(const int *__restrict__ list, const int *__restrict__ bStart
       for (int w = 1; w < kGjThreads / 32; w++)
         if (wbest[w] > pb || (wbest[w] == pb && wbi[w] < pv)) { pb = wbest[w]; pv = wbi[w]; }
       if (t == 0) perm[k] = pv;
-      // read phase: the pivot row (old row pv, scaled) to sRk, and the old row
-      // k, which moves to row pv, to sOk
-      const TV piv = P[kk * M + pv];
-      if (piv == (TV)0) bad = bad ? bad : k + 1;
-      const TV d = (piv != (TV)0) ? (TV)1 / piv : (TV)0;
+      // read phase: the pivot row (old row pv, scaled; sRk[kk] = 1/pivot) and
+      // the old row k, which moves to row pv
       if (t < nb) {
+        const TV piv = P[kk * M + pv];
+        const TV d = (piv != (TV)0) ? (TV)1 / piv : (TV)0;
         sRk[t] = (t == kk) ? d : P[t * M + pv] * d;
         sOk[t] = P[t * M + k];
       }
+      if (P[kk * M + pv] == (TV)0) bad = bad ? bad : k + 1;
       __syncthreads();
-      // write phase
+      // write phase, and the candidates for the next column
+      const TV d = sRk[kk];
+      best = (TV)-1;
+      bi = M;
+      const bool more = kk + 1 < nb;
       for (int i = t; i < M; i += kGjThreads) {
         if (i == k) {
           for (int c = 0; c < nb; c++) P[c * M + k] = sRk[c];
-        } else if (i == pv) {   // (only reached when pv != k) the old row k, eliminated
+          continue;   // the pivot row is no candidate
+        }
+        if (i == pv) {   // (only reached when pv != k) the old row k, eliminated
           const TV f = sOk[kk];
           for (int c = 0; c < nb; c++) P[c * M + i] = (c == kk) ? -f * d : sOk[c] - f * sRk[c];
         } else {
           const TV f = P[kk * M + i];
           for (int c = 0; c < nb; c++) P[c * M + i] = (c == kk) ? -f * d : P[c * M + i] - f * sRk[c];
         }
+        if (more && i > k) {
+          const TV v = fabs(P[(kk + 1) * M + i]);
+          if (v > best) { best = v; bi = i; }
+        }
       }
-      __syncthreads();   // sRk/sOk are rewritten by the next step; its search reads own rows only
+      // the next step's first barrier orders this write phase before its reads
     }
     __syncthreads();
     if (rank == 0)
