@@ -1,13 +1,15 @@
 """Benchmark of the FABIPB GMRES matvec on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision mixed|fp64] [--case star204800|sphere20480]
+                    [--precision mixed|fp64] [--case star204800|star2097152|sphere20480]
 
 Workload (one "step" = one operator application y = (D - K)x, the GMRES
 matvec of src/fabipb.c:1237): the star-shaped globular surface of 204,800
 flat triangles (octahedral geodesic, frequency 160, radius 25 A perturbed by
 l=2..6 harmonics), Taylor order p=4, MAC ratio 0.7, octree depth 5 (mean
 leaf 46 panels), eps 2/80, kappa 0.1257, synthetic seeded inputs.
+--case star2097152 runs the same measurement on the 2,097,152-panel star
+(frequency 512, radius 50 A, depth 6, 100,000 charges).
 
 Reported:
   value      matvec/s with x, y resident in HBM (device time, CUDA events on
@@ -47,9 +49,13 @@ CASES = {
     # name: (generator, kwargs, solver options)
     "star204800": ("star", dict(freq=160, radius=25.0, n_charges=20000, seed=1),
                    dict(order=4, depth=5, sep_ratio=0.7, eps1=2.0, eps2=80.0, tol=1e-5, restart=10)),
+    # the north-star size: 2,097,152 triangles (octahedral freq 512, radius 50 A), 100,000 charges
+    "star2097152": ("star", dict(freq=512, radius=50.0, n_charges=100000, seed=7),
+                    dict(order=4, depth=6, sep_ratio=0.7, eps1=2.0, eps2=80.0, tol=1e-6, restart=10)),
     "sphere20480": ("sphere", dict(nsub=5, radius=20.0, n_charges=500, seed=0),
                     dict(order=3, depth=3, sep_ratio=0.8, eps1=1.0, eps2=80.0, tol=1e-4, restart=10)),
 }
+PANELS = {"star204800": 204800, "star2097152": 2097152, "sphere20480": 20480}
 METRIC = "matvec/s"
 FLOP_PER_PAIR = 60.0   # algorithmic count per near panel pair (KER4 + apply)
 
@@ -187,8 +193,8 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "matvec/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded star surface, 204,800 panels)",
-            "config": {"workload": name, "panels": 204800 if name == "star204800" else 20480,
+            "data": "synthetic (seeded %s surface, %d panels)" % (CASES[name][0], PANELS[name]),
+            "config": {"workload": name, "panels": PANELS[name],
                        "order": opts["order"], "depth": opts["depth"], "sep_ratio": opts["sep_ratio"]},
             "cpu_baseline": {"value": value, "unit": "matvec/s", "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": "matvec/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -412,7 +418,8 @@ def run_ours(args):
         peak_src = "FP64 SIMT FMA pipe: %d SMs x 64 lanes x 2 flop x %.0f MHz (median SM clock sampled)" % (n_sm, sm_mhz)
     traffic = None
     # DRAM bytes per launch from the committed ncu summary of this kernel and workload
-    tname = "near_apply_kernel_%s_%s.md" % ("float" if prec == lib.MIXED else "double", args.case)
+    kname = "near_apply_f2_kernel<0>" if prec == lib.MIXED else "near_apply_kernel<double,0>"
+    tname = "%s_%s.md" % ("near_apply_f2_kernel" if prec == lib.MIXED else "near_apply_kernel_double", args.case)
     prof = os.path.join(ROOT, "profiles", tname)
     if os.path.exists(prof):
         with open(prof) as fp:
@@ -428,7 +435,7 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": "matvec/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 * total_s / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec == lib.MIXED else "f64",
-        "data": "synthetic (seeded star surface, 20,000 seeded charges)",
+        "data": "synthetic (seeded %s surface, %d seeded charges)" % (CASES[name][0], CASES[name][1]["n_charges"]),
         "config": {"workload": name, "panels": surf.n, "order": opts["order"], "depth": opts["depth"],
                    "sep_ratio": opts["sep_ratio"], "eps1": opts["eps1"], "eps2": opts["eps2"],
                    "precision": args.precision, "parallelism": "replicas" if world > 1 else "single",
@@ -437,7 +444,7 @@ def run_ours(args):
                    "l2": "256 MiB buffer written between steps, outside the timed intervals"},
         "e2e": {"value": e2e_rate * world, "unit": "matvec/s", "h2d_bytes_per_step": n2 * 8,
                 "d2h_bytes_per_step": n2 * 8},
-        "roofline": {"kernel": "near_apply_kernel<%s>" % ("float" if prec == lib.MIXED else "double"),
+        "roofline": {"kernel": kname,
                      "bound": "fp32" if prec == lib.MIXED else "fp64", "achieved": achieved, "peak": peak,
                      "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_source": peak_src, "flop_per_pair": FLOP_PER_PAIR,
