@@ -9,7 +9,7 @@ flat triangles (octahedral geodesic, frequency 160, radius 25 A perturbed by
 l=2..6 harmonics), Taylor order p=4, MAC ratio 0.7, octree depth 5 (mean
 leaf 46 panels), eps 2/80, kappa 0.1257, synthetic seeded inputs.
 --case star2097152 runs the same measurement on the 2,097,152-panel star
-(frequency 512, radius 50 A, depth 6, 100,000 charges).
+(frequency 512, radius 50 A, depth 7: mean leaf 31 panels, 100,000 charges).
 
 Reported:
   value      matvec/s with x, y resident in HBM (device time, CUDA events on
@@ -51,7 +51,7 @@ CASES = {
                    dict(order=4, depth=5, sep_ratio=0.7, eps1=2.0, eps2=80.0, tol=1e-5, restart=10)),
     # the north-star size: 2,097,152 triangles (octahedral freq 512, radius 50 A), 100,000 charges
     "star2097152": ("star", dict(freq=512, radius=50.0, n_charges=100000, seed=7),
-                    dict(order=4, depth=6, sep_ratio=0.7, eps1=2.0, eps2=80.0, tol=1e-6, restart=10)),
+                    dict(order=4, depth=7, sep_ratio=0.7, eps1=2.0, eps2=80.0, tol=1e-6, restart=10)),
     "sphere20480": ("sphere", dict(nsub=5, radius=20.0, n_charges=500, seed=0),
                     dict(order=3, depth=3, sep_ratio=0.8, eps1=1.0, eps2=80.0, tol=1e-4, restart=10)),
 }
@@ -236,7 +236,7 @@ def pass_report(surf, info, x_ptr, flush, reps, prec_is_mixed, sm_mhz, n_sm):
         "near": ("flop", FLOP_PER_PAIR * info["near_panel_pairs"], near_peak),
         "q2m": ("bytes", 8.0 * (2 * nmom(pl) * n + 2 * n + 2 * nmom(p) * leaves), hbm),
         "m2m": ("bytes", 8.0 * 2 * nmom(p) * 2 * cubes, hbm),
-        "m2l": ("flop", 8.0 * comb(p + 6, 6) * info["m2l_pairs"], fp64),
+        "m2l": ("flop", 8.0 * comb(p + 6, 6) * info["m2l_pairs"], fp32 if prec_is_mixed and p <= 5 else fp64),
         "l2l": ("bytes", 8.0 * 4 * nmom(p) * 2 * cubes, hbm),
         "l2p": ("bytes", 8.0 * (2 * nmom(pl) * n + 4 * nmom(p) * leaves + 6 * n), hbm),
     }
@@ -245,7 +245,7 @@ def pass_report(surf, info, x_ptr, flush, reps, prec_is_mixed, sm_mhz, n_sm):
         t = ms[k] / 1000.0
         if kind == "flop":
             ach = amount / t / 1e12
-            out[k] = {"ms": ms[k], "bound": ("fp32" if (k == "near" and prec_is_mixed) else "fp64"),
+            out[k] = {"ms": ms[k], "bound": ("fp32" if peak == fp32 else "fp64"),
                       "achieved": ach, "unit": "TFLOP/s", "peak": peak, "frac": ach / peak,
                       "algorithmic": amount}
         else:
@@ -257,7 +257,7 @@ def pass_report(surf, info, x_ptr, flush, reps, prec_is_mixed, sm_mhz, n_sm):
     return out
 
 
-def solve_report(pan, ch, opts, device, st):
+def solve_report(pan, ch, opts, device, st, reps=3):
     """Full solves of the same case in both precisions: direct RHS, block-LU
     preconditioner, device GMRES from x0 = b (as the reference CLI), energy.
     Times are CUDA-event times on the library's stream (the calls are
@@ -266,10 +266,13 @@ def solve_report(pan, ch, opts, device, st):
     import torch
     from fabipb_b200 import lib
     out = {}
+    runs = {"mixed": [], "fp64": []}
     kcal = 2.0 * np.pi * 332.0716
-    # each precision runs twice and the second run is reported: the first
-    # pays the one-time loading of the kernels it is the first to use
-    for tag, prec in (("mixed", lib.MIXED), ("mixed", lib.MIXED), ("fp64", lib.FP64), ("fp64", lib.FP64)):
+    # each precision runs 1 + reps times: the first pays the one-time loading
+    # of the kernels it is the first to use and is not reported; every time
+    # reported is the median over the other reps runs
+    seq = [("mixed", lib.MIXED)] * (1 + reps) + [("fp64", lib.FP64)] * (1 + reps)
+    for tag, prec in seq:
         ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         torch.cuda.synchronize()
         w0 = time.perf_counter()
@@ -315,6 +318,21 @@ def solve_report(pan, ch, opts, device, st):
                                "forward_iterations": itf, "backward_iterations": itb, "info": [inff, infb],
                                "charges": int(len(ch.q)), "energy_direct_kcal_mol": ef * kcal}
         s.close()
+        runs[tag].append(out.pop(tag))
+    med = lambda v: float(np.median(v))
+    for tag, rs in runs.items():
+        rs = rs[1:]
+        r = dict(rs[-1])
+        for k in ("gmres_s", "setup_s", "energy_s", "wall_s"):
+            r[k] = med([q[k] for q in rs])
+        r["refined"] = dict(rs[-1]["refined"], gmres_s=med([q["refined"]["gmres_s"] for q in rs]))
+        a = dict(rs[-1]["adjoint"])
+        a["forward_s"] = med([q["adjoint"]["forward_s"] for q in rs])
+        a["backward_s"] = med([q["adjoint"]["backward_s"] for q in rs])
+        a["backward_over_forward"] = a["backward_s"] / a["forward_s"]
+        r["adjoint"] = a
+        r["runs"] = len(rs)
+        out[tag] = r
     m, f = out["mixed"], out["fp64"]
     out["energy_rel_err_mixed_vs_fp64"] = abs(m["energy_kcal_mol"] - f["energy_kcal_mol"]) / abs(f["energy_kcal_mol"])
     out["gmres_speedup_mixed_vs_fp64"] = f["gmres_s"] / m["gmres_s"]

@@ -79,17 +79,28 @@ __global__ void near_targets_kernel(int n, const double *__restrict__ vtx, const
   tgtN[i] = q;
 }
 
+// Source records of one apply: {position, A*sigma_dpdn}, {normal, A*sigma_pot}.
+// scaleNormal 1 (2): the normal is stored multiplied by the second (first)
+// weight, for the packed FP32 kernel, whose pair formula takes the source
+// normal only in terms that carry that weight.
 template <typename T>
 __global__ void near_pack_kernel(int n, const typename Vec4<T>::t *__restrict__ tgtP,
                                  const typename Vec4<T>::t *__restrict__ tgtN, const double *__restrict__ area,
                                  const double *__restrict__ sgm, typename Vec4<T>::t *srcA,
-                                 typename Vec4<T>::t *srcB) {
+                                 typename Vec4<T>::t *srcB, int scaleNormal) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   typename Vec4<T>::t a = tgtP[i], b = tgtN[i];
   double A = area[i];
-  a.w = (T)(A * sgm[n + i]);  // weight of the dpdn density
-  b.w = (T)(A * sgm[i]);      // weight of the potential density
+  const double wa = A * sgm[n + i], wb = A * sgm[i];
+  a.w = (T)wa;  // weight of the dpdn density
+  b.w = (T)wb;  // weight of the potential density
+  if (scaleNormal) {
+    const T w = (T)(scaleNormal == 1 ? wb : wa);
+    b.x *= w;
+    b.y *= w;
+    b.z *= w;
+  }
   srcA[i] = a;
   srcB[i] = b;
 }
@@ -243,7 +254,12 @@ near_apply_kernel(int nWork, const int2 *__restrict__ work, const int *__restric
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
-template <bool ADJ>
+// m = w n_s is the source normal multiplied by the weight of the terms it
+// enters: wb in the forward block (y1 wb = t1(m) (eps c - 1), y3 wb = dd(m)
+// (c - 1) - kap2 e u(m)), wa in the transposed one; so those terms need no
+// weight multiply.  SELF (the target's own leaf, the only tile holding the
+// coincident pair d = 0): 1/r is taken as 0 there, which zeroes every term.
+template <bool ADJ, bool SELF>
 __device__ __forceinline__ void near_pair2(const float4 A, const float4 B, const float4 C, const float4 D, float2 tx,
                                            float2 ty, float2 tz, float2 tnx, float2 tny, float2 tnz, float kappa,
                                            float kexp, float eps, float ieps, float kap2, float2 &acc0,
@@ -253,11 +269,16 @@ __device__ __forceinline__ void near_pair2(const float4 A, const float4 B, const
   const float2 dy = __fadd2_rn(ty, make_float2(A.z, A.w));
   const float2 dz = __fadd2_rn(tz, make_float2(B.x, B.y));
   const float2 wa = make_float2(B.z, B.w), wb = make_float2(D.z, D.w);
-  const float2 snx = make_float2(C.x, C.y), sny = make_float2(C.z, C.w), snz = make_float2(D.x, D.y);
+  const float2 mx = make_float2(C.x, C.y), my = make_float2(C.z, C.w), mz = make_float2(D.x, D.y);
   const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
   float2 g;
-  g.x = r2.x > 0.f ? rsqrt_t(r2.x) : 0.f;   // 1/r, 0 for the coincident pair
-  g.y = r2.y > 0.f ? rsqrt_t(r2.y) : 0.f;
+  if (SELF) {
+    g.x = r2.x > 0.f ? rsqrt_t(r2.x) : 0.f;
+    g.y = r2.y > 0.f ? rsqrt_t(r2.y) : 0.f;
+  } else {   // distinct leaves: distinct panel centroids, r > 0
+    g.x = rsqrt_t(r2.x);
+    g.y = rsqrt_t(r2.y);
+  }
   const float2 r = __fmul2_rn(r2, g);
   const float2 ea = __fmul2_rn(f2(kexp), r);
   float2 e;
@@ -266,26 +287,45 @@ __device__ __forceinline__ void near_pair2(const float4 A, const float4 B, const
   const float2 c = __fmul2_rn(__ffma2_rn(f2(kappa), r, one), e);    // (kappa r + 1) e^{-kappa r}
   const float2 g2 = __fmul2_rn(g, g), h = __fmul2_rn(g2, g);
   const float2 ipX = __ffma2_rn(tnz, dz, __ffma2_rn(tny, dy, __fmul2_rn(tnx, dx)));
-  const float2 ipY = __ffma2_rn(snz, dz, __ffma2_rn(sny, dy, __fmul2_rn(snx, dx)));
-  const float2 ip0 = __ffma2_rn(tnz, snz, __ffma2_rn(tny, sny, __fmul2_rn(tnx, snx)));
+  const float2 ipY = __ffma2_rn(mz, dz, __ffma2_rn(my, dy, __fmul2_rn(mx, dx)));     // w n_s.d
+  const float2 ip0 = __ffma2_rn(tnz, mz, __ffma2_rn(tny, my, __fmul2_rn(tnx, mx)));  // w n_t.n_s
   const float2 t1 = __fmul2_rn(ipY, h), t2 = __fmul2_rn(ipX, h), u = __fmul2_rn(ipX, t1);
-  const float2 y0 = __fmul2_rn(g, __ffma2_rn(e, m1, one));                                   // G0 - Gk
-  const float2 dd = __fmul2_rn(__ffma2_rn(u, f2(-3.f), __fmul2_rn(ip0, g)), g2);             // d2 G0
-  const float2 y3 = __ffma2_rn(dd, __fadd2_rn(c, m1), __fmul2_rn(__fmul2_rn(f2(-kap2), e), u));
+  const float2 y0 = __ffma2_rn(make_float2(-e.x, -e.y), g, g);                       // G0 - Gk
+  const float2 dd = __fmul2_rn(__ffma2_rn(u, f2(-3.f), __fmul2_rn(ip0, g)), g2);     // w d2 G0
+  const float2 cm1 = __fadd2_rn(c, m1);
+  const float2 ke = __fmul2_rn(f2(-kap2), e);
   if (ADJ) {
-    const float2 q1 = __fmul2_rn(t2, __ffma2_rn(f2(-eps), c, one));    // -t2 (eps c - 1)
-    const float2 q2 = __fmul2_rn(t1, __ffma2_rn(f2(-ieps), c, one));   // -t1 (c/eps - 1)
-    acc0 = __ffma2_rn(y3, wa, acc0);
-    acc0 = __ffma2_rn(q1, wb, acc0);
+    // out_pot += y3 wa - t2 (eps c - 1) wb, out_dpdn += y0 wb - t1 (c/eps - 1) wa
+    acc0 = __ffma2_rn(dd, cm1, acc0);
+    acc0 = __ffma2_rn(ke, u, acc0);
+    acc0 = __ffma2_rn(__fmul2_rn(t2, __ffma2_rn(f2(-eps), c, one)), wb, acc0);
     acc1 = __ffma2_rn(y0, wb, acc1);
-    acc1 = __ffma2_rn(q2, wa, acc1);
+    acc1 = __ffma2_rn(t1, __ffma2_rn(f2(-ieps), c, one), acc1);
   } else {
-    const float2 y1 = __fmul2_rn(t1, __ffma2_rn(f2(eps), c, m1));      // eps dGk/dn_y - dG0/dn_y
-    const float2 y2 = __fmul2_rn(t2, __ffma2_rn(f2(ieps), c, m1));     // dGk/dn_x / eps - dG0/dn_x
+    // out_pot += y0 wa + y1 wb, out_dpdn += y2 wa + y3 wb
     acc0 = __ffma2_rn(y0, wa, acc0);
-    acc0 = __ffma2_rn(y1, wb, acc0);
-    acc1 = __ffma2_rn(y2, wa, acc1);
-    acc1 = __ffma2_rn(y3, wb, acc1);
+    acc0 = __ffma2_rn(t1, __ffma2_rn(f2(eps), c, m1), acc0);
+    acc1 = __ffma2_rn(__fmul2_rn(t2, __ffma2_rn(f2(ieps), c, m1)), wa, acc1);
+    acc1 = __ffma2_rn(dd, cm1, acc1);
+    acc1 = __ffma2_rn(ke, u, acc1);
+  }
+}
+
+// one staged tile of up to 32 sources (np packed source pairs) for a target
+template <bool ADJ, bool SELF>
+__device__ __forceinline__ void near_tile2(const float4 (*sP)[4], int np, int k, int sub, float2 tx, float2 ty,
+                                           float2 tz, float2 tnx, float2 tny, float2 tnz, float kappa, float kexp,
+                                           float eps, float ieps, float kap2, float2 &acc0, float2 &acc1) {
+  if (k == 1) {   // warp-uniform: a full group
+#pragma unroll 2
+    for (int q = 0; q < np; q++)
+      near_pair2<ADJ, SELF>(sP[q][0], sP[q][1], sP[q][2], sP[q][3], tx, ty, tz, tnx, tny, tnz, kappa, kexp, eps,
+                            ieps, kap2, acc0, acc1);
+  } else {
+#pragma unroll 2
+    for (int q = sub; q < np; q += k)
+      near_pair2<ADJ, SELF>(sP[q][0], sP[q][1], sP[q][2], sP[q][3], tx, ty, tz, tnx, tny, tnz, kappa, kexp, eps,
+                            ieps, kap2, acc0, acc1);
   }
 }
 
@@ -336,17 +376,12 @@ near_apply_f2_kernel(int nWork, const int2 *__restrict__ work, const int *__rest
       pf[8] = b.x; pf[10] = b.y; pf[12] = b.z; pf[14] = b.w;
       __syncwarp();
       const int np = (m + 1) >> 1;
-      if (k == 1) {   // warp-uniform: a full group
-#pragma unroll 2
-        for (int q = 0; q < np; q++)
-          near_pair2<ADJ>(sP[warp][q][0], sP[warp][q][1], sP[warp][q][2], sP[warp][q][3], tx, ty, tz, tnx, tny,
-                          tnz, kappa, kexp, eps, ieps, kap2, acc0, acc1);
-      } else {
-#pragma unroll 2
-        for (int q = sub; q < np; q += k)
-          near_pair2<ADJ>(sP[warp][q][0], sP[warp][q][1], sP[warp][q][2], sP[warp][q][3], tx, ty, tz, tnx, tny,
-                          tnz, kappa, kexp, eps, ieps, kap2, acc0, acc1);
-      }
+      if (S == L)   // warp-uniform
+        near_tile2<ADJ, true>(sP[warp], np, k, sub, tx, ty, tz, tnx, tny, tnz, kappa, kexp, eps, ieps, kap2, acc0,
+                              acc1);
+      else
+        near_tile2<ADJ, false>(sP[warp], np, k, sub, tx, ty, tz, tnx, tny, tnz, kappa, kexp, eps, ieps, kap2, acc0,
+                               acc1);
       __syncwarp();
     }
   }
@@ -611,9 +646,10 @@ static void launch_near_t(Context &c, const void *tgtP, const void *tgtN, void *
   const double kap = c.prm.kappa, eps = c.epsilon;
   const unsigned grid = ceil_div(c.nWork, kNearWarps);
   const double kexp = sizeof(T) == 4 ? -kap * 1.4426950408889634 : -kap;   // float: exp2 argument
+  const bool packed = sizeof(T) == 4 && FB_NEAR_PACKED;
   near_pack_kernel<T><<<ceil_div(n, 256), 256, 0, s>>>(n, (const V *)tgtP, (const V *)tgtN, c.d_area, sgm, (V *)srcA,
-                                                       (V *)srcB);
-  if (sizeof(T) == 4 && FB_NEAR_PACKED) {
+                                                       (V *)srcB, packed ? (ADJ ? 2 : 1) : 0);
+  if (packed) {
     near_apply_f2_kernel<ADJ><<<grid, kNearWarps * 32, 0, s>>>(
         c.nWork, c.d_work, c.d_leafStart, c.d_leafCount, c.d_nearOff, c.d_nearSrc, c.d_leafCtr,
         (const float4 *)tgtP, (const float4 *)tgtN, (const float4 *)srcA, (const float4 *)srcB, c.d_spOff, c.d_spSrc,

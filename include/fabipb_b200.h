@@ -92,8 +92,9 @@ int fabipb_b200_matvec(void *ctx, double alpha, const double *x, double beta, do
 /* iterative refinement (no counterpart in the reference): FP64 residuals
    r = b - A x (in a mixed context through the FP64 near-field P2P), each
    correction solved by GMRES with the context's operator (the FP32 P2P in a
-   mixed context) to the relative tolerance tol_inner from zero, x += d,
-   until ||P^-1 r|| / ||b|| <= tol.  x holds the initial guess.  *outer =
+   mixed context) from zero to the relative tolerance tol_inner, or only to
+   half the reduction the outer tolerance still needs (0.5 tol ||b|| / ||r||)
+   when that is looser, x += d, until ||P^-1 r|| / ||b|| <= tol.  x holds the initial guess.  *outer =
    corrections made, *iters = inner GMRES iterations in total (at most
    maxit), *info = 0 converged, 1 out of iterations, 2 NaN. */
 int fabipb_b200_solve_refined(void *ctx, const double *b, double *x, int restart, int maxit, double tol_inner,
