@@ -496,6 +496,15 @@ __host__ __device__ constexpr int m2l_entries() {
 #ifndef FB_M2L_MIN_BLOCKS
 #define FB_M2L_MIN_BLOCKS 3
 #endif
+// moment staging of m2l_unrolled_kernel: flattened over (source, coefficient)
+// with this many loads in flight per lane (0: one source at a time)
+#ifndef FB_M2L_STAGE_FLAT
+#define FB_M2L_STAGE_FLAT 1
+#endif
+#ifndef FB_M2L_STAGE_UNROLL
+#define FB_M2L_STAGE_UNROLL 8
+#endif
+constexpr int kM2LStageUnroll = FB_M2L_STAGE_UNROLL;
 #ifndef FB_M2L_MIN_BLOCKS_F32
 #define FB_M2L_MIN_BLOCKS_F32 4
 #endif
@@ -614,6 +623,18 @@ m2l_unrolled_kernel(int nDst, const int *__restrict__ dstList, const int *__rest
     const int nb = min(32, o1 - b0);
     const int mySrc = live ? m2lSrc[k] : 0;
     __syncwarp();   // the previous batch's reads of sC are done
+#if FB_M2L_STAGE_FLAT
+    // stage the batch's moments: the 32 x NMP (source, coefficient) entries
+    // dealt over the lanes in order, so a load instruction reads consecutive
+    // coefficients of one or two sources and the batch's loads are independent
+#pragma unroll kM2LStageUnroll
+    for (int q = lane; q < 32 * NMP; q += 32) {
+      const int j = q / NMP, e = q - j * NMP;
+      const int sj = __shfl_sync(0xffffffffu, mySrc, j);
+      sC[m2l_slot(e, j)] = j < nb ? Vec2<TV>::make(momPot[(size_t)sj * NM + e], momDpdn[(size_t)sj * NM + e])
+                                  : Vec2<TV>::make(0.0, 0.0);
+    }
+#else
     // stage the batch's moments: one source at a time, lanes over coefficients
 #pragma unroll 1
     for (int j = 0; j < 32; j++) {
@@ -626,6 +647,7 @@ m2l_unrolled_kernel(int nDst, const int *__restrict__ dstList, const int *__rest
                                       : Vec2<TV>::make(0.0, 0.0);
       }
     }
+#endif
     M2LTensors<PM, TV, Sh::TSMEM> T;
     const V2 *tp = tens + (ADJ ? pairIdx[live ? k : o0] : (live ? k : o0));
     if constexpr (Sh::TSMEM) {
