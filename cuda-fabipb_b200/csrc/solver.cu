@@ -368,11 +368,13 @@ pc_gj_invert_kernel(const int *__restrict__ list, const int *__restrict__ bStart
 // x = blockdiag(inv) * b, block b gathers its pot/dpdn halves
 // Block-diagonal apply with the explicit inverses, one thread block per tile
 // of kPcRows rows of one diagonal block (tiles of large blocks spread over
-// many SMs).  Thread (row, quarter) sums a quarter of the columns; the
-// column-major inverse makes a warp's loads 32 consecutive doubles.  The
-// reference's per-block solve order (x = [pot; dpdn] of the cube's panels)
-// is src/precond_fmm.c:861-953.
-constexpr int kPcRows = 64, kPcSplit = 4;
+// many SMs).  The block's inputs are gathered into shared memory (in chunks
+// of kPcChunk columns); warp w sums the columns c = w mod kPcWarps, each lane
+// two consecutive rows (one 8- or 16-byte load of the column-major inverse
+// per column, eight loads in flight), and the warps' partial sums are added
+// in a fixed order.  The reference's per-block solve order (x = [pot; dpdn]
+// of the cube's panels) is src/precond_fmm.c:861-953.
+constexpr int kPcRows = 64, kPcWarps = 8, kPcChunk = 2048;
 
 // streams the block factorisations are spread over
 #ifndef FB_PC_STREAMS
@@ -380,59 +382,107 @@ constexpr int kPcRows = 64, kPcSplit = 4;
 #endif
 
 template <typename TI>
-__global__ void __launch_bounds__(kPcRows * kPcSplit)
+__global__ void __launch_bounds__(kPcWarps * 32)
 pc_apply_kernel(int n, const int2 *__restrict__ tiles, const int *__restrict__ bStart, const int *__restrict__ bSize,
                 const long long *__restrict__ bOff, const int *__restrict__ colSrc, const TI *__restrict__ inv,
                 const double *__restrict__ rhs, double *x) {
-  __shared__ double red[kPcSplit][kPcRows];
+  typedef typename Vec2<TI>::t V2;
+  __shared__ double xs[kPcChunk];
+  __shared__ double red[kPcWarps][kPcRows];
   const int2 tl = tiles[blockIdx.x];
   const int b = tl.x, r0 = tl.y;
   const int hm = bSize[b], st = bStart[b], M = 2 * hm;
-  const int rr = threadIdx.x % kPcRows, q = threadIdx.x / kPcRows;
-  const int r = r0 + rr;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r = r0 + 2 * lane;   // M is even: rows r and r + 1 are both in or both out
   const TI *Ib = inv + bOff[b];
   const int *cs = colSrc + 2 * (size_t)st;
-  const int c0 = (int)(((long long)M * q) / kPcSplit), c1 = (int)(((long long)M * (q + 1)) / kPcSplit);
-  double y = 0.0;
-  if (r < M) {
-#pragma unroll 4
-    for (int c = c0; c < c1; c++) {
-      const int g = cs[c];
-      const double xc = (g < hm) ? rhs[st + g] : rhs[n + st + g - hm];
-      y += (double)Ib[(size_t)c * M + r] * xc;
+  double y0 = 0.0, y1 = 0.0;
+  for (int k0 = 0; k0 < M; k0 += kPcChunk) {
+    const int kn = min(kPcChunk, M - k0);
+    __syncthreads();   // the previous chunk's reads are done
+    for (int c = threadIdx.x; c < kn; c += blockDim.x) {
+      const int g = cs[k0 + c];
+      xs[c] = (g < hm) ? rhs[st + g] : rhs[n + st + g - hm];
+    }
+    __syncthreads();
+    if (r < M) {
+      const TI *col = Ib + (size_t)k0 * M + r;
+#pragma unroll 8
+      for (int c = warp; c < kn; c += kPcWarps) {
+        const V2 a = *reinterpret_cast<const V2 *>(col + (size_t)c * M);
+        const double xc = xs[c];
+        y0 += (double)a.x * xc;
+        y1 += (double)a.y * xc;
+      }
     }
   }
-  red[q][rr] = y;
+  red[warp][2 * lane] = y0;
+  red[warp][2 * lane + 1] = y1;
   __syncthreads();
-  if (q == 0 && r < M) {
-    const double t = ((red[0][rr] + red[1][rr]) + red[2][rr]) + red[3][rr];
-    if (r < hm) x[st + r] = t;
-    else x[n + st + r - hm] = t;
+  if (threadIdx.x < kPcRows) {
+    const int rr = r0 + threadIdx.x;
+    if (rr < M) {
+      double t = red[0][threadIdx.x];
+#pragma unroll
+      for (int w = 1; w < kPcWarps; w++) t += red[w][threadIdx.x];
+      if (rr < hm) x[st + rr] = t;
+      else x[n + st + rr - hm] = t;
+    }
   }
 }
 
 // Transposed block-diagonal apply (adjoint solves): output c of a block is
-// column c of its inverse dotted with the block's input, one warp per output,
-// lanes over the (contiguous) column; tiles as for pc_apply_kernel.
+// column c of its inverse dotted with the block's input.  Tiles of kPcRows
+// outputs; the block's input is staged in shared memory in chunks, a warp per
+// output column, each lane two consecutive rows per step.
 template <typename TI>
-__global__ void __launch_bounds__(kPcRows * kPcSplit)
+__global__ void __launch_bounds__(kPcWarps * 32)
 pc_apply_t_kernel(int n, const int2 *__restrict__ tiles, const int *__restrict__ bStart, const int *__restrict__ bSize,
                   const long long *__restrict__ bOff, const int *__restrict__ colSrc, const TI *__restrict__ inv,
                   const double *__restrict__ rhs, double *x) {
+  typedef typename Vec2<TI>::t V2;
+  __shared__ double xs[kPcChunk];
   const int2 tl = tiles[blockIdx.x];
   const int b = tl.x, c0 = tl.y;
   const int hm = bSize[b], st = bStart[b], M = 2 * hm;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const TI *Ib = inv + bOff[b];
-  for (int c = c0 + warp; c < min(M, c0 + kPcRows); c += nw) {
-    const TI *col = Ib + (size_t)c * M;
-    double y = 0.0;
-    for (int r = lane; r < M; r += 32) y += (double)col[r] * ((r < hm) ? rhs[st + r] : rhs[n + st + r - hm]);
-    for (int o = 16; o > 0; o >>= 1) y += __shfl_xor_sync(0xffffffffu, y, o);
-    if (lane == 0) {
+  constexpr int kCols = kPcRows / kPcWarps;   // output columns per warp
+  double y[kCols];
+#pragma unroll
+  for (int q = 0; q < kCols; q++) y[q] = 0.0;
+  for (int k0 = 0; k0 < M; k0 += kPcChunk) {
+    const int kn = min(kPcChunk, M - k0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < kn; i += blockDim.x) {
+      const int rr = k0 + i;
+      xs[i] = (rr < hm) ? rhs[st + rr] : rhs[n + st + rr - hm];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kCols; q++) {
+      const int c = c0 + warp + q * kPcWarps;
+      if (c < M) {
+        const TI *col = Ib + (size_t)c * M + k0;
+        double acc = 0.0;
+#pragma unroll 4
+        for (int i = 2 * lane; i < kn; i += 64) {   // kn is even
+          const V2 a = *reinterpret_cast<const V2 *>(col + i);
+          acc += (double)a.x * xs[i] + (double)a.y * xs[i + 1];
+        }
+        y[q] += acc;
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < kCols; q++) {
+    double v = y[q];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int c = c0 + warp + q * kPcWarps;
+    if (lane == 0 && c < M) {
       const int g = colSrc[2 * (size_t)st + c];   // stored column c is output component g
-      if (g < hm) x[st + g] = y;
-      else x[n + st + g - hm] = y;
+      if (g < hm) x[st + g] = v;
+      else x[n + st + g - hm] = v;
     }
   }
 }
@@ -757,17 +807,17 @@ bool precond_apply(Context &c, const double *b, double *x, bool adjoint) {
   PrecondDev &p = *c.pc;
   if (p.mode == 2 && adjoint) {
     if (p.d_invF)
-      pc_apply_t_kernel<float><<<p.nTiles, kPcRows * kPcSplit, 0, c.stream>>>(c.n, p.d_tiles, p.d_start, p.d_size,
+      pc_apply_t_kernel<float><<<p.nTiles, kPcWarps * 32, 0, c.stream>>>(c.n, p.d_tiles, p.d_start, p.d_size,
                                                                              p.d_off, p.d_colSrc, p.d_invF, b, x);
     else
-      pc_apply_t_kernel<double><<<p.nTiles, kPcRows * kPcSplit, 0, c.stream>>>(c.n, p.d_tiles, p.d_start, p.d_size,
+      pc_apply_t_kernel<double><<<p.nTiles, kPcWarps * 32, 0, c.stream>>>(c.n, p.d_tiles, p.d_start, p.d_size,
                                                                               p.d_off, p.d_colSrc, p.d_inv, b, x);
   } else if (p.mode == 2) {
     if (p.d_invF)
-      pc_apply_kernel<float><<<p.nTiles, kPcRows * kPcSplit, 0, c.stream>>>(c.n, p.d_tiles, p.d_start, p.d_size,
+      pc_apply_kernel<float><<<p.nTiles, kPcWarps * 32, 0, c.stream>>>(c.n, p.d_tiles, p.d_start, p.d_size,
                                                                            p.d_off, p.d_colSrc, p.d_invF, b, x);
     else
-      pc_apply_kernel<double><<<p.nTiles, kPcRows * kPcSplit, 0, c.stream>>>(c.n, p.d_tiles, p.d_start, p.d_size,
+      pc_apply_kernel<double><<<p.nTiles, kPcWarps * 32, 0, c.stream>>>(c.n, p.d_tiles, p.d_start, p.d_size,
                                                                              p.d_off, p.d_colSrc, p.d_inv, b, x);
   } else if (p.mode == 3) {
     pc_diag_kernel<<<ceil_div(c.n, 256), 256, 0, c.stream>>>(c.n, c.d_area, (1.0 + c.epsilon) / 2.0,
