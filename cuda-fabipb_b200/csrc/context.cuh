@@ -65,6 +65,7 @@ struct Context {
   int *d_kidFirst = nullptr, *d_kidCount = nullptr;  // FMM indices of the children
   int *d_ordM2L = nullptr;                     // per FMM cube
   int nConvList = 0;                           // entries of d_lst
+  std::vector<int> h_lstOff, h_mOff;           // host copies of the list offsets
   long long nM2LPairs = 0;
   double2 *d_m2lTens = nullptr;                // [nMom][pairs] (D G0, D Gk) per M2L pair
   float2 *d_m2lTensF = nullptr;                // the same in FP32 (mixed contexts, orders <= 4)

@@ -259,40 +259,65 @@ __global__ void q2m_kernel(int nLeaves, int n, int NMleaf, int NM, const int *__
   }
 }
 
-// M2M: one block per parent cube at one level; threads over output indices
-__global__ void m2m_kernel(int first, int count, int NM, int ordOut, int ordIn, const int *__restrict__ kidFirst,
-                           const int *__restrict__ kidCount, const double *__restrict__ ctr,
-                           const int *__restrict__ lstOff, const int *__restrict__ lst, double *momPot,
-                           double *momDpdn) {
+// M2M: one block per parent cube at one level, one warp per child (children
+// w, w + 8, ... when a cube had more than eight), lanes over the output
+// coefficients; the warps' shifted moments are added in warp order.
+// L2L: one warp per child cube, eight cubes per block.
+constexpr int kShiftWarps = 8;
+
+__global__ void __launch_bounds__(kShiftWarps * 32)
+m2m_kernel(int first, int count, int NM, int ordOut, int ordIn, const int *__restrict__ kidFirst,
+           const int *__restrict__ kidCount, const double *__restrict__ ctr, const int *__restrict__ gOff,
+           const int *__restrict__ gLst, int nLst, double *momPot, double *momDpdn) {
+  // per warp: shift entries a, child moments b1, b2, and the child's shifted
+  // contribution o1, o2 (nOut each); then the term list (offsets, entries)
   extern __shared__ double sm[];
-  double *a = sm, *b1 = sm + NM, *b2 = sm + 2 * NM;
-  int f = first + blockIdx.x;
-  if (blockIdx.x >= count) return;
-  int nOut = nmom(ordOut), nIn = nmom(ordIn);
-  double o1 = 0.0, o2 = 0.0;
-  int al = threadIdx.x;
-  for (int k = 0; k < kidCount[f]; k++) {
-    int kid = kidFirst[f] + k;
-    double t[3] = {ctr[3 * kid] - ctr[3 * f], ctr[3 * kid + 1] - ctr[3 * f + 1], ctr[3 * kid + 2] - ctr[3 * f + 2]};
-    for (int e = threadIdx.x; e < nOut; e += blockDim.x) {
+  if ((int)blockIdx.x >= count) return;
+  const int f = first + blockIdx.x;
+  const int nOut = nmom(ordOut), nIn = nmom(ordIn);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int *lstOff = reinterpret_cast<int *>(sm + (size_t)kShiftWarps * 5 * nOut), *lst = lstOff + nOut + 1;
+  for (int e = threadIdx.x; e <= nOut; e += blockDim.x) lstOff[e] = gOff[e];
+  for (int e = threadIdx.x; e < nLst; e += blockDim.x) lst[e] = gLst[e];
+  __syncthreads();
+  const int nk = kidCount[f];
+  double *a = sm + (size_t)warp * 5 * nOut, *b1 = a + nOut, *b2 = b1 + nOut, *o1 = b2 + nOut, *o2 = o1 + nOut;
+  for (int e = lane; e < nOut; e += 32) o1[e] = o2[e] = 0.0;
+  for (int k = warp; k < nk; k += kShiftWarps) {
+    const int kid = kidFirst[f] + k;
+    const double t[3] = {ctr[3 * kid] - ctr[3 * f], ctr[3 * kid + 1] - ctr[3 * f + 1],
+                         ctr[3 * kid + 2] - ctr[3 * f + 2]};
+    __syncwarp();   // the previous child's reads of a, b1, b2 are done
+    for (int e = lane; e < nOut; e += 32) {
       a[e] = conv_entry(t, e);
       b1[e] = (e < nIn) ? momPot[(size_t)kid * NM + e] : 0.0;
       b2[e] = (e < nIn) ? momDpdn[(size_t)kid * NM + e] : 0.0;
     }
-    __syncthreads();
-    if (al < nOut) {
+    __syncwarp();
+    for (int al = lane; al < nOut; al += 32) {
+      double s1 = 0.0, s2 = 0.0;
       for (int q = lstOff[al]; q < lstOff[al + 1]; q++) {
-        int ent = lst[q];
-        int ia = ent & 1023, ib = (ent >> 10) & 1023;
-        o1 += a[ia] * b1[ib];
-        o2 += a[ia] * b2[ib];
+        const int ent = lst[q];
+        const int ia = ent & 1023, ib = (ent >> 10) & 1023;
+        s1 += a[ia] * b1[ib];
+        s2 += a[ia] * b2[ib];
       }
+      o1[al] += s1;
+      o2[al] += s2;
     }
-    __syncthreads();
   }
-  if (al < nOut) {
-    momPot[(size_t)f * NM + al] = o1;
-    momDpdn[(size_t)f * NM + al] = o2;
+  __syncthreads();
+  // the warps' contributions in warp order
+  const int nw = min(nk, kShiftWarps);
+  for (int al = threadIdx.x; al < nOut; al += blockDim.x) {
+    double s1 = 0.0, s2 = 0.0;
+    for (int k = 0; k < nw; k++) {
+      const double *ok = sm + (size_t)k * 5 * nOut + 3 * nOut;
+      s1 += ok[al];
+      s2 += ok[nOut + al];
+    }
+    momPot[(size_t)f * NM + al] = s1;
+    momDpdn[(size_t)f * NM + al] = s2;
   }
 }
 
@@ -691,26 +716,34 @@ __global__ void tensors_to_float_kernel(long long n, const double2 *__restrict__
 }
 
 // L2L: one block per child cube of one level (parents one level up)
-__global__ void l2l_kernel(int first, int count, int NM, int ordIn, int ordOut, const int *__restrict__ parent,
-                           const double *__restrict__ ctr, const int *__restrict__ lstOff,
-                           const int *__restrict__ lst, double *lec1, double *lec2, double *lec3, double *lec4) {
+__global__ void __launch_bounds__(kShiftWarps * 32)
+l2l_kernel(int first, int count, int NM, int ordIn, int ordOut, const int *__restrict__ parent,
+           const double *__restrict__ ctr, const int *__restrict__ gOff, const int *__restrict__ gLst, int nLst,
+           double *lec1, double *lec2, double *lec3, double *lec4) {
+  // per warp: shift entries a and the parent's locals i1..i4 (nIn each); then
+  // the term list (offsets, entries)
   extern __shared__ double sm[];
   const int nIn = nmom(ordIn), nOut = nmom(ordOut);
-  double *a = sm, *i1 = sm + nIn, *i2 = i1 + nIn, *i3 = i2 + nIn, *i4 = i3 + nIn;
-  if ((int)blockIdx.x >= count) return;
-  const int f = first + blockIdx.x;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int *lstOff = reinterpret_cast<int *>(sm + (size_t)kShiftWarps * 5 * nIn), *lst = lstOff + nOut + 1;
+  for (int e = threadIdx.x; e <= nOut; e += blockDim.x) lstOff[e] = gOff[e];
+  for (int e = threadIdx.x; e < nLst; e += blockDim.x) lst[e] = gLst[e];
+  __syncthreads();
+  const int cube = blockIdx.x * kShiftWarps + warp;
+  if (cube >= count) return;   // warp-uniform; no block barrier follows
+  double *a = sm + (size_t)warp * 5 * nIn, *i1 = a + nIn, *i2 = i1 + nIn, *i3 = i2 + nIn, *i4 = i3 + nIn;
+  const int f = first + cube;
   const int p = parent[f];
   const double t[3] = {ctr[3 * f] - ctr[3 * p], ctr[3 * f + 1] - ctr[3 * p + 1], ctr[3 * f + 2] - ctr[3 * p + 2]};
-  for (int e = threadIdx.x; e < nIn; e += blockDim.x) {
+  for (int e = lane; e < nIn; e += 32) {
     a[e] = conv_entry(t, e);
     i1[e] = lec1[(size_t)p * NM + e];
     i2[e] = lec2[(size_t)p * NM + e];
     i3[e] = lec3[(size_t)p * NM + e];
     i4[e] = lec4[(size_t)p * NM + e];
   }
-  __syncthreads();
-  const int al = threadIdx.x;
-  if (al < nOut) {
+  __syncwarp();
+  for (int al = lane; al < nOut; al += 32) {
     const int degA = c_mi[al].w;
     double t1 = 0.0, t2 = 0.0, t3 = 0.0, t4 = 0.0;
     for (int q = lstOff[al]; q < lstOff[al + 1]; q++) {
@@ -891,6 +924,8 @@ bool setup_fmm(Context &c) {
   lstOff[c.NM] = (int)lst.size();
   mOff[c.NM] = (int)mLst.size();
   c.nConvList = (int)lst.size();
+  c.h_lstOff = lstOff;
+  c.h_mOff = mOff;
   if (!c.arena.upload(&c.d_lstOff, lstOff, s) || !c.arena.upload(&c.d_lst, lst, s) ||
       !c.arena.upload(&c.d_mOff, mOff, s) || !c.arena.upload(&c.d_mLst, mLst, s))
     return false;
@@ -997,11 +1032,12 @@ bool launch_far_upward(Context &c, const double *sgm, bool adjoint, cudaEvent_t 
   if (marks) cudaEventRecord(marks[0], s);
   for (int lev = depth - 1; lev >= height; lev--) {
     int ordOut = pt.ordMom[lev], ordIn = pt.ordMom[lev + 1];
-    int thr = std::max(32, ((nmom(ordOut) + 31) / 32) * 32);
-    size_t shm = 3 * (size_t)nmom(ordOut) * sizeof(double);
-    m2m_kernel<<<pt.fmmLevelCount[lev], thr, shm, s>>>(pt.fmmLevelStart[lev], pt.fmmLevelCount[lev], c.NM, ordOut,
-                                                       ordIn, c.d_kidFirst, c.d_kidCount, c.d_cubeCtr, c.d_mOff,
-                                                       c.d_mLst, up1, up2);
+    const int nOut = nmom(ordOut), nLst = c.h_mOff[nOut];
+    const size_t shm = (size_t)kShiftWarps * 5 * nOut * sizeof(double) + (size_t)(nOut + 1 + nLst) * sizeof(int);
+    if (shm > 48 * 1024) cudaFuncSetAttribute(m2m_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    m2m_kernel<<<pt.fmmLevelCount[lev], kShiftWarps * 32, shm, s>>>(
+        pt.fmmLevelStart[lev], pt.fmmLevelCount[lev], c.NM, ordOut, ordIn, c.d_kidFirst, c.d_kidCount, c.d_cubeCtr,
+        c.d_mOff, c.d_mLst, nLst, up1, up2);
   }
   if (marks) cudaEventRecord(marks[1], s);
   if (!launch_m2l_only(c, adjoint, fp64)) return false;
@@ -1011,11 +1047,12 @@ bool launch_far_upward(Context &c, const double *sgm, bool adjoint, cudaEvent_t 
   double *d1 = adjoint ? c.d_mom : c.d_lec, *d2 = adjoint ? c.d_mom + plane : c.d_lec + plane;
   for (int lev = height; lev < depth; lev++) {
     int ordIn = pt.ordMom[lev], ordOut = pt.ordMom[lev + 1];
-    int thr = std::max(32, ((nmom(ordOut) + 31) / 32) * 32);
-    size_t shm = 5 * (size_t)nmom(ordIn) * sizeof(double);
-    l2l_kernel<<<pt.fmmLevelCount[lev + 1], thr, shm, s>>>(
+    const int nOut = nmom(ordOut), nLst = c.h_lstOff[nOut];
+    const size_t shm = (size_t)kShiftWarps * 5 * nmom(ordIn) * sizeof(double) + (size_t)(nOut + 1 + nLst) * sizeof(int);
+    if (shm > 48 * 1024) cudaFuncSetAttribute(l2l_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    l2l_kernel<<<ceil_div(pt.fmmLevelCount[lev + 1], kShiftWarps), kShiftWarps * 32, shm, s>>>(
         pt.fmmLevelStart[lev + 1], pt.fmmLevelCount[lev + 1], c.NM, ordIn, ordOut, c.d_fmmParent, c.d_cubeCtr,
-        c.d_lstOff, c.d_lst, d1, d2, c.d_lec + 2 * plane, c.d_lec + 3 * plane);
+        c.d_lstOff, c.d_lst, nLst, d1, d2, c.d_lec + 2 * plane, c.d_lec + 3 * plane);
   }
   if (adjoint) FB_CUDA(cudaMemsetAsync(c.d_lec + 2 * plane, 0, 2 * plane * sizeof(double), s));
   if (marks) cudaEventRecord(marks[3], s);

@@ -762,8 +762,12 @@ bool precond_setup(Context &c, int mode) {
     p.maxM = std::max(p.maxM, 2 * hm);
   }
   p.nBlocks = (int)p.hSize.size();
+  // apply tiles, the largest blocks' first (a tile's cost grows with its block's size)
+  std::vector<int> order(p.nBlocks);
+  for (int b = 0; b < p.nBlocks; b++) order[b] = b;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return p.hSize[a] > p.hSize[b]; });
   std::vector<int2> tiles;
-  for (int b = 0; b < p.nBlocks; b++)
+  for (int b : order)
     for (int r0 = 0; r0 < 2 * p.hSize[b]; r0 += kPcRows) tiles.push_back(make_int2(b, r0));
   p.nTiles = (int)tiles.size();
   FB_CHECK(p.maxM <= 46340, "preconditioner block %d too large (increase -t)", p.maxM);
