@@ -232,13 +232,14 @@ def pass_report(surf, info, x_ptr, flush, reps, prec_is_mixed, sm_mhz, n_sm):
     fp32 = n_sm * 128 * 2 * sm_mhz * 1e6 / 1e12
     fp64 = n_sm * 64 * 2 * sm_mhz * 1e6 / 1e12
     near_peak = fp32 if prec_is_mixed else fp64
+    qb = 4.0 if prec_is_mixed else 8.0   # bytes per leaf-matrix entry (FP32 copies in a mixed context)
     work = {
         "near": ("flop", FLOP_PER_PAIR * info["near_panel_pairs"], near_peak),
-        "q2m": ("bytes", 8.0 * (2 * nmom(pl) * n + 2 * n + 2 * nmom(p) * leaves), hbm),
+        "q2m": ("bytes", qb * 2 * nmom(pl) * n + 8.0 * (2 * n + 2 * nmom(p) * leaves), hbm),
         "m2m": ("bytes", 8.0 * 2 * nmom(p) * 2 * cubes, hbm),
         "m2l": ("flop", 8.0 * comb(p + 6, 6) * info["m2l_pairs"], fp32 if prec_is_mixed and p <= 5 else fp64),
         "l2l": ("bytes", 8.0 * 4 * nmom(p) * 2 * cubes, hbm),
-        "l2p": ("bytes", 8.0 * (2 * nmom(pl) * n + 4 * nmom(p) * leaves + 6 * n), hbm),
+        "l2p": ("bytes", qb * 2 * nmom(pl) * n + 8.0 * (4 * nmom(p) * leaves + 6 * n), hbm),
     }
     out = {}
     for k, (kind, amount, peak) in work.items():

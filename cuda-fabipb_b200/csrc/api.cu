@@ -168,7 +168,7 @@ bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y
   FB_CUDA(cudaEventRecord(c.evJoin, c.sideStream));
   if (!launch_far_upward(c, x, adjoint, nullptr, fp64)) return false;
   FB_CUDA(cudaStreamWaitEvent(c.stream, c.evJoin, 0));
-  if (!launch_l2p(c, -alpha, beta, y, x, s1, s2, adjoint, c.d_nearOut)) return false;
+  if (!launch_l2p(c, -alpha, beta, y, x, s1, s2, adjoint, c.d_nearOut, fp64)) return false;
   return true;
 }
 

@@ -52,6 +52,7 @@ struct Context {
   int P = 0, NM = 0;                       // max order, nmom(max order)
   int leafOrder = 0, NMleaf = 0;
   double *d_Q0 = nullptr, *d_Q1 = nullptr; // [NMleaf][n]: moments, noments
+  float *d_Q0F = nullptr, *d_Q1F = nullptr; // their FP32 copies (mixed contexts)
   double *d_cubeCtr = nullptr;             // 3 per FMM cube
   int *d_m2lOff = nullptr, *d_m2lSrc = nullptr;
   int *d_fmmParent = nullptr;              // parent FMM index (or -1)
@@ -68,7 +69,7 @@ struct Context {
   std::vector<int> h_lstOff, h_mOff;           // host copies of the list offsets
   long long nM2LPairs = 0;
   double2 *d_m2lTens = nullptr;                // [nMom][pairs] (D G0, D Gk) per M2L pair
-  float2 *d_m2lTensF = nullptr;                // the same in FP32 (mixed contexts, orders <= 4)
+  float2 *d_m2lTensF = nullptr;                // the same in FP32 (mixed contexts, orders <= 5)
   // transposed M2L lists (adjoint operator, built on first use)
   bool m2lAdjReady = false;
   std::vector<int> h_m2lDstT;
@@ -121,8 +122,9 @@ bool launch_far_upward(Context &c, const double *sgm, bool adjoint = false, cuda
                        bool fp64 = false);
 // L2P: out = beta*out + alpha*far + diag*(area .* x) (diag part optional)
 // (addend: a vector added to out, the near field computed beside the far passes)
+// (fp64: the FP64 leaf matrices also in a mixed context, for refinement residuals)
 bool launch_l2p(Context &c, double alpha, double beta, double *out, const double *diagX,
-                double s1, double s2, bool adjoint = false, const double *addend = nullptr);
+                double s1, double s2, bool adjoint = false, const double *addend = nullptr, bool fp64 = false);
 bool launch_m2l_only(Context &c, bool adjoint = false, bool fp64 = false);
 bool launch_rhs(Context &c, int useTree, double *rhs);
 bool launch_energy(Context &c, const double *sgm, double *raw_host);

@@ -234,9 +234,12 @@ __global__ void leaf_moments_kernel(int n, int order, const double *__restrict__
 // Q2M: one block per leaf, warp w sums rows m = w, w+8, ... over the leaf panels
 // swap = 1 reads the two halves of sgm exchanged (the adjoint of L2P:
 // momPot <- Q1 . second half, momDpdn <- Q0 . first half).
+// TQ: the leaf matrices' storage type (FP32 copies in a mixed context; the
+// sums are FP64 either way)
+template <typename TQ>
 __global__ void q2m_kernel(int nLeaves, int n, int NMleaf, int NM, const int *__restrict__ leafStart,
                            const int *__restrict__ leafCount, const int *__restrict__ leafFmm,
-                           const double *__restrict__ Q0, const double *__restrict__ Q1,
+                           const TQ *__restrict__ Q0, const TQ *__restrict__ Q1,
                            const double *__restrict__ sgm, int swap, double *momPot, double *momDpdn) {
   int L = blockIdx.x;
   if (L >= nLeaves) return;
@@ -244,6 +247,7 @@ __global__ void q2m_kernel(int nLeaves, int n, int NMleaf, int NM, const int *__
   int st = leafStart[L], cnt = leafCount[L], f = leafFmm[L];
   for (int m = warp; m < NMleaf; m += nw) {
     double sp = 0.0, sd = 0.0;
+#pragma unroll 4
     for (int j = lane; j < cnt; j += 32) {
       sp += Q1[(size_t)m * n + st + j] * sgm[(swap ? n : 0) + st + j];
       sd += Q0[(size_t)m * n + st + j] * sgm[(swap ? 0 : n) + st + j];
@@ -715,7 +719,12 @@ __global__ void tensors_to_float_kernel(long long n, const double2 *__restrict__
     b[i] = make_float2((float)a[i].x, (float)a[i].y);
 }
 
-// L2L: one block per child cube of one level (parents one level up)
+__global__ void to_float_kernel(long long n, const double *__restrict__ a, float *b) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+// L2L: one warp per child cube of one level (parents one level up)
 __global__ void __launch_bounds__(kShiftWarps * 32)
 l2l_kernel(int first, int count, int NM, int ordIn, int ordOut, const int *__restrict__ parent,
            const double *__restrict__ ctr, const int *__restrict__ gOff, const int *__restrict__ gLst, int nLst,
@@ -764,9 +773,10 @@ l2l_kernel(int first, int count, int NM, int ordIn, int ordOut, const int *__res
 
 // L2P: out[i] = beta*out[i] + alpha*Q0^T(lec1+lec2) + s1*A*x[i]  (and the
 // dpdn half with Q1, lec3+lec4, s2).  diagX may be null.
+template <typename TQ>
 __global__ void l2p_kernel(int n, int NMleaf, int NM, const int *__restrict__ leafOfPanel,
-                           const int *__restrict__ leafFmm, const double *__restrict__ Q0,
-                           const double *__restrict__ Q1, const double *__restrict__ lec1,
+                           const int *__restrict__ leafFmm, const TQ *__restrict__ Q0,
+                           const TQ *__restrict__ Q1, const double *__restrict__ lec1,
                            const double *__restrict__ lec2, const double *__restrict__ lec3,
                            const double *__restrict__ lec4, double alpha, double beta, const double *__restrict__ area,
                            const double *__restrict__ diagX, double s1, double s2, int swap,
@@ -776,8 +786,8 @@ __global__ void l2p_kernel(int n, int NMleaf, int NM, const int *__restrict__ le
   const size_t f = (size_t)leafFmm[leafOfPanel[i]] * NM;
   double a = 0.0, b = 0.0;
   for (int m = 0; m < NMleaf; m++) {
-    a += Q0[(size_t)m * n + i] * (lec1[f + m] + lec2[f + m]);
-    b += Q1[(size_t)m * n + i] * (lec3[f + m] + lec4[f + m]);
+    a += (double)Q0[(size_t)m * n + i] * (lec1[f + m] + lec2[f + m]);
+    b += (double)Q1[(size_t)m * n + i] * (lec3[f + m] + lec4[f + m]);
   }
   if (swap) {   // the adjoint of Q2M: the Q0 value belongs to the dpdn half
     const double t = a;
@@ -981,6 +991,13 @@ bool setup_fmm(Context &c) {
   tm.mark("m2l_tensors");
   FB_DISPATCH_ORDER(c.leafOrder, launch_leaf_moments, c, c.leafOrder);
   FB_CUDA(cudaGetLastError());
+  if (c.mixed) {   // the FP32 copies Q2M and L2P read in a mixed context
+    const long long nq = (long long)c.NMleaf * c.n;
+    if (!c.arena.alloc_n(&c.d_Q0F, (size_t)nq) || !c.arena.alloc_n(&c.d_Q1F, (size_t)nq)) return false;
+    to_float_kernel<<<1184, 256, 0, s>>>(nq, c.d_Q0, c.d_Q0F);
+    to_float_kernel<<<1184, 256, 0, s>>>(nq, c.d_Q1, c.d_Q1F);
+    FB_CUDA(cudaGetLastError());
+  }
   tm.mark("leaf_moments");
   return true;
 }
@@ -1027,8 +1044,12 @@ bool launch_far_upward(Context &c, const double *sgm, bool adjoint, cudaEvent_t 
   c.launches += 1 + 2 * (depth - height);
   // upward arrays: moments (forward) or adjoint locals (adjoint)
   double *up1 = adjoint ? c.d_lec + plane : c.d_mom, *up2 = adjoint ? c.d_lec : c.d_mom + plane;
-  q2m_kernel<<<pt.nLeaves, 256, 0, s>>>(pt.nLeaves, c.n, c.NMleaf, c.NM, c.d_leafStart, c.d_leafCount, c.d_leafFmm,
-                                        c.d_Q0, c.d_Q1, sgm, adjoint ? 1 : 0, up1, up2);
+  if (c.d_Q0F && !fp64)
+    q2m_kernel<float><<<pt.nLeaves, 256, 0, s>>>(pt.nLeaves, c.n, c.NMleaf, c.NM, c.d_leafStart, c.d_leafCount,
+                                                 c.d_leafFmm, c.d_Q0F, c.d_Q1F, sgm, adjoint ? 1 : 0, up1, up2);
+  else
+    q2m_kernel<double><<<pt.nLeaves, 256, 0, s>>>(pt.nLeaves, c.n, c.NMleaf, c.NM, c.d_leafStart, c.d_leafCount,
+                                                  c.d_leafFmm, c.d_Q0, c.d_Q1, sgm, adjoint ? 1 : 0, up1, up2);
   if (marks) cudaEventRecord(marks[0], s);
   for (int lev = depth - 1; lev >= height; lev--) {
     int ordOut = pt.ordMom[lev], ordIn = pt.ordMom[lev + 1];
@@ -1069,15 +1090,21 @@ bool launch_m2l_only(Context &c, bool adjoint, bool fp64) {
 }
 
 bool launch_l2p(Context &c, double alpha, double beta, double *out, const double *diagX, double s1, double s2,
-                bool adjoint, const double *addend) {
+                bool adjoint, const double *addend, bool fp64) {
   const size_t plane = (size_t)c.pt.nFmm * c.NM;
   c.launches += 1;
   // adjoint: Q0 . (adjoint dpdn moments + 0) -> dpdn half, Q1 . (adjoint pot moments + 0) -> pot half
   const double *l1 = adjoint ? c.d_mom + plane : c.d_lec, *l2 = c.d_lec + (adjoint ? 2 : 1) * plane;
   const double *l3 = adjoint ? c.d_mom : c.d_lec + 2 * plane, *l4 = c.d_lec + 3 * plane;
-  l2p_kernel<<<ceil_div(c.n, 256), 256, 0, c.stream>>>(c.n, c.NMleaf, c.NM, c.d_leafOfPanel, c.d_leafFmm, c.d_Q0,
-                                                       c.d_Q1, l1, l2, l3, l4, alpha, beta, c.d_area, diagX, s1, s2,
-                                                       adjoint ? 1 : 0, addend, out);
+  if (c.d_Q0F && !fp64)
+    l2p_kernel<float><<<ceil_div(c.n, 256), 256, 0, c.stream>>>(c.n, c.NMleaf, c.NM, c.d_leafOfPanel, c.d_leafFmm,
+                                                                c.d_Q0F, c.d_Q1F, l1, l2, l3, l4, alpha, beta,
+                                                                c.d_area, diagX, s1, s2, adjoint ? 1 : 0, addend, out);
+  else
+    l2p_kernel<double><<<ceil_div(c.n, 256), 256, 0, c.stream>>>(c.n, c.NMleaf, c.NM, c.d_leafOfPanel, c.d_leafFmm,
+                                                                 c.d_Q0, c.d_Q1, l1, l2, l3, l4, alpha, beta,
+                                                                 c.d_area, diagX, s1, s2, adjoint ? 1 : 0, addend,
+                                                                 out);
   FB_CUDA(cudaGetLastError());
   return true;
 }
