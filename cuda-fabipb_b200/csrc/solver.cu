@@ -370,11 +370,15 @@ pc_gj_invert_kernel(const int *__restrict__ list, const int *__restrict__ bStart
 // of kPcRows rows of one diagonal block (tiles of large blocks spread over
 // many SMs).  The block's inputs are gathered into shared memory (in chunks
 // of kPcChunk columns); warp w sums the columns c = w mod kPcWarps, each lane
-// two consecutive rows (one 8- or 16-byte load of the column-major inverse
-// per column, eight loads in flight), and the warps' partial sums are added
-// in a fixed order.  The reference's per-block solve order (x = [pot; dpdn]
+// kPcRpl consecutive rows (8- or 16-byte loads of the column-major inverse,
+// eight columns in flight), and the warps' partial sums are added in a fixed
+// order.  The reference's per-block solve order (x = [pot; dpdn]
 // of the cube's panels) is src/precond_fmm.c:861-953.
-constexpr int kPcRows = 64, kPcWarps = 8, kPcChunk = 2048;
+#ifndef FB_PC_RPL
+#define FB_PC_RPL 4
+#endif
+constexpr int kPcRpl = FB_PC_RPL;   // rows per lane (2 or 4)
+constexpr int kPcRows = 32 * kPcRpl, kPcWarps = 8, kPcChunk = 2048;
 
 // streams the block factorisations are spread over
 #ifndef FB_PC_STREAMS
@@ -393,10 +397,11 @@ pc_apply_kernel(int n, const int2 *__restrict__ tiles, const int *__restrict__ b
   const int b = tl.x, r0 = tl.y;
   const int hm = bSize[b], st = bStart[b], M = 2 * hm;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int r = r0 + 2 * lane;   // M is even: rows r and r + 1 are both in or both out
+  const int r = r0 + kPcRpl * lane;   // M is even: rows r and r + 1 are both in or both out
   const TI *Ib = inv + bOff[b];
   const int *cs = colSrc + 2 * (size_t)st;
-  double y0 = 0.0, y1 = 0.0;
+  double y0 = 0.0, y1 = 0.0, y2 = 0.0, y3 = 0.0;
+  const bool q2 = kPcRpl == 4 && r + 2 < M;
   for (int k0 = 0; k0 < M; k0 += kPcChunk) {
     const int kn = min(kPcChunk, M - k0);
     __syncthreads();   // the previous chunk's reads are done
@@ -413,18 +418,27 @@ pc_apply_kernel(int n, const int2 *__restrict__ tiles, const int *__restrict__ b
         const double xc = xs[c];
         y0 += (double)a.x * xc;
         y1 += (double)a.y * xc;
+        if (kPcRpl == 4 && q2) {
+          const V2 a2 = *reinterpret_cast<const V2 *>(col + (size_t)c * M + 2);
+          y2 += (double)a2.x * xc;
+          y3 += (double)a2.y * xc;
+        }
       }
     }
   }
-  red[warp][2 * lane] = y0;
-  red[warp][2 * lane + 1] = y1;
+  red[warp][kPcRpl * lane] = y0;
+  red[warp][kPcRpl * lane + 1] = y1;
+  if (kPcRpl == 4) {
+    red[warp][kPcRpl * lane + 2] = y2;
+    red[warp][kPcRpl * lane + 3] = y3;
+  }
   __syncthreads();
-  if (threadIdx.x < kPcRows) {
-    const int rr = r0 + threadIdx.x;
+  for (int i = threadIdx.x; i < kPcRows; i += blockDim.x) {
+    const int rr = r0 + i;
     if (rr < M) {
-      double t = red[0][threadIdx.x];
+      double t = red[0][i];
 #pragma unroll
-      for (int w = 1; w < kPcWarps; w++) t += red[w][threadIdx.x];
+      for (int w = 1; w < kPcWarps; w++) t += red[w][i];
       if (rr < hm) x[st + rr] = t;
       else x[n + st + rr - hm] = t;
     }
