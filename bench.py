@@ -22,7 +22,10 @@ Reported:
              against the FP32 SIMT peak of the measured SM clock;
   cpu_baseline  the reference CPU solver compiled from its own sources
              (oracle/_ref), timed on a bounded sample of matvecs on this
-             host's cores.
+             host's cores;
+  ref_gpu_baseline  (--ref-gpu) the reference's own CUDA backend compiled
+             from its sources for sm_100a (oracle/_ref/ref_harness_gpu), the
+             same matvec with -g=1 on this GPU.
 With --impl reference the line times that reference CPU matvec itself.
 N>1 GPUs run independent replicas (the path does not shard: replicas only);
 value is the sum over replicas, timed as the max over ranks.
@@ -110,6 +113,25 @@ def cpu_reference_rate(base, opts, reps, warmup=1, budget=60.0):
         orc.matvec(x)
     dt = time.perf_counter() - t0
     return reps / dt, "port", cores, "%d timed matvecs of the full mesh (FP64 restatement)" % reps
+
+
+def ref_gpu_rate(base, opts, reps=10):
+    """matvec/s of the reference's own CUDA backend (src/gpu_backend_cuda.cu,
+    compiled from its sources into oracle/_ref by `make -C oracle refgpu`):
+    MtVmain with -g=1 on this GPU, host wall time of `reps` calls after two
+    warm-up calls.  None when that build is absent or the run fails."""
+    from oracle import oracle as O
+    if not os.path.exists(O.REF_HARNESS_GPU):
+        return None
+    try:
+        pre = os.path.join(tempfile.gettempdir(), "fabipb_refgpu_time")
+        out = O.run_ref_harness("time", base, pre, ref_opts(opts), threads=os.cpu_count() or 1, reps=reps,
+                                warmup=2, gpu=True, timeout=900)
+        r = json.loads(out.strip().splitlines()[-1])
+    except Exception as e:   # a baseline, not the product: report the failure, keep the line
+        return {"value": None, "error": str(e)[:200]}
+    return {"value": r["matvec_per_s"], "unit": "matvec/s", "kind": "reference CUDA backend (-g=1, FP64)",
+            "sample": "%d timed MtVmain calls after 2 warm-up, host wall time" % r["reps"]}
 
 
 class ClockSampler:
@@ -447,6 +469,7 @@ def run_ours(args):
     passes = pass_report(surf, info, x.data_ptr(), flush, args.steps, prec == lib.MIXED, sm_mhz, n_sm)
     solve = None if args.no_solve else solve_report(pan, ch, opts, local, stream)
     cpu = None
+    ref_gpu = ref_gpu_rate(base, opts) if args.ref_gpu else None
     if not args.no_cpu_baseline:
         v, kind, cores, sample = cpu_reference_rate(base, opts, args.cpu_reps, 1, budget=30.0)
         cpu = {"value": v, "unit": "matvec/s", "cores": cores, "kind": kind, "sample": sample}
@@ -469,6 +492,7 @@ def run_ours(args):
                      "peak_source": peak_src, "flop_per_pair": FLOP_PER_PAIR,
                      "pairs_per_launch": pairs, "launch_ms": near_s * 1000.0},
         "cpu_baseline": cpu,
+        "ref_gpu_baseline": ref_gpu,
         "gpu_launches": launches,
         "clocks": clocks,
         "setup_s": info["setup_seconds"],
@@ -492,6 +516,8 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=90.0,
                     help="seconds of timed reference matvecs at most (--impl reference)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-gpu", action="store_true",
+                    help="also time the reference's own CUDA backend (oracle/_ref/ref_harness_gpu, -g=1)")
     ap.add_argument("--no-solve", action="store_true", help="skip the mixed/FP64 solve report")
     args = ap.parse_args()
     if args.impl == "reference":

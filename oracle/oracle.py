@@ -20,6 +20,9 @@ LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 REF_HARNESS = os.path.join(REF_DIR, "ref_harness")
 REF_BINARY = os.path.join(REF_DIR, "fabipb_ref")
+# the reference's own CUDA backend built from its sources (make -C oracle refgpu)
+REF_HARNESS_GPU = os.path.join(REF_DIR, "ref_harness_gpu")
+REF_BINARY_GPU = os.path.join(REF_DIR, "fabipb_refgpu")
 
 
 class Params(C.Structure):
@@ -235,9 +238,12 @@ def ref_env(threads=None):
 
 
 def run_ref_harness(mode, base, out_prefix, opts, sigma=None, threads=None, reps=None, warmup=None,
-                    extra_env=None, budget=None):
-    """Run oracle/_ref/ref_harness; return stdout.  Mesh files must sit at ``base``."""
-    cmd = [REF_HARNESS, mode, base, out_prefix] + list(opts)
+                    extra_env=None, budget=None, gpu=False, timeout=None):
+    """Run oracle/_ref/ref_harness (gpu: ref_harness_gpu with -g=1, the
+    reference's CUDA backend); return stdout.  Mesh files must sit at ``base``."""
+    cmd = [REF_HARNESS_GPU if gpu else REF_HARNESS, mode, base, out_prefix] + list(opts)
+    if gpu:
+        cmd.append("-g=1")
     if sigma is not None:
         path = out_prefix + ".sigma.in"
         np.ascontiguousarray(sigma, dtype=np.float64).tofile(path)
@@ -251,7 +257,7 @@ def run_ref_harness(mode, base, out_prefix, opts, sigma=None, threads=None, reps
     env = ref_env(threads)
     if extra_env:
         env.update(extra_env)
-    r = subprocess.run(cmd, env=env, capture_output=True, text=True, check=True)
+    r = subprocess.run(cmd, env=env, capture_output=True, text=True, check=True, timeout=timeout)
     return r.stdout
 
 

@@ -18,6 +18,9 @@
  *
  * usage: ref_harness <mode> <mesh-base> <out-prefix> [reference options]
  *        [--sigma=<file of 2N doubles>] [--reps=K] [--warmup=W]
+ *
+ * Linked with the reference's CUDA backend instead of its stub (ref_harness_gpu,
+ * `make refgpu`), option -g=1 runs the same entry points through that backend.
  */
 
 #include <stdio.h>
@@ -113,6 +116,7 @@ int main(int argc, char **argv) {
     else if ((v = optv(a, "eps1"))) epsilon1 = atof(v);
     else if ((v = optv(a, "eps2"))) epsilon2 = atof(v);
     else if ((v = optv(a, "P"))) { sys->precondCacheMode = atoi(v); precondExplicit = 1; }
+    else if ((v = optv(a, "g"))) { sys->gpuMode = atoi(v); sys->gpuQ2MMode = sys->gpuMode > 0; }
     else if (strncmp(a, "--sigma=", 8) == 0) sigmaPath = a + 8;
     else if (strncmp(a, "--reps=", 7) == 0) reps = atoi(a + 7);
     else if (strncmp(a, "--warmup=", 9) == 0) warmup = atoi(a + 9);
