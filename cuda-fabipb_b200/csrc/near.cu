@@ -312,17 +312,21 @@ __device__ __forceinline__ void near_pair2(const float4 A, const float4 B, const
 }
 
 // one staged tile of up to 32 sources (np packed source pairs) for a target
+#ifndef FB_NEAR_UNROLL
+#define FB_NEAR_UNROLL 4
+#endif
+constexpr int kNearUnroll = FB_NEAR_UNROLL;
 template <bool ADJ, bool SELF>
 __device__ __forceinline__ void near_tile2(const float4 (*sP)[4], int np, int k, int sub, float2 tx, float2 ty,
                                            float2 tz, float2 tnx, float2 tny, float2 tnz, float kappa, float kexp,
                                            float eps, float ieps, float kap2, float2 &acc0, float2 &acc1) {
   if (k == 1) {   // warp-uniform: a full group
-#pragma unroll 2
+#pragma unroll kNearUnroll
     for (int q = 0; q < np; q++)
       near_pair2<ADJ, SELF>(sP[q][0], sP[q][1], sP[q][2], sP[q][3], tx, ty, tz, tnx, tny, tnz, kappa, kexp, eps,
                             ieps, kap2, acc0, acc1);
   } else {
-#pragma unroll 2
+#pragma unroll kNearUnroll
     for (int q = sub; q < np; q += k)
       near_pair2<ADJ, SELF>(sP[q][0], sP[q][1], sP[q][2], sP[q][3], tx, ty, tz, tnx, tny, tnz, kappa, kexp, eps,
                             ieps, kap2, acc0, acc1);
