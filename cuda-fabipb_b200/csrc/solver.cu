@@ -139,8 +139,13 @@ __host__ __device__ constexpr size_t gj_smem_bytes(int maxM) {
   return (size_t)NB * maxM * sizeof(TV) + 64 * NB * sizeof(TV) + (size_t)maxM * sizeof(int);
 }
 
+// resident blocks per SM the register allocation of pc_gj_invert_kernel<float>
+// aims at (the FP64 kernel keeps one: at two it spills)
+#ifndef FB_GJ_MIN_BLOCKS
+#define FB_GJ_MIN_BLOCKS 2
+#endif
 template <typename TV, int NB, int CS>
-__global__ void __launch_bounds__(kGjThreads, 1)
+__global__ void __launch_bounds__(kGjThreads, sizeof(TV) == 4 ? FB_GJ_MIN_BLOCKS : 1)
 pc_gj_invert_kernel(const int *__restrict__ list, const int *__restrict__ bStart, const int *__restrict__ bSize,
                     const long long *__restrict__ bOff, const long long *__restrict__ yOff, TV *inv, TV *yAll,
                     int *colSrc, int *info) {
@@ -150,6 +155,7 @@ pc_gj_invert_kernel(const int *__restrict__ list, const int *__restrict__ bStart
   __shared__ TV wbest[kGjThreads / 32];
   __shared__ int wbi[kGjThreads / 32];
   __shared__ int sPos[2 * NB], sSrc[2 * NB], sCnt;
+  __shared__ TV gBuf[64 * 2 * NB];   // one column tile's moved rows
   __shared__ TV sRk[NB], sOk[NB];
   const int rank = (CS > 1) ? (int)(blockIdx.x % CS) : 0;
   const int b = list[blockIdx.x / CS];
@@ -258,29 +264,33 @@ pc_gj_invert_kernel(const int *__restrict__ list, const int *__restrict__ bStart
       sCnt = cnt;
     }
     __syncthreads();
-    // this CTA's columns: gather the interchanged rows, rows k0.. to Y, zero them (a warp per column)
+    // this CTA's columns: gather the interchanged rows, rows k0.. to Y, zero
+    // them; per 64-column tile all (column, moved row) reads are issued
+    // together into gBuf, then, after a barrier, written back
     const int cnt = sCnt;
-    for (int jt = 64 * rank; jt < M; jt += 64 * CS)
-      for (int j = jt + warp; j < min(M, jt + 64); j += kGjThreads / 32) {
-        if (j >= k0 && j < k0 + nb) continue;
-        TV *col = A + (size_t)j * M;
-        TV v = (TV)0;
-        int r = -1;
-        if (lane < cnt) {
-          r = sPos[lane];
-          v = col[sSrc[lane]];
-        }
-        __syncwarp();
-        if (lane < cnt) {
+    for (int jt = 64 * rank; jt < M; jt += 64 * CS) {
+      const int ne = 64 * cnt;
+#pragma unroll 4
+      for (int e = t; e < ne; e += kGjThreads) {
+        const int jl = e / cnt, q = e - jl * cnt, j = jt + jl;
+        if (j < M && (j < k0 || j >= k0 + nb)) gBuf[e] = A[(size_t)j * M + sSrc[q]];
+      }
+      __syncthreads();
+      for (int e = t; e < ne; e += kGjThreads) {
+        const int jl = e / cnt, q = e - jl * cnt, j = jt + jl;
+        if (j < M && (j < k0 || j >= k0 + nb)) {
+          const int r = sPos[q];
+          TV *col = A + (size_t)j * M;
           if (r >= k0 && r < k0 + nb) {
-            Y[(size_t)j * NB + (r - k0)] = v;
+            Y[(size_t)j * NB + (r - k0)] = gBuf[e];
             col[r] = (TV)0;
           } else {
-            col[r] = v;
+            col[r] = gBuf[e];
           }
         }
       }
-    __syncthreads();
+      __syncthreads();
+    }
     // A(:, j) += P * Y(:, j) over this CTA's 64-column tiles; thread: 4 rows x 4 columns
     const int tr = t % 16, tc = t / 16;
     for (int jt = 64 * rank; jt < M; jt += 64 * CS) {
