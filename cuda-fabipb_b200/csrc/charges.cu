@@ -37,6 +37,7 @@ struct ChargeTreeDev {
   double *d_partial = nullptr;                 // energy partial sums
   int partialCap = 0;
   double *d_posOrig = nullptr, *d_chrOrig = nullptr;  // input order (direct RHS)
+  float4 *d_chgF = nullptr;   // FP32 (position - root box centre, charge), mixed contexts
 };
 
 void free_charges(Context &c) {
@@ -215,8 +216,8 @@ __global__ void rhs_direct_kernel(int n, int m, int q, const double *__restrict_
           double r[3];
           for (int k = 0; k < 3; k++) r[k] = r0[k] + t[ix] * (ax2[k] + t[jx] * ax0[k]);
           const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
-          const double ri = 1.0 / sqrt(r2);
-          const double r3i = ri / r2;
+          const double ri = rsqrt(r2);
+          const double r3i = ri * ri * ri;
           const double ip = nx[0] * r[0] + nx[1] * r[1] + nx[2] * r[2];
           i0 += ri * t[ix] * w[ix] * w[jx];
           i1 += (-ip * r3i) * t[ix] * w[ix] * w[jx];
@@ -229,6 +230,70 @@ __global__ void rhs_direct_kernel(int n, int m, int q, const double *__restrict_
   if (valid) {
     rhs[X] = s0 * fac;
     rhs[n + X] = s1 * fac;
+  }
+}
+
+// Mixed contexts, one-point rule (q = 1): the same direct sum in FP32.  The
+// panel's quadrature point and the charges are taken relative to the root
+// box centre (differences in FP64, then rounded), the pair terms use the
+// MUFU reciprocal square root, and every 64 charges are summed in FP32 and
+// added to the panel's FP64 totals.
+constexpr int kRhsTileF = 1024;
+
+__global__ void charges_to_float_kernel(int m, const double *__restrict__ pos, const double *__restrict__ chr,
+                                        double ox, double oy, double oz, float4 *out) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  out[j] = make_float4((float)(pos[3 * (size_t)j] - ox), (float)(pos[3 * (size_t)j + 1] - oy),
+                       (float)(pos[3 * (size_t)j + 2] - oz), (float)chr[j]);
+}
+
+__global__ void __launch_bounds__(256)
+rhs_direct_f32_kernel(int n, int m, const double *__restrict__ vtx, const double *__restrict__ nrm,
+                      const double *__restrict__ area, const float4 *__restrict__ chg, double ox, double oy,
+                      double oz, double fac, double *rhs) {
+  __shared__ float4 sc[kRhsTileF];
+  const int X = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = X < n;
+  const int Xs = valid ? X : 0;
+  const double *v0 = vtx + 9 * (size_t)Xs;
+  const double t = c_tLeg[1][0], wt = c_wLeg[1][0];
+  float px, py, pz;
+  {
+    double p[3];
+    for (int k = 0; k < 3; k++) p[k] = v0[k] + t * ((v0[3 + k] - v0[k]) + t * (v0[6 + k] - v0[3 + k]));
+    px = (float)(p[0] - ox);
+    py = (float)(p[1] - oy);
+    pz = (float)(p[2] - oz);
+  }
+  const float nx = (float)nrm[3 * (size_t)Xs], ny = (float)nrm[3 * (size_t)Xs + 1], nz = (float)nrm[3 * (size_t)Xs + 2];
+  double s0 = 0.0, s1 = 0.0;
+  for (int base = 0; base < m; base += kRhsTileF) {
+    const int cnt = min(kRhsTileF, m - base);
+    for (int j = threadIdx.x; j < cnt; j += blockDim.x) sc[j] = chg[base + j];
+    __syncthreads();
+    for (int j0 = 0; j0 < cnt; j0 += 64) {   // FP32 sums of 64 charges at a time
+      const int j1 = min(cnt, j0 + 64);
+      float a0 = 0.f, a1 = 0.f;
+#pragma unroll 8
+      for (int j = j0; j < j1; j++) {
+        const float4 cj = sc[j];
+        const float dx = px - cj.x, dy = py - cj.y, dz = pz - cj.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        const float ri = rsqrt_t(r2);
+        const float qr3 = cj.w * (ri * ri * ri);
+        a0 += cj.w * ri;
+        a1 += qr3 * (nx * dx + ny * dy + nz * dz);
+      }
+      s0 += (double)a0;
+      s1 -= (double)a1;
+    }
+    __syncthreads();
+  }
+  if (valid) {
+    const double W = 2.0 * area[Xs] * t * wt * wt * fac;
+    rhs[X] = s0 * W;
+    rhs[n + X] = s1 * W;
   }
 }
 
@@ -402,6 +467,21 @@ bool launch_rhs(Context &c, int useTree, double *rhs) {
   FB_CHECK(c.ct != nullptr && c.nChar > 0, "no charges set (fabipb_b200_set_charges)");
   FB_CHECK(c.prm.quad_order >= 1 && c.prm.quad_order <= 10, "quadrature order %d outside 1..10", c.prm.quad_order);
   c.launches += 1;
+  if (!useTree && c.mixed && c.prm.quad_order == 1) {
+    const bool hasRoot = c.pt.t.x.size() >= 3;   // the root box centre as the origin
+    const double ox = hasRoot ? c.pt.t.x[0] : 0.0, oy = hasRoot ? c.pt.t.x[1] : 0.0, oz = hasRoot ? c.pt.t.x[2] : 0.0;
+    if (!c.ct->d_chgF) {
+      if (!c.ct->arena.alloc_n(&c.ct->d_chgF, (size_t)c.nChar)) return false;
+      charges_to_float_kernel<<<ceil_div(c.nChar, 256), 256, 0, c.stream>>>(c.nChar, c.ct->d_posOrig, c.ct->d_chrOrig,
+                                                                           ox, oy, oz, c.ct->d_chgF);
+      c.launches += 1;
+    }
+    rhs_direct_f32_kernel<<<ceil_div(c.n, 256), 256, 0, c.stream>>>(
+        c.n, c.nChar, c.d_vtx, c.d_nrm, c.d_area, c.ct->d_chgF, ox, oy, oz,
+        c.rhsFac != 0.0 ? c.rhsFac : kFourPiI / c.prm.eps1, rhs);
+    FB_CUDA(cudaGetLastError());
+    return true;
+  }
   if (!useTree) {
     rhs_direct_kernel<<<ceil_div(c.n, 128), 128, 0, c.stream>>>(c.n, c.nChar, c.prm.quad_order, c.d_vtx, c.d_nrm,
                                                                 c.d_area, c.ct->d_posOrig, c.ct->d_chrOrig,
