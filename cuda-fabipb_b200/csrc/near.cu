@@ -25,6 +25,9 @@
 #include <thread>
 #include <unordered_map>
 
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
 #include "context.cuh"
 #include "quad.cuh"
 
@@ -481,6 +484,170 @@ inline uint64_t dbits(double v) {
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Special-pair search on the device: the panels sharing a vertex with X (by
+// exact coordinates, -0.0 = 0.0, as nrCommonVtx, src/numQuad.c:312), X itself,
+// kept when their leaves are near, ascending, as CSR by X.  The 3N corners are
+// sorted by a 64-bit hash of their coordinates; equal-hash runs are checked
+// for exact equality (a collision sends the search to the host path, as does
+// a panel with more than kSpCand candidates).
+// ---------------------------------------------------------------------------
+constexpr int kSpCand = 64;
+
+__device__ __forceinline__ unsigned long long vtx_bits(double v) {
+  return (unsigned long long)__double_as_longlong(v == 0.0 ? 0.0 : v);
+}
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {   // splitmix64 finaliser
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+
+__global__ void corner_keys_kernel(int nc, const double *__restrict__ vtx, unsigned long long *keys, int *vals) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nc) return;
+  const double *x = vtx + 3 * (size_t)i;   // corner i = vertex i%3 of panel i/3
+  keys[i] = mix64(vtx_bits(x[0]) + mix64(vtx_bits(x[1]) + mix64(vtx_bits(x[2]))));
+  vals[i] = i;
+}
+
+__global__ void corner_runs_kernel(int nc, const unsigned long long *__restrict__ keys, const int *__restrict__ vals,
+                                   const double *__restrict__ vtx, int *flag, int *err) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nc) return;
+  int f = 1;
+  if (p > 0 && keys[p] == keys[p - 1]) {
+    f = 0;
+    const double *a = vtx + 3 * (size_t)vals[p], *b = vtx + 3 * (size_t)vals[p - 1];
+    for (int k = 0; k < 3; k++)
+      if (vtx_bits(a[k]) != vtx_bits(b[k])) atomicExch(err, 1);   // hash collision
+  }
+  flag[p] = f;
+}
+
+// gid: inclusive scan of the run flags (group g = gid - 1)
+__global__ void corner_groups_kernel(int nc, const int *__restrict__ flag, const int *__restrict__ gid,
+                                     const int *__restrict__ vals, int *gStart, int *cornerGroup) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nc) return;
+  const int g = gid[p] - 1;
+  if (flag[p]) gStart[g] = p;
+  if (p == nc - 1) gStart[g + 1] = nc;
+  cornerGroup[vals[p]] = g;
+}
+
+// WRITE = false: count per panel into cnt; true: write the sources at off[X]
+template <bool WRITE>
+__global__ void special_pairs_kernel(int n, const int *__restrict__ cornerGroup, const int *__restrict__ gStart,
+                                     const int *__restrict__ vals, const int *__restrict__ leafOf,
+                                     const int *__restrict__ nearOff, const int *__restrict__ nearSorted, int *cnt,
+                                     const int *__restrict__ off, int *spSrc, int *spDst, int *err) {
+  const int X = blockIdx.x * blockDim.x + threadIdx.x;
+  if (X >= n) return;
+  int cand[kSpCand];
+  int m = 0;
+  cand[m++] = X;
+  for (int k = 0; k < 3; k++) {
+    const int g = cornerGroup[3 * X + k];
+    for (int p = gStart[g]; p < gStart[g + 1]; p++) {
+      if (m == kSpCand) {
+        atomicExch(err, 2);
+        if (!WRITE) cnt[X] = 0;
+        return;
+      }
+      cand[m++] = vals[p] / 3;
+    }
+  }
+  for (int i = 1; i < m; i++) {   // insertion sort of the few candidates
+    const int v = cand[i];
+    int j = i - 1;
+    while (j >= 0 && cand[j] > v) {
+      cand[j + 1] = cand[j];
+      j--;
+    }
+    cand[j + 1] = v;
+  }
+  const int L = leafOf[X];
+  const int *ns = nearSorted + nearOff[L];
+  const int nn = nearOff[L + 1] - nearOff[L];
+  int o = WRITE ? off[X] : 0, c = 0;
+  for (int i = 0; i < m; i++) {
+    if (i > 0 && cand[i] == cand[i - 1]) continue;
+    const int Y = cand[i], LY = leafOf[Y];
+    int lo = 0, hi = nn;   // LY in the sorted near list of L?
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (ns[mid] < LY) lo = mid + 1;
+      else hi = mid;
+    }
+    if (lo < nn && ns[lo] == LY) {
+      if (WRITE) {
+        spSrc[o] = Y;
+        spDst[o] = X;
+        o++;
+      }
+      c++;
+    }
+  }
+  if (!WRITE) cnt[X] = c;
+}
+
+// 1: tables built (c.d_spOff, c.d_spSrc, *d_spDst, c.nSpecial); 0: use the
+// host search instead; -1: CUDA error (message set)
+static int special_pairs_device(Context &c, const std::vector<int> &nearSortedFlat, int **d_spDst) {
+  const int n = c.n, nc = 3 * n;
+  cudaStream_t s = c.stream;
+  DevArena tmp;
+  unsigned long long *keys = nullptr, *keysS = nullptr;
+  int *vals = nullptr, *valsS = nullptr, *flag = nullptr, *gid = nullptr, *cornerGroup = nullptr, *gStart = nullptr;
+  int *cnt = nullptr, *err = nullptr, *d_nearSorted = nullptr;
+  if (!tmp.alloc_n(&keys, nc) || !tmp.alloc_n(&keysS, nc) || !tmp.alloc_n(&vals, nc) || !tmp.alloc_n(&valsS, nc) ||
+      !tmp.alloc_n(&flag, nc) || !tmp.alloc_n(&gid, nc) || !tmp.alloc_n(&cornerGroup, nc) ||
+      !tmp.alloc_n(&gStart, (size_t)nc + 1) || !tmp.alloc_n(&cnt, (size_t)n + 1) || !tmp.alloc_n(&err, 1) ||
+      !tmp.upload(&d_nearSorted, nearSortedFlat, s))
+    return -1;
+  FB_CUDA(cudaMemsetAsync(err, 0, sizeof(int), s));
+  size_t tb1 = 0, tb2 = 0, tb3 = 0;
+  FB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb1, keys, keysS, vals, valsS, nc, 0, 64, s));
+  FB_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tb2, flag, gid, nc, s));
+  FB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb3, cnt, cnt, n + 1, s));
+  void *tbuf = nullptr;
+  if (!tmp.alloc(&tbuf, std::max(tb1, std::max(tb2, tb3)))) return -1;
+  const size_t tbytes = std::max(tb1, std::max(tb2, tb3));
+  corner_keys_kernel<<<ceil_div(nc, 256), 256, 0, s>>>(nc, c.d_vtx, keys, vals);
+  size_t tb = tbytes;
+  FB_CUDA(cub::DeviceRadixSort::SortPairs(tbuf, tb, keys, keysS, vals, valsS, nc, 0, 64, s));
+  corner_runs_kernel<<<ceil_div(nc, 256), 256, 0, s>>>(nc, keysS, valsS, c.d_vtx, flag, err);
+  tb = tbytes;
+  FB_CUDA(cub::DeviceScan::InclusiveSum(tbuf, tb, flag, gid, nc, s));
+  corner_groups_kernel<<<ceil_div(nc, 256), 256, 0, s>>>(nc, flag, gid, valsS, gStart, cornerGroup);
+  special_pairs_kernel<false><<<ceil_div(n, 128), 128, 0, s>>>(n, cornerGroup, gStart, valsS, c.d_leafOfPanel,
+                                                               c.d_nearOff, d_nearSorted, cnt, nullptr, nullptr,
+                                                               nullptr, err);
+  FB_CUDA(cudaMemsetAsync(cnt + n, 0, sizeof(int), s));
+  if (!c.arena.alloc_n(&c.d_spOff, (size_t)n + 1)) return -1;
+  tb = tbytes;
+  FB_CUDA(cub::DeviceScan::ExclusiveSum(tbuf, tb, cnt, c.d_spOff, n + 1, s));
+  int hErr = 0, total = 0;
+  FB_CUDA(cudaMemcpyAsync(&hErr, err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  FB_CUDA(cudaMemcpyAsync(&total, c.d_spOff + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+  FB_CUDA(cudaStreamSynchronize(s));
+  FB_CUDA(cudaGetLastError());
+  if (hErr) return 0;
+  c.nSpecial = total;
+  if (!c.arena.alloc_n(&c.d_spSrc, (size_t)std::max(total, 1)) || !c.arena.alloc_n(d_spDst, (size_t)std::max(total, 1)))
+    return -1;
+  special_pairs_kernel<true><<<ceil_div(n, 128), 128, 0, s>>>(n, cornerGroup, gStart, valsS, c.d_leafOfPanel,
+                                                              c.d_nearOff, d_nearSorted, nullptr, c.d_spOff,
+                                                              c.d_spSrc, *d_spDst, err);
+  FB_CUDA(cudaGetLastError());
+  FB_CUDA(cudaStreamSynchronize(s));   // the temporaries are freed on return
+  return 1;
+}
+
+static bool special_pairs_host(Context &c, const std::vector<int> &nearSortedFlat, int **d_spDst);
+static bool setup_near_targets(Context &c);
+
 bool setup_near(Context &c) {
   const PanelTree &pt = c.pt;
   const int n = c.n;
@@ -534,7 +701,37 @@ bool setup_near(Context &c) {
 
   StageTimer tm("near_setup", s);
   // special pairs: panels sharing a vertex (exact coordinates), restricted to
-  // near leaf pairs, plus the panel itself
+  // near leaf pairs, plus the panel itself -- on the device, or on the host
+  // when the device search declines
+  std::vector<int> nearSortedFlat(pt.nearSrc.size());
+  for (int L = 0; L < pt.nLeaves; L++) {
+    std::copy(pt.nearSrc.begin() + pt.nearOff[L], pt.nearSrc.begin() + pt.nearOff[L + 1],
+              nearSortedFlat.begin() + pt.nearOff[L]);
+    std::sort(nearSortedFlat.begin() + pt.nearOff[L], nearSortedFlat.begin() + pt.nearOff[L + 1]);
+  }
+  int *d_spDst = nullptr;
+  // FABIPB_B200_HOST_SPECIAL=1 forces the host search (the tests compare the two)
+  const int onDevice = getenv("FABIPB_B200_HOST_SPECIAL") ? 0 : special_pairs_device(c, nearSortedFlat, &d_spDst);
+  if (onDevice < 0) return false;
+  if (onDevice == 0 && !special_pairs_host(c, nearSortedFlat, &d_spDst)) return false;
+  tm.mark("special_pairs");
+  if (!c.arena.alloc_n(&c.d_spK, (size_t)std::max<long long>(c.nSpecial, 1))) return false;
+  if (c.nSpecial > 0) {
+    special_coeff_kernel<<<ceil_div(c.nSpecial, 128), 128, 0, s>>>(
+        c.nSpecial, d_spDst, c.d_spSrc, c.d_vtx, c.d_nrm, c.d_area, c.prm.quad_order, c.prm.kappa,
+        c.epsilon, c.d_spK, nullptr);
+    FB_CUDA(cudaGetLastError());
+  }
+  tm.mark("special_coeff");
+  return setup_near_targets(c);
+}
+
+// The host search (used when the device search declines): vertex ids from a
+// hash map of exact coordinates, per panel its sharing panels, on host threads.
+static bool special_pairs_host(Context &c, const std::vector<int> &nearSortedFlat, int **d_spDst) {
+  const PanelTree &pt = c.pt;
+  const int n = c.n;
+  cudaStream_t s = c.stream;
   std::unordered_map<VKey, int, VKeyHash> vid;
   vid.reserve((size_t)n * 2);
   std::vector<int> pv(3 * (size_t)n);
@@ -563,11 +760,6 @@ bool setup_near(Context &c) {
   std::vector<int> leafOf(n);
   for (int L = 0; L < pt.nLeaves; L++)
     for (int k = 0; k < pt.leafCount[L]; k++) leafOf[pt.leafStart[L] + k] = L;
-  std::vector<std::vector<int>> nearSorted(pt.nLeaves);
-  for (int L = 0; L < pt.nLeaves; L++) {
-    nearSorted[L].assign(pt.nearSrc.begin() + pt.nearOff[L], pt.nearSrc.begin() + pt.nearOff[L + 1]);
-    std::sort(nearSorted[L].begin(), nearSorted[L].end());
-  }
   // per panel: itself and the panels sharing a vertex with it, ascending,
   // kept when their leaves are near; chunks of panels on host threads, merged
   // in panel order
@@ -589,10 +781,11 @@ bool setup_near(Context &c) {
       }
       std::sort(cand.begin(), cand.end());
       cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
-      const std::vector<int> &ns = nearSorted[leafOf[X]];
+      const int *nb = nearSortedFlat.data() + pt.nearOff[leafOf[X]];
+      const int *ne = nearSortedFlat.data() + pt.nearOff[leafOf[X] + 1];
       int cnt = 0;
       for (int Y : cand)
-        if (std::binary_search(ns.begin(), ns.end(), leafOf[Y])) {
+        if (std::binary_search(nb, ne, leafOf[Y])) {
           out.push_back(Y);
           cnt++;
         }
@@ -612,21 +805,16 @@ bool setup_near(Context &c) {
   for (int X = 0; X < n; X++)
     for (int e = spOff[X]; e < spOff[X + 1]; e++) spDst[e] = X;
   c.nSpecial = (long long)spSrc.size();
-  tm.mark("special_pairs_host");
-  int *d_spDst = nullptr;
   if (!c.arena.upload(&c.d_spOff, spOff, s)) return false;
   if (!c.arena.upload(&c.d_spSrc, spSrc, s)) return false;
-  if (!c.arena.upload(&d_spDst, spDst, s)) return false;
-  if (!c.arena.alloc_n(&c.d_spK, (size_t)std::max<long long>(c.nSpecial, 1))) return false;
-  if (c.nSpecial > 0) {
-    special_coeff_kernel<<<ceil_div(c.nSpecial, 128), 128, 0, s>>>(
-        c.nSpecial, d_spDst, c.d_spSrc, c.d_vtx, c.d_nrm, c.d_area, c.prm.quad_order, c.prm.kappa,
-        c.epsilon, c.d_spK, nullptr);
-    FB_CUDA(cudaGetLastError());
-  }
+  if (!c.arena.upload(d_spDst, spDst, s)) return false;
+  return true;
+}
 
-  tm.mark("special_coeff");
-  // static target geometry relative to the leaf centres
+// static target geometry relative to the leaf centres
+static bool setup_near_targets(Context &c) {
+  const int n = c.n;
+  cudaStream_t s = c.stream;
   size_t vb = c.mixed ? sizeof(float4) : sizeof(double4);
   if (!c.arena.alloc(&c.d_tgtP, vb * n) || !c.arena.alloc(&c.d_tgtN, vb * n) ||
       !c.arena.alloc(&c.d_srcA, vb * n) || !c.arena.alloc(&c.d_srcB, vb * n))

@@ -96,6 +96,19 @@ def test_apply_alpha_beta_semantics(case_dir, golden_meta, oracles):
     assert rel_l2(got, ref) < 1e-12
 
 
+@pytest.mark.parametrize("name", CASES)
+def test_special_pairs_device_matches_host(name, case_dir, golden_meta, monkeypatch):
+    """The device special-pair search (sorted corner hashes) builds the same
+    CSR table as the host search (hash map of exact coordinates): same count,
+    and the FP64 near field is bit-identical."""
+    sg = make_golden.seeded_sigma(surface(case_dir, golden_meta, name, lib.FP64)[0].n, 3)
+    s_dev, _, _ = surface(case_dir, golden_meta, name, lib.FP64)
+    monkeypatch.setenv("FABIPB_B200_HOST_SPECIAL", "1")
+    s_host, _, _ = surface(case_dir, golden_meta, name, lib.FP64)
+    assert s_dev.info()["special_pairs"] == s_host.info()["special_pairs"] > 0
+    assert np.array_equal(s_dev.apply(sg, part=lib.NEAR), s_host.apply(sg, part=lib.NEAR))
+
+
 @pytest.mark.parametrize("precision", [lib.FP64, lib.MIXED])
 @pytest.mark.parametrize("name", CASES)
 def test_rhs_direct(name, precision, case_dir, golden_meta):
