@@ -1,6 +1,7 @@
 // api.cu -- context lifecycle, composite operators and the plain-pointer C ABI
 // declared in include/fabipb_b200.h.
 #include <chrono>
+#include <thread>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -111,11 +112,20 @@ bool setup_geometry(Context &c, const double *vtx, const double *nrm, const doub
   c.h_vtx.resize(9 * (size_t)n);
   c.h_nrm.resize(3 * (size_t)n);
   c.h_area.resize(n);
-  for (int i = 0; i < n; i++) {
-    int o = pt.order[i];
-    memcpy(&c.h_vtx[9 * (size_t)i], &vtx[9 * (size_t)o], 9 * sizeof(double));
-    memcpy(&c.h_nrm[3 * (size_t)i], &nrm[3 * (size_t)o], 3 * sizeof(double));
-    c.h_area[i] = area[o];
+  {   // the panels in tree order, gathered on host threads
+    auto gather = [&](int i0, int i1) {
+      for (int i = i0; i < i1; i++) {
+        int o = pt.order[i];
+        memcpy(&c.h_vtx[9 * (size_t)i], &vtx[9 * (size_t)o], 9 * sizeof(double));
+        memcpy(&c.h_nrm[3 * (size_t)i], &nrm[3 * (size_t)o], 3 * sizeof(double));
+        c.h_area[i] = area[o];
+      }
+    };
+    const int nth = n < 65536 ? 1 : (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (int th = 1; th < nth; th++) pool.emplace_back(gather, (int)((long long)n * th / nth), (int)((long long)n * (th + 1) / nth));
+    gather(0, (int)((long long)n / nth));
+    for (auto &t : pool) t.join();
   }
   std::vector<int> leafOf(n);
   std::vector<double> leafCtr(3 * (size_t)pt.nLeaves);
