@@ -69,6 +69,62 @@ __global__ void energy_weights_kernel(int n, int m, int q, const double *__restr
   out[n + X] = s0;   // dpdn slot
 }
 
+// Mixed contexts, one-point rule: the same weights with FP32 pair terms
+// (positions relative to the root box centre, MUFU rsqrt/exp2), summed in
+// FP32 over 64 charges at a time and in FP64 above.
+__global__ void __launch_bounds__(256)
+energy_weights_f32_kernel(int n, int m, const double *__restrict__ vtx, const double *__restrict__ nrm,
+                          const double *__restrict__ area, const float4 *__restrict__ chg, double ox, double oy,
+                          double oz, float kappa, float kexp, float eps, double *out) {
+  __shared__ float4 sc[kRhsTileF];
+  const int X = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool valid = X < n;
+  const int Xs = valid ? X : 0;
+  const double *v0 = vtx + 9 * (size_t)Xs;
+  const double t = c_tLeg[1][0], wt = c_wLeg[1][0];
+  float px, py, pz;
+  {
+    double p[3];
+    for (int k = 0; k < 3; k++) p[k] = v0[k] + t * ((v0[3 + k] - v0[k]) + t * (v0[6 + k] - v0[3 + k]));
+    px = (float)(p[0] - ox);
+    py = (float)(p[1] - oy);
+    pz = (float)(p[2] - oz);
+  }
+  const float nx = (float)nrm[3 * (size_t)Xs], ny = (float)nrm[3 * (size_t)Xs + 1], nz = (float)nrm[3 * (size_t)Xs + 2];
+  const float f4 = (float)kFourPiI;
+  double s0 = 0.0, s1 = 0.0;
+  for (int base = 0; base < m; base += kRhsTileF) {
+    const int cnt = min(kRhsTileF, m - base);
+    for (int j = threadIdx.x; j < cnt; j += blockDim.x) sc[j] = chg[base + j];
+    __syncthreads();
+    for (int j0 = 0; j0 < cnt; j0 += 64) {
+      const int j1 = min(cnt, j0 + 64);
+      float a0 = 0.f, a1 = 0.f;
+#pragma unroll 4
+      for (int j = j0; j < j1; j++) {
+        const float4 cj = sc[j];
+        const float dx = px - cj.x, dy = py - cj.y, dz = pz - cj.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        const float ri = rsqrt_t(r2);
+        const float r = r2 * ri;
+        const float e = expneg_t(kexp, r);
+        const float G0 = f4 * ri;
+        const float ip = nx * dx + ny * dy + nz * dz;
+        const float dG0dn = -ip * G0 * ri * ri;
+        a0 += cj.w * (G0 - e * G0);                                 // G0 - Gk
+        a1 += cj.w * ((eps * (kappa * r + 1.f) * e - 1.f) * dG0dn);  // eps dGk/dn - dG0/dn
+      }
+      s0 += (double)a0;
+      s1 += (double)a1;
+    }
+    __syncthreads();
+  }
+  if (!valid) return;
+  const double W = 2.0 * area[Xs] * t * wt * wt;
+  out[X] = s1 * W;       // pot slot
+  out[n + X] = s0 * W;   // dpdn slot
+}
+
 // Per surface quadrature point: position, normal and the four weights
 //   a1 = 2A t w w sigma_dpdn, a2 = 2A t w w sigma_pot,
 //   a3 = 2A t w w fac lambda_pot, a4 = 2A t w w fac lambda_dpdn.
@@ -92,8 +148,86 @@ __global__ void grad_records_kernel(int n, int q, const double *__restrict__ vtx
   rw[id] = make_double2(a * fac * lam[X], a * fac * lam[n + X]);
 }
 
+// The records of a mixed context, one-point rule, in FP32, with the weights
+// pre-combined for charge_grad_f32_kernel (f = 1/(4 pi), a_i as above):
+//   rp = (x_w - o, f a1),  rn = (n, f a2 eps),
+//   rx = (f a1 + a3, a4 - f a2, f a1 kappa, f a2 eps kappa^2).
+__global__ void grad_records_f32_kernel(int n, const double *__restrict__ vtx, const double *__restrict__ nrm,
+                                        const double *__restrict__ area, const double *__restrict__ sgm,
+                                        const double *__restrict__ lam, double fac, double ox, double oy, double oz,
+                                        double kappa, double eps, float4 *rp, float4 *rn, float4 *rx) {
+  const int X = blockIdx.x * blockDim.x + threadIdx.x;
+  if (X >= n) return;
+  const double *v0 = vtx + 9 * (size_t)X;
+  const double t = c_tLeg[1][0], w = c_wLeg[1][0];
+  double p[3];
+  for (int k = 0; k < 3; k++) p[k] = v0[k] + t * ((v0[3 + k] - v0[k]) + t * (v0[6 + k] - v0[3 + k]));
+  const double a = 2.0 * area[X] * t * w * w;
+  const double f1 = kFourPiI * a * sgm[n + X], f2 = kFourPiI * a * sgm[X];
+  const double a3 = a * fac * lam[X], a4 = a * fac * lam[n + X];
+  rp[X] = make_float4((float)(p[0] - ox), (float)(p[1] - oy), (float)(p[2] - oz), (float)f1);
+  rn[X] = make_float4((float)nrm[3 * (size_t)X], (float)nrm[3 * (size_t)X + 1], (float)nrm[3 * (size_t)X + 2],
+                      (float)(f2 * eps));
+  rx[X] = make_float4((float)(f1 + a3), (float)(a4 - f2), (float)(f1 * kappa), (float)(f2 * eps * kappa * kappa));
+}
+
 constexpr int kGradCharges = 128;   // charges per block
 constexpr int kGradTile = 128;      // records staged per step
+
+// charge_grad_kernel with FP32 pair terms (records and charges relative to
+// the root box centre), FP32 sums over 64 records at a time, FP64 above.  With
+// A = f a1 (1 - e) + a3 and B = f a2 (eps c - 1) + a4 (e = exp(-kappa r),
+// c = (kappa r + 1) e), the record's term and its gradient in x are
+//   phi  = A/r - (n.x) B/r^3,
+//   grad = x [f a1 kappa e/r^2 - A/r^3 + (n.x)/r^3 (3B/r^2 + f a2 eps kappa^2 e)] - n B/r^3.
+__global__ void __launch_bounds__(kGradCharges)
+charge_grad_f32_kernel(long long nRec, int m, long long chunkLen, const float4 *__restrict__ rp,
+                       const float4 *__restrict__ rn, const float4 *__restrict__ rx, const float4 *__restrict__ chg,
+                       float kappa, float kexp, double4 *part) {
+  __shared__ float4 sp[kGradTile], sn[kGradTile], sx_[kGradTile];
+  const int k = blockIdx.x * kGradCharges + threadIdx.x;
+  const bool valid = k < m;
+  const float4 ck = valid ? chg[k] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const long long r0 = (long long)blockIdx.y * chunkLen, r1 = min(nRec, r0 + chunkLen);
+  double phi = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;   // gradient with respect to x = x_w - r_k
+  for (long long b = r0; b < r1; b += kGradTile) {
+    const int cnt = (int)min((long long)kGradTile, r1 - b);
+    for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+      sp[j] = rp[b + j];
+      sn[j] = rn[b + j];
+      sx_[j] = rx[b + j];
+    }
+    __syncthreads();
+    for (int j0 = 0; j0 < cnt; j0 += 64) {
+      const int j1 = min(cnt, j0 + 64);
+      float fphi = 0.f, fx = 0.f, fy = 0.f, fz = 0.f;
+#pragma unroll 2
+      for (int j = j0; j < j1; j++) {
+        const float4 P = sp[j], N = sn[j], R = sx_[j];
+        const float x = P.x - ck.x, y = P.y - ck.y, z = P.z - ck.z;
+        const float r2 = x * x + y * y + z * z;
+        const float ri = rsqrt_t(r2), r = r2 * ri, ri2 = ri * ri, ri3 = ri2 * ri;
+        const float e = expneg_t(kexp, r), c = (kappa * r + 1.f) * e;
+        const float ip = N.x * x + N.y * y + N.z * z;
+        const float A = R.x - P.w * e;          // f a1 (1 - e) + a3
+        const float B = N.w * c + R.y;          // f a2 eps c + a4 - f a2
+        const float t = ip * ri3;
+        fphi += A * ri - t * B;
+        const float sxv = R.z * e * ri2 - A * ri3 + t * (3.f * ri2 * B + R.w * e);
+        const float snv = -ri3 * B;
+        fx += sxv * x + snv * N.x;
+        fy += sxv * y + snv * N.y;
+        fz += sxv * z + snv * N.z;
+      }
+      phi += (double)fphi;
+      gx += (double)fx;
+      gy += (double)fy;
+      gz += (double)fz;
+    }
+    __syncthreads();
+  }
+  if (valid) part[(size_t)blockIdx.y * m + k] = make_double4(phi, -gx, -gy, -gz);   // d/dr_k = -d/dx
+}
 
 // phi_k and grad_{r_k} phi_k over one chunk of the records, for a tile of
 // charges (one thread per charge); part[chunk][k] = (phi, grad).
@@ -202,6 +336,16 @@ static bool adj_state(Context &c) {
 bool launch_energy_weights(Context &c, double *e) {
   FB_CHECK(c.ct != nullptr && c.nChar > 0, "no charges set (fabipb_b200_set_charges)");
   FB_CHECK(c.prm.quad_order >= 1 && c.prm.quad_order <= 10, "quadrature order %d outside 1..10", c.prm.quad_order);
+  if (c.mixed && c.prm.quad_order == 1) {
+    double ox, oy, oz;
+    if (!charges_f32(c, &ox, &oy, &oz)) return false;
+    energy_weights_f32_kernel<<<ceil_div(c.n, 256), 256, 0, c.stream>>>(
+        c.n, c.nChar, c.d_vtx, c.d_nrm, c.d_area, c.ct->d_chgF, ox, oy, oz, (float)c.prm.kappa,
+        (float)(-c.prm.kappa * 1.4426950408889634), (float)c.epsilon, e);
+    c.launches += 1;
+    FB_CUDA(cudaGetLastError());
+    return true;
+  }
   energy_weights_kernel<<<ceil_div(c.n, 128), 128, 0, c.stream>>>(c.n, c.nChar, c.prm.quad_order, c.d_vtx, c.d_nrm,
                                                                   c.d_area, c.ct->d_posOrig, c.ct->d_chrOrig,
                                                                   c.prm.kappa, c.epsilon, e);
@@ -249,8 +393,17 @@ bool adjoint_backward(Context &c, double scale, int restart, int maxit, double t
     a.recCap = nRec;
   }
   const double fac = c.rhsFac != 0.0 ? c.rhsFac : kFourPiI / c.prm.eps1;
-  grad_records_kernel<<<ceil_div(nRec, 256), 256, 0, c.stream>>>(c.n, q, c.d_vtx, c.d_nrm, c.d_area, a.d_sigma,
-                                                                 a.d_lam, fac, a.d_rp, a.d_rn, a.d_rw);
+  const bool f32 = c.mixed && q == 1;   // FP32 pair terms (records of 48 bytes in the FP64 arrays' space)
+  double ox = 0.0, oy = 0.0, oz = 0.0;
+  if (f32) {
+    if (!charges_f32(c, &ox, &oy, &oz)) return false;
+    grad_records_f32_kernel<<<ceil_div(nRec, 256), 256, 0, c.stream>>>(
+        c.n, c.d_vtx, c.d_nrm, c.d_area, a.d_sigma, a.d_lam, fac, ox, oy, oz, c.prm.kappa, c.epsilon,
+        (float4 *)a.d_rp, (float4 *)a.d_rn, (float4 *)a.d_rw);
+  } else {
+    grad_records_kernel<<<ceil_div(nRec, 256), 256, 0, c.stream>>>(c.n, q, c.d_vtx, c.d_nrm, c.d_area, a.d_sigma,
+                                                                   a.d_lam, fac, a.d_rp, a.d_rn, a.d_rw);
+  }
   // enough blocks to fill the GPU: chunks of the records times tiles of charges
   const int tiles = (int)ceil_div(m, kGradCharges);
   const long long want = (2368LL + tiles - 1) / tiles, most = (nRec + 4095) / 4096;
@@ -261,8 +414,13 @@ bool adjoint_backward(Context &c, double scale, int restart, int maxit, double t
     a.partCap = (long long)nChunks * m;
   }
   dim3 grid(tiles, nChunks);
-  charge_grad_kernel<<<grid, kGradCharges, 0, c.stream>>>(nRec, m, chunkLen, a.d_rp, a.d_rn, a.d_rw,
-                                                         c.ct->d_posOrig, c.prm.kappa, c.epsilon, a.d_part);
+  if (f32)
+    charge_grad_f32_kernel<<<grid, kGradCharges, 0, c.stream>>>(
+        nRec, m, chunkLen, (const float4 *)a.d_rp, (const float4 *)a.d_rn, (const float4 *)a.d_rw, c.ct->d_chgF,
+        (float)c.prm.kappa, (float)(-c.prm.kappa * 1.4426950408889634), a.d_part);
+  else
+    charge_grad_kernel<<<grid, kGradCharges, 0, c.stream>>>(nRec, m, chunkLen, a.d_rp, a.d_rn, a.d_rw,
+                                                           c.ct->d_posOrig, c.prm.kappa, c.epsilon, a.d_part);
   charge_grad_reduce_kernel<<<ceil_div(m, 256), 256, 0, c.stream>>>(m, nChunks, a.d_part, c.ct->d_chrOrig, scale,
                                                                     dEdq, dEdx);
   c.launches += 3;

@@ -882,31 +882,45 @@ __global__ void special_transpose_kernel(long long nSp, const long long *__restr
   spKT[e] = make_double4(d.w, d.y, d.z, d.x);
 }
 
+// mate[e] of entry e = (X, Y): the index of (Y, X); *bad = X + 1 when missing
+__global__ void special_mate_kernel(int n, const int *__restrict__ spOff, const int *__restrict__ spSrc,
+                                    long long *mate, int *bad) {
+  const int X = blockIdx.x * blockDim.x + threadIdx.x;
+  if (X >= n) return;
+  for (int e = spOff[X]; e < spOff[X + 1]; e++) {
+    const int Y = spSrc[e];
+    int lo = spOff[Y], hi = spOff[Y + 1];
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (spSrc[mid] < X) lo = mid + 1;
+      else hi = mid;
+    }
+    if (lo < spOff[Y + 1] && spSrc[lo] == X) mate[e] = lo;
+    else atomicExch(bad, X + 1);
+  }
+}
+
 static bool setup_near_adjoint(Context &c) {
   if (c.d_spKT) return true;
   // the special-pair set is symmetric (shared vertex, near leaf pairs): find
-  // for every entry (X, Y) the entry (Y, X)
+  // for every entry (X, Y) the entry (Y, X), by binary search in the
+  // (ascending) row of Y, on the device
   const int n = c.n;
-  std::vector<int> spOff(n + 1), spSrc((size_t)c.nSpecial);
-  FB_CUDA(cudaMemcpyAsync(spOff.data(), c.d_spOff, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-  if (c.nSpecial > 0)
-    FB_CUDA(cudaMemcpyAsync(spSrc.data(), c.d_spSrc, c.nSpecial * sizeof(int), cudaMemcpyDeviceToHost, c.stream));
-  FB_CUDA(cudaStreamSynchronize(c.stream));
-  std::vector<long long> mate((size_t)c.nSpecial);
-  for (int X = 0; X < n; X++)
-    for (int e = spOff[X]; e < spOff[X + 1]; e++) {
-      const int Y = spSrc[e];
-      const int *b = spSrc.data() + spOff[Y], *en = spSrc.data() + spOff[Y + 1];
-      const int *hit = std::find(b, en, X);
-      FB_CHECK(hit != en, "special pair (%d,%d) has no mirror entry", X, Y);
-      mate[e] = (long long)(hit - spSrc.data());
-    }
+  DevArena tmp;
   long long *d_mate = nullptr;
-  if (!c.arena.upload(&d_mate, mate, c.stream)) return false;
+  int *d_bad = nullptr;
+  if (!tmp.alloc_n(&d_mate, (size_t)std::max<long long>(c.nSpecial, 1)) || !tmp.alloc_n(&d_bad, 1)) return false;
+  FB_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), c.stream));
+  special_mate_kernel<<<ceil_div(n, 256), 256, 0, c.stream>>>(n, c.d_spOff, c.d_spSrc, d_mate, d_bad);
+  int bad = 0;
+  FB_CUDA(cudaMemcpyAsync(&bad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, c.stream));
+  FB_CUDA(cudaStreamSynchronize(c.stream));
+  FB_CHECK(bad == 0, "special pair (%d, .) has no mirror entry", bad - 1);
   if (!c.arena.alloc_n(&c.d_spKT, (size_t)std::max<long long>(c.nSpecial, 1))) return false;
   if (c.nSpecial > 0)
     special_transpose_kernel<<<ceil_div(c.nSpecial, 256), 256, 0, c.stream>>>(c.nSpecial, d_mate, c.d_spK, c.d_spKT);
   FB_CUDA(cudaGetLastError());
+  FB_CUDA(cudaStreamSynchronize(c.stream));   // the mates are freed on return
   return true;
 }
 
