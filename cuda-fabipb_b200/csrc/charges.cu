@@ -463,19 +463,30 @@ static void launch_walk(Context &c, int mode, const double *sgm, double *rhs, do
     default: launch_walk<9>(__VA_ARGS__); break;      \
   }
 
+// The FP32 charge records of a mixed context (position minus the root box
+// centre, charge), made on first use; the origin is returned.
+bool charges_f32(Context &c, double *ox, double *oy, double *oz) {
+  const bool hasRoot = c.pt.t.x.size() >= 3;
+  *ox = hasRoot ? c.pt.t.x[0] : 0.0;
+  *oy = hasRoot ? c.pt.t.x[1] : 0.0;
+  *oz = hasRoot ? c.pt.t.x[2] : 0.0;
+  if (!c.ct->d_chgF) {
+    if (!c.ct->arena.alloc_n(&c.ct->d_chgF, (size_t)c.nChar)) return false;
+    charges_to_float_kernel<<<ceil_div(c.nChar, 256), 256, 0, c.stream>>>(c.nChar, c.ct->d_posOrig, c.ct->d_chrOrig,
+                                                                         *ox, *oy, *oz, c.ct->d_chgF);
+    c.launches += 1;
+    FB_CUDA(cudaGetLastError());
+  }
+  return true;
+}
+
 bool launch_rhs(Context &c, int useTree, double *rhs) {
   FB_CHECK(c.ct != nullptr && c.nChar > 0, "no charges set (fabipb_b200_set_charges)");
   FB_CHECK(c.prm.quad_order >= 1 && c.prm.quad_order <= 10, "quadrature order %d outside 1..10", c.prm.quad_order);
   c.launches += 1;
   if (!useTree && c.mixed && c.prm.quad_order == 1) {
-    const bool hasRoot = c.pt.t.x.size() >= 3;   // the root box centre as the origin
-    const double ox = hasRoot ? c.pt.t.x[0] : 0.0, oy = hasRoot ? c.pt.t.x[1] : 0.0, oz = hasRoot ? c.pt.t.x[2] : 0.0;
-    if (!c.ct->d_chgF) {
-      if (!c.ct->arena.alloc_n(&c.ct->d_chgF, (size_t)c.nChar)) return false;
-      charges_to_float_kernel<<<ceil_div(c.nChar, 256), 256, 0, c.stream>>>(c.nChar, c.ct->d_posOrig, c.ct->d_chrOrig,
-                                                                           ox, oy, oz, c.ct->d_chgF);
-      c.launches += 1;
-    }
+    double ox, oy, oz;
+    if (!charges_f32(c, &ox, &oy, &oz)) return false;
     rhs_direct_f32_kernel<<<ceil_div(c.n, 256), 256, 0, c.stream>>>(
         c.n, c.nChar, c.d_vtx, c.d_nrm, c.d_area, c.ct->d_chgF, ox, oy, oz,
         c.rhsFac != 0.0 ? c.rhsFac : kFourPiI / c.prm.eps1, rhs);
