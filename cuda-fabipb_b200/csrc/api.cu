@@ -96,6 +96,8 @@ Context::~Context() {
   free_adjoint(*this);
   arena.release();
   if (sideStream) cudaStreamDestroy(sideStream);
+  if (farStream) cudaStreamDestroy(farStream);
+  if (evFar) cudaEventDestroy(evFar);
   if (evFork) cudaEventDestroy(evFork);
   if (evJoin) cudaEventDestroy(evJoin);
   if (ownStream && stream) cudaStreamDestroy(stream);
@@ -167,6 +169,9 @@ bool op_apply(Context &c, int part, double alpha, const double *sgm, double beta
   return true;
 }
 
+#ifndef FB_FAR_PRIORITY
+#define FB_FAR_PRIORITY 1
+#endif
 // y = alpha*(D - K)x + beta*y, D = diag(s1*A, s2*A) (MtVmain); adjoint: (D - K^T)
 bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y, bool adjoint, bool fp64) {
   double s1 = (1.0 + c.epsilon) / 2.0 * alpha;
@@ -176,7 +181,19 @@ bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y
   FB_CUDA(cudaStreamWaitEvent(c.sideStream, c.evFork, 0));
   if (!launch_near(c, x, -alpha, c.d_nearOut, adjoint, fp64, c.sideStream, false)) return false;
   FB_CUDA(cudaEventRecord(c.evJoin, c.sideStream));
+#if FB_FAR_PRIORITY
+  // the far passes on the high-priority stream (the launch helpers use c.stream)
+  FB_CUDA(cudaStreamWaitEvent(c.farStream, c.evFork, 0));
+  cudaStream_t user = c.stream;
+  c.stream = c.farStream;
+  const bool farOk = launch_far_upward(c, x, adjoint, nullptr, fp64);
+  c.stream = user;
+  if (!farOk) return false;
+  FB_CUDA(cudaEventRecord(c.evFar, c.farStream));
+  FB_CUDA(cudaStreamWaitEvent(c.stream, c.evFar, 0));
+#else
   if (!launch_far_upward(c, x, adjoint, nullptr, fp64)) return false;
+#endif
   FB_CUDA(cudaStreamWaitEvent(c.stream, c.evJoin, 0));
   if (!launch_l2p(c, -alpha, beta, y, x, s1, s2, adjoint, c.d_nearOut, fp64)) return false;
   return true;
@@ -219,9 +236,13 @@ int create_context(const fabipb_b200_params *p, int n, const double *vtx, const 
     ok = false;
   }
   c->ownStream = ok;
+  int prLeast = 0, prGreatest = 0;
+  if (ok) cudaDeviceGetStreamPriorityRange(&prLeast, &prGreatest);
   if (ok && (cudaStreamCreateWithFlags(&c->sideStream, cudaStreamNonBlocking) != cudaSuccess ||
+             cudaStreamCreateWithPriority(&c->farStream, cudaStreamNonBlocking, prGreatest) != cudaSuccess ||
              cudaEventCreateWithFlags(&c->evFork, cudaEventDisableTiming) != cudaSuccess ||
-             cudaEventCreateWithFlags(&c->evJoin, cudaEventDisableTiming) != cudaSuccess)) {
+             cudaEventCreateWithFlags(&c->evJoin, cudaEventDisableTiming) != cudaSuccess ||
+             cudaEventCreateWithFlags(&c->evFar, cudaEventDisableTiming) != cudaSuccess)) {
     set_error("stream/event creation failed");
     ok = false;
   }

@@ -80,7 +80,10 @@ struct Context {
   double *d_refR = nullptr, *d_refD = nullptr, *d_refZ = nullptr;   // iterative refinement (first use)
   // the matvec runs the near field on a second stream beside the far passes
   cudaStream_t sideStream = nullptr;
-  cudaEvent_t evFork = nullptr, evJoin = nullptr;
+  // the far passes on a high-priority stream, so that their (short, latency-
+  // bound) blocks are dispatched ahead of the near field's as SMs free up
+  cudaStream_t farStream = nullptr;
+  cudaEvent_t evFork = nullptr, evJoin = nullptr, evFar = nullptr;
   double *d_nearOut = nullptr;             // 2N: the near-field term of the current matvec
 
   // ---- charges, RHS, energy -------------------------------------------

@@ -650,7 +650,6 @@ static bool setup_near_targets(Context &c);
 
 bool setup_near(Context &c) {
   const PanelTree &pt = c.pt;
-  const int n = c.n;
   cudaStream_t s = c.stream;
   if (c.prm.quad_order != 1) {
     set_error("the device near field implements the one-point panel rule (-q=1); got -q=%d",
