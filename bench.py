@@ -9,7 +9,9 @@ flat triangles (octahedral geodesic, frequency 160, radius 25 A perturbed by
 l=2..6 harmonics), Taylor order p=4, MAC ratio 0.7, octree depth 5 (mean
 leaf 46 panels), eps 2/80, kappa 0.1257, synthetic seeded inputs.
 --case star2097152 runs the same measurement on the 2,097,152-panel star
-(frequency 512, radius 50 A, depth 7: mean leaf 31 panels, 100,000 charges).
+(frequency 512, radius 50 A, depth 7: mean leaf 31 panels, 100,000 charges),
+--case star8388608 on the 8,388,608-panel star (frequency 1024, radius 100 A,
+depth 8, 2,000,000 charges; with --solve-reps 1 --no-adjoint for a short run).
 
 Reported:
   value      matvec/s with x, y resident in HBM (device time, CUDA events on
@@ -55,10 +57,13 @@ CASES = {
     # the north-star size: 2,097,152 triangles (octahedral freq 512, radius 50 A), 100,000 charges
     "star2097152": ("star", dict(freq=512, radius=50.0, n_charges=100000, seed=7),
                     dict(order=4, depth=7, sep_ratio=0.7, eps1=2.0, eps2=80.0, tol=1e-6, restart=10)),
+    # the scale-stress size: 8,388,608 triangles (freq 1024, radius 100 A), 2,000,000 charges
+    "star8388608": ("star", dict(freq=1024, radius=100.0, n_charges=2000000, seed=11),
+                    dict(order=4, depth=8, sep_ratio=0.7, eps1=2.0, eps2=80.0, tol=1e-6, restart=10)),
     "sphere20480": ("sphere", dict(nsub=5, radius=20.0, n_charges=500, seed=0),
                     dict(order=3, depth=3, sep_ratio=0.8, eps1=1.0, eps2=80.0, tol=1e-4, restart=10)),
 }
-PANELS = {"star204800": 204800, "star2097152": 2097152, "sphere20480": 20480}
+PANELS = {"star204800": 204800, "star2097152": 2097152, "star8388608": 8388608, "sphere20480": 20480}
 METRIC = "matvec/s"
 FLOP_PER_PAIR = 60.0   # algorithmic count per near panel pair (KER4 + apply)
 
@@ -184,6 +189,7 @@ class ClockSampler:
                         reasons.add(nm)
         load = [v for v in sm if smax and v > 0.3 * smax] or sm
         return {"sm_mhz": float(np.median(load)) if load else None, "sm_max_mhz": smax,
+                "sm_mhz_p10": float(np.percentile(sm, 10)) if sm else None,
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
@@ -280,7 +286,7 @@ def pass_report(surf, info, x_ptr, flush, reps, prec_is_mixed, sm_mhz, n_sm):
     return out
 
 
-def solve_report(pan, ch, opts, device, st, reps=3):
+def solve_report(pan, ch, opts, device, st, reps=3, adjoint=True):
     """Full solves of the same case in both precisions: RHS (direct, or the
     charge-tree treecode above 2e11 panel-charge pairs as the reference), block-LU
     preconditioner, device GMRES from x0 = b (as the reference CLI), energy.
@@ -291,6 +297,7 @@ def solve_report(pan, ch, opts, device, st, reps=3):
     from fabipb_b200 import lib
     out = {}
     runs = {"mixed": [], "fp64": []}
+    mem_peak = {"mixed": 0.0, "fp64": 0.0}   # device memory in use after the solver set-up, GiB
     kcal = 2.0 * np.pi * 332.0716
     # each precision runs 1 + reps times: the first pays the one-time loading
     # of the kernels it is the first to use and is not reported; every time
@@ -311,6 +318,9 @@ def solve_report(pan, ch, opts, device, st, reps=3):
         b = s.rhs(use_tree=use_tree)
         s.precond_setup(2)
         ev[1].record(st)
+        torch.cuda.synchronize()
+        free, total = torch.cuda.mem_get_info()
+        mem_peak[tag] = max(mem_peak[tag], (total - free) / 2**30)
         x, it, res, info = s.solve(b, b.copy(), restart=opts["restart"], maxit=100, tol=opts["tol"])
         ev[2].record(st)
         e = s.energy_raw(x) * kcal
@@ -330,6 +340,10 @@ def solve_report(pan, ch, opts, device, st, reps=3):
         out[tag] = {"gmres_s": ev[1].elapsed_time(ev[2]) / 1000.0, "setup_s": ev[0].elapsed_time(ev[1]) / 1000.0,
                     "energy_s": ev[2].elapsed_time(ev[3]) / 1000.0, "wall_s": wall, "iterations": it,
                     "residual": res, "info": info, "energy_kcal_mol": e, "refined": refined}
+        if not adjoint:
+            s.close()
+            runs[tag].append(out.pop(tag))
+            continue
         # gradients of the (direct) energy: forward = RHS + GMRES + energy,
         # backward = adjoint GMRES + dE/dq, dE/dx of every charge
         ag = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
@@ -352,13 +366,16 @@ def solve_report(pan, ch, opts, device, st, reps=3):
         r = dict(rs[-1])
         for k in ("gmres_s", "setup_s", "energy_s", "wall_s"):
             r[k] = med([q[k] for q in rs])
+        r["wall_s_runs"] = [q["wall_s"] for q in rs]
         r["refined"] = dict(rs[-1]["refined"], gmres_s=med([q["refined"]["gmres_s"] for q in rs]))
-        a = dict(rs[-1]["adjoint"])
-        a["forward_s"] = med([q["adjoint"]["forward_s"] for q in rs])
-        a["backward_s"] = med([q["adjoint"]["backward_s"] for q in rs])
-        a["backward_over_forward"] = a["backward_s"] / a["forward_s"]
-        r["adjoint"] = a
+        if adjoint:
+            a = dict(rs[-1]["adjoint"])
+            a["forward_s"] = med([q["adjoint"]["forward_s"] for q in rs])
+            a["backward_s"] = med([q["adjoint"]["backward_s"] for q in rs])
+            a["backward_over_forward"] = a["backward_s"] / a["forward_s"]
+            r["adjoint"] = a
         r["runs"] = len(rs)
+        r["device_mem_gib"] = mem_peak[tag]
         out[tag] = r
     m, f = out["mixed"], out["fp64"]
     out["energy_rel_err_mixed_vs_fp64"] = abs(m["energy_kcal_mol"] - f["energy_kcal_mol"]) / abs(f["energy_kcal_mol"])
@@ -379,6 +396,9 @@ def run_ours(args):
     opts = CASES[name][2]
     base = case_base(name)
     pan, ch = meshio.load_case(base)
+    # the reference's CUDA backend first, in its own process, while this
+    # process holds no device memory yet
+    ref_gpu = ref_gpu_rate(base, opts) if (args.ref_gpu and rank == 0) else None
     prec = lib.MIXED if args.precision == "mixed" else lib.FP64
     prm = lib.params(order=opts["order"], depth=opts["depth"], sep_ratio=opts["sep_ratio"], eps1=opts["eps1"],
                      eps2=opts["eps2"], precision=prec, device=local)
@@ -472,9 +492,17 @@ def run_ours(args):
             m = re.search(r"dram_bytes_per_launch \| (\d+)", fp.read())
         traffic = int(m.group(1)) if m else None
     passes = pass_report(surf, info, x.data_ptr(), flush, args.steps, prec == lib.MIXED, sm_mhz, n_sm)
-    solve = None if args.no_solve else solve_report(pan, ch, opts, local, stream)
+    mem_ctx = None
+    if not args.no_solve:   # the matvec context is not needed any more: free it before the solves
+        free, total = torch.cuda.mem_get_info()
+        mem_ctx = (total - free) / 2**30
+        surf.close()
+    solve = None
+    if not args.no_solve:
+        with ClockSampler(local) as clk2:   # the clocks during the solves too
+            solve = solve_report(pan, ch, opts, local, stream, reps=args.solve_reps, adjoint=not args.no_adjoint)
+        solve["clocks"] = clk2.summary()
     cpu = None
-    ref_gpu = ref_gpu_rate(base, opts) if args.ref_gpu else None
     if not args.no_cpu_baseline:
         v, kind, cores, sample = cpu_reference_rate(base, opts, args.cpu_reps, 1, budget=30.0)
         cpu = {"value": v, "unit": "matvec/s", "cores": cores, "kind": kind, "sample": sample}
@@ -503,6 +531,7 @@ def run_ours(args):
         "setup_s": info["setup_seconds"],
         "passes": passes,
         "solve": solve,
+        "device_mem_gib_matvec_context": mem_ctx,
     }
     if pg:
         pg.destroy_process_group()
@@ -524,6 +553,8 @@ def main():
     ap.add_argument("--ref-gpu", action="store_true",
                     help="also time the reference's own CUDA backend (oracle/_ref/ref_harness_gpu, -g=1)")
     ap.add_argument("--no-solve", action="store_true", help="skip the mixed/FP64 solve report")
+    ap.add_argument("--solve-reps", type=int, default=3, help="reported runs per precision (after one warm-up run)")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the forward/backward gradient timing")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

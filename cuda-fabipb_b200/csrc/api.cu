@@ -90,6 +90,28 @@ bool init_quad_tables() {
   return true;
 }
 
+// once per device (the current one): the default memory pool keeps freed memory
+bool pool_keep_memory() {
+  static std::mutex mu;
+  static bool done[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return true;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done[dev]) return true;
+  cudaMemPool_t pool = nullptr;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) {
+    set_error("no default memory pool on device %d", dev);
+    return false;
+  }
+  uint64_t keep = UINT64_MAX;
+  if (cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+    set_error("memory pool set-up failed on device %d", dev);
+    return false;
+  }
+  done[dev] = true;
+  return true;
+}
+
 Context::~Context() {
   free_charges(*this);
   free_precond(*this);

@@ -58,16 +58,25 @@ struct StageTimer {
     }                                \
   } while (0)
 
-// Plain device allocation owned by a context; freed in reverse order.
+// Device allocations owned by a context (or a set-up step), freed together
+// in reverse order.  They come from the device's default memory pool, which
+// is told once per device to keep freed memory (release threshold: no limit):
+// contexts made and dropped in turn, and the set-up steps' temporaries, reuse
+// memory that is already mapped instead of mapping it anew each time.
+// Allocation is complete when alloc returns (usable from any stream);
+// release waits for the device first, as cudaFree does.
+bool pool_keep_memory();
 struct DevArena {
   std::vector<void *> ptrs;
   size_t bytes = 0;
   bool alloc(void **p, size_t n) {
     *p = nullptr;
     if (n == 0) n = 16;
-    cudaError_t e = cudaMalloc(p, n);
+    if (!pool_keep_memory()) return false;
+    cudaError_t e = cudaMallocAsync(p, n, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) {
-      set_error("cudaMalloc of %.3f MiB failed: %s", n / 1048576.0, cudaGetErrorString(e));
+      set_error("device allocation of %.3f MiB failed: %s", n / 1048576.0, cudaGetErrorString(e));
       *p = nullptr;
       return false;
     }
@@ -92,7 +101,10 @@ struct DevArena {
     return true;
   }
   void release() {
-    for (size_t i = ptrs.size(); i-- > 0;) cudaFree(ptrs[i]);
+    if (ptrs.empty()) return;
+    cudaDeviceSynchronize();   // nothing in flight still uses the memory
+    for (size_t i = ptrs.size(); i-- > 0;) cudaFreeAsync(ptrs[i], 0);
+    cudaStreamSynchronize(0);
     ptrs.clear();
     bytes = 0;
   }

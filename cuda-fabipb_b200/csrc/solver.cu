@@ -68,8 +68,7 @@ __global__ void pc_assemble_kernel(int nBlocks, const int *__restrict__ bStart, 
                                    const long long *__restrict__ bOff, const double *__restrict__ vtx,
                                    const double *__restrict__ nrm, const double *__restrict__ area, int q,
                                    double kappa, double eps, double s1, double s2, TO *A) {
-  const int b = blockIdx.y;
-  if (b >= nBlocks) return;
+  for (int b = blockIdx.y; b < nBlocks; b += gridDim.y) {   // (the grid's y extent is capped at 65535)
   const int hm = bSize[b], st = bStart[b], M = 2 * hm;
   const long long pairs = (long long)hm * hm;
   TO *Ab = A + bOff[b];
@@ -98,21 +97,23 @@ __global__ void pc_assemble_kernel(int nBlocks, const int *__restrict__ bStart, 
     Ab[(size_t)(i + hm) * M + j] = (TO)(-K[3]);
     Ab[(size_t)(i + hm) * M + j + hm] = (TO)(-K[2] + d1);
   }
+  }
 }
 
 // the listed blocks of I := identity, and their column index the identity
 __global__ void identity_kernel(int nList, const int *__restrict__ list, const int *__restrict__ bStart,
                                 const int *__restrict__ bSize, const long long *__restrict__ bOff, double *I,
                                 int *colSrc) {
-  if ((int)blockIdx.y >= nList) return;
-  const int b = list[blockIdx.y];
-  const int M = 2 * bSize[b];
-  const long long e = (long long)M * M;
-  double *Ib = I + bOff[b];
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < e; p += (long long)gridDim.x * blockDim.x)
-    Ib[p] = ((p / M) == (p % M)) ? 1.0 : 0.0;
-  if (blockIdx.x == 0)
-    for (int c = threadIdx.x; c < M; c += blockDim.x) colSrc[2LL * bStart[b] + c] = c;
+  for (int li = blockIdx.y; li < nList; li += gridDim.y) {   // (y extent capped at 65535)
+    const int b = list[li];
+    const int M = 2 * bSize[b];
+    const long long e = (long long)M * M;
+    double *Ib = I + bOff[b];
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < e; p += (long long)gridDim.x * blockDim.x)
+      Ib[p] = ((p / M) == (p % M)) ? 1.0 : 0.0;
+    if (blockIdx.x == 0)
+      for (int c = threadIdx.x; c < M; c += blockDim.x) colSrc[2LL * bStart[b] + c] = c;
+  }
 }
 
 // In-place inversion of the preconditioner blocks by blocked Gauss-Jordan
@@ -548,7 +549,7 @@ static bool factor_cusolver(Context &c, PrecondDev &p, const std::vector<int> &b
   int *d_list = nullptr;
   FB_CUDA(cudaMalloc((void **)&d_list, blocks.size() * sizeof(int)));
   FB_CUDA(cudaMemcpyAsync(d_list, blocks.data(), blocks.size() * sizeof(int), cudaMemcpyHostToDevice, s));
-  dim3 grid(64, (unsigned)blocks.size());
+  dim3 grid(64, (unsigned)std::min<size_t>(blocks.size(), 65535));
   identity_kernel<<<grid, 256, 0, s>>>((int)blocks.size(), d_list, p.d_start, p.d_size, p.d_off, p.d_inv, p.d_colSrc);
   cudaEvent_t evA = nullptr;
   bool ok = cudaEventCreateWithFlags(&evA, cudaEventDisableTiming) == cudaSuccess;
@@ -804,7 +805,7 @@ bool precond_setup(Context &c, int mode) {
   // FP64 contexts invert in FP64; mixed contexts assemble and invert in FP32
   // (the preconditioner only steers GMRES; its inverse is stored in FP32)
   const double s1 = (1.0 + c.epsilon) / 2.0, s2 = (1.0 + 1.0 / c.epsilon) / 2.0;
-  dim3 grid(64, p.nBlocks);
+  dim3 grid(64, std::min(p.nBlocks, 65535));
   bool ok;
   if (c.mixed) {
     FB_CHECK(p.maxM <= gj_max_rows<float>(), "preconditioner block of %d rows above the FP32 limit %d", p.maxM,
