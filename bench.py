@@ -54,7 +54,7 @@ CASES = {
     # name: (generator, kwargs, solver options)
     "star204800": ("star", dict(freq=160, radius=25.0, n_charges=20000, seed=1),
                    dict(order=4, depth=5, sep_ratio=0.7, eps1=2.0, eps2=80.0, tol=1e-5, restart=10)),
-    # the north-star size: 2,097,152 triangles (octahedral freq 512, radius 50 A), 100,000 charges
+    # the 2.1M-panel size: 2,097,152 triangles (octahedral freq 512, radius 50 A), 100,000 charges
     "star2097152": ("star", dict(freq=512, radius=50.0, n_charges=100000, seed=7),
                     dict(order=4, depth=7, sep_ratio=0.7, eps1=2.0, eps2=80.0, tol=1e-6, restart=10)),
     # the scale-stress size: 8,388,608 triangles (freq 1024, radius 100 A), 2,000,000 charges
@@ -94,9 +94,6 @@ def cpu_reference_rate(base, opts, reps, warmup=1, budget=60.0):
     exceed `budget` seconds (at least one is always timed)."""
     from oracle import oracle as O
     cores = os.cpu_count() or 1
-    if not O.ref_available() and os.path.isdir("/root/reference/src"):
-        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=False,
-                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
     if O.ref_available():
         pre = os.path.join(tempfile.gettempdir(), "fabipb_ref_time")
         out = O.run_ref_harness("time", base, pre, ref_opts(opts), threads=cores, reps=reps,
