@@ -190,16 +190,35 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_setup(args):
+def dist_setup(args, backend="nccl"):
+    """One process per GPU under torchrun (RANK/WORLD_SIZE/LOCAL_RANK from the
+    environment); the path does not shard, so the ranks are independent
+    replicas and the process group only carries barriers and the timing
+    reduction."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     pg = None
     if world > 1:
         import torch.distributed as dist
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
+        dist.init_process_group(backend, init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
         pg = dist
     return rank, world, local, pg
+
+
+def replica_times(pg, total_s, e2e_s, device="cuda"):
+    """The slowest replica's device and end-to-end times (max over ranks)."""
+    if not pg:
+        return total_s, e2e_s
+    import torch
+    t = torch.tensor([total_s, e2e_s], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t[0]), float(t[1])
+
+
+def replica_value(world, steps, total_s):
+    """Whole-job matvec/s: every replica did `steps` matvecs in at most total_s."""
+    return world * steps / total_s
 
 
 def run_reference(args):
@@ -457,11 +476,9 @@ def run_ours(args):
     total_s = sum(step_ms) / 1000.0
     e2e_rate = args.steps / e2e_s
     if pg:
-        t = torch.tensor([total_s, e2e_s], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_s, e2e_s = float(t[0]), float(t[1])
+        total_s, e2e_s = replica_times(pg, total_s, e2e_s)
         e2e_rate = args.steps / e2e_s
-    value = world * args.steps / total_s
+    value = replica_value(world, args.steps, total_s)
     if rank != 0:
         if pg:
             pg.destroy_process_group()
