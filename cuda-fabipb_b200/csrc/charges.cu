@@ -300,9 +300,12 @@ rhs_direct_f32_kernel(int n, int m, const double *__restrict__ vtx, const double
 // ---------------------------------------------------------------------------
 // charge-tree walks: mode 0 = RHS (Coulomb), mode 1 = energy (G0 - Gk)
 // ---------------------------------------------------------------------------
-template <int PM>
-__device__ void walk_point(int mode, const double *qp, const double *nx, double theta, int height, int depth,
-                           double kappa, double eps, int NM, const double *__restrict__ ctr,
+// T = float (the energy walks of a mixed context): derivative tables, their
+// contraction and the direct leaf terms in FP32 (the point-to-cluster
+// offsets in FP64, then rounded); the per-panel sums stay FP64.
+template <int PM, typename T = double>
+__device__ void walk_point(int mode, const double *qp, const double *nxd, double theta, int height, int depth,
+                           double kappad, double epsd, int NM, const double *__restrict__ ctr,
                            const double *__restrict__ rad, const int *__restrict__ level,
                            const int *__restrict__ kidStart, const int *__restrict__ kidCount,
                            const int *__restrict__ itemStart, const int *__restrict__ itemCount,
@@ -312,20 +315,23 @@ __device__ void walk_point(int mode, const double *qp, const double *nx, double 
   int stack[8 * 20 + 4];
   int sp = 0;
   stack[sp++] = 0;
-  double d0[ND], dk[ND];
+  T d0[ND], dk[ND];
+  const T nx[3] = {(T)nxd[0], (T)nxd[1], (T)nxd[2]};
+  const T kappa = (T)kappad, eps = (T)epsd;
   while (sp > 0) {
     const int c = stack[--sp];
     double r[3] = {qp[0] - ctr[3 * c], qp[1] - ctr[3 * c + 1], qp[2] - ctr[3 * c + 2]};
     const double dist = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
     if (rad[c] < theta * dist && level[c] >= height) {
       const int ord = order[c], nmo = nmom(ord);
-      derivs<PM>(ord + 1, r, kappa, mode == 0, d0, dk);
+      const T rt[3] = {(T)r[0], (T)r[1], (T)r[2]};
+      derivs_inplace<PM, T>(ord + 1, rt, kappa, mode == 0, d0, dk, 1);
       const double *mc = mom + (size_t)c * NM;
-      double y0 = 0.0, y1 = 0.0;
+      T y0 = (T)0, y1 = (T)0;
       for (int i = 0; i < nmo; i++) {
         const char4 a = c_mi[i];
         const int e1 = IDX(a.x + 1, a.y, a.z), e2 = IDX(a.x, a.y + 1, a.z), e3 = IDX(a.x, a.y, a.z + 1);
-        const double sm = c_sgn3[i] * mc[i];
+        const T sm = (T)(c_sgn3[i] * mc[i]);
         if (mode == 0) {
           y0 += sm * d0[i];
           y1 += sm * (nx[0] * d0[e1] + nx[1] * d0[e2] + nx[2] * d0[e3]);
@@ -334,40 +340,42 @@ __device__ void walk_point(int mode, const double *qp, const double *nx, double 
           y1 += sm * eps * (nx[0] * dk[e1] + nx[1] * dk[e2] + nx[2] * dk[e3]);
         } else {
           y0 += sm * (d0[i] - dk[i]);
-          const double dn0 = nx[0] * d0[e1] + nx[1] * d0[e2] + nx[2] * d0[e3];
-          const double dnk = nx[0] * dk[e1] + nx[1] * dk[e2] + nx[2] * dk[e3];
+          const T dn0 = nx[0] * d0[e1] + nx[1] * d0[e2] + nx[2] * d0[e3];
+          const T dnk = nx[0] * dk[e1] + nx[1] * dk[e2] + nx[2] * dk[e3];
           y1 += sm * (eps * dnk - dn0);
         }
       }
       if (mode == 0) {
-        y[0] += y0 / kFourPiI;
-        y[1] += y1 / kFourPiI;
+        y[0] += (double)y0 / kFourPiI;
+        y[1] += (double)y1 / kFourPiI;
       } else {
-        y[0] += y0;
-        y[1] += y1;
+        y[0] += (double)y0;
+        y[1] += (double)y1;
       }
       continue;
     }
     if (level[c] == depth) {
       const int s0 = itemStart[c], s1 = s0 + itemCount[c];
       for (int j = s0; j < s1; j++) {
-        const double x[3] = {qp[0] - pos[3 * (size_t)j], qp[1] - pos[3 * (size_t)j + 1], qp[2] - pos[3 * (size_t)j + 2]};
-        const double r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
-        const double ip = nx[0] * x[0] + nx[1] * x[1] + nx[2] * x[2];
+        const T x[3] = {(T)(qp[0] - pos[3 * (size_t)j]), (T)(qp[1] - pos[3 * (size_t)j + 1]),
+                        (T)(qp[2] - pos[3 * (size_t)j + 2])};
+        const T r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+        const T ip = nx[0] * x[0] + nx[1] * x[1] + nx[2] * x[2];
+        const T q = (T)chr[j];
         if (mode == 0) {
-          const double ri = 1.0 / sqrt(r2), r3i = ri / r2;
-          y[0] += chr[j] * ri;
-          y[1] += chr[j] * (-ip * r3i);
+          const T ri = (T)1 / sqrt(r2), r3i = ri / r2;
+          y[0] += (double)(q * ri);
+          y[1] += (double)(q * (-ip * r3i));
         } else {
-          const double rn = sqrt(r2), G0 = kFourPiI / rn, ek = exp(-kappa * rn);
-          const double Gk = ek * G0, coef = (kappa * rn + 1.0) * ek;
-          const double dG0dn = -ip * G0 / r2, dGkdn = coef * dG0dn;
+          const T rn = sqrt(r2), G0 = (T)kFourPiI / rn, ek = exp(-kappa * rn);
+          const T Gk = ek * G0, coef = (kappa * rn + (T)1) * ek;
+          const T dG0dn = -ip * G0 / r2, dGkdn = coef * dG0dn;
           if (mode == 2) {
-            y[0] += chr[j] * Gk;
-            y[1] += chr[j] * eps * dGkdn;
+            y[0] += (double)(q * Gk);
+            y[1] += (double)(q * eps * dGkdn);
           } else {
-            y[0] += chr[j] * (G0 - Gk);
-            y[1] += chr[j] * (eps * dGkdn - dG0dn);
+            y[0] += (double)(q * (G0 - Gk));
+            y[1] += (double)(q * (eps * dGkdn - dG0dn));
           }
         }
       }
@@ -378,7 +386,7 @@ __device__ void walk_point(int mode, const double *qp, const double *nx, double 
   }
 }
 
-template <int PM>
+template <int PM, typename T>
 __global__ void tree_walk_kernel(int mode, int n, int q, const double *__restrict__ vtx, const double *__restrict__ nrm,
                                  const double *__restrict__ area, double theta, int height, int depth, double kappa,
                                  double eps, int NM, const double *__restrict__ ctr, const double *__restrict__ rad,
@@ -405,7 +413,7 @@ __global__ void tree_walk_kernel(int mode, int n, int q, const double *__restric
       for (int jx = 0; jx < q; jx++) {
         double qp[3], y[2] = {0.0, 0.0};
         for (int k = 0; k < 3; k++) qp[k] = v0[k] + t[ix] * (ax2[k] + t[jx] * ax0[k]);
-        walk_point<PM>(mode, qp, nx, theta, height, depth, kappa, eps, NM, ctr, rad, level, kidStart, kidCount,
+        walk_point<PM, T>(mode, qp, nx, theta, height, depth, kappa, eps, NM, ctr, rad, level, kidStart, kidCount,
                        itemStart, itemCount, order, mom, pos, chr, y);
         o0 += y[0] * t[ix] * w[ix] * w[jx];
         o1 += y[1] * t[ix] * w[ix] * w[jx];
@@ -445,7 +453,9 @@ static void launch_walk(Context &c, int mode, const double *sgm, double *rhs, do
   ChargeTreeDev &d = *c.ct;
   // the screened-only walk uses the RHS acceptance ratio (treecode.c:731)
   const double theta = (mode == 1) ? c.prm.energy_theta : c.prm.rhs_theta;
-  tree_walk_kernel<PM><<<ceil_div(c.n, 256), 256, 0, c.stream>>>(
+  // the energy walks of a mixed context in FP32 (the RHS walk stays FP64)
+  auto kern = (c.mixed && mode != 0) ? tree_walk_kernel<PM, float> : tree_walk_kernel<PM, double>;
+  kern<<<ceil_div(c.n, 256), 256, 0, c.stream>>>(
       mode, c.n, c.prm.quad_order, c.d_vtx, c.d_nrm, c.d_area, theta, d.height, d.depth, c.prm.kappa, c.epsilon,
       c.NM, d.d_ctr, d.d_rad, d.d_level, d.d_kidStart, d.d_kidCount, d.d_itemStart, d.d_itemCount, d.d_order,
       d.d_mom, d.d_pos, d.d_chr, c.rhsFac != 0.0 ? c.rhsFac : kFourPiI / c.prm.eps1, sgm, rhs, partial);

@@ -102,24 +102,24 @@ __device__ __forceinline__ double conv_entry(const double *t, int g) {
 // down lets one table per kernel be updated in place.  Entry e of the result
 // lives at d0[e*stride] (stride 1 for a private array, the block width for a
 // shared-memory column).
-template <int PM>
-__device__ void derivs_inplace(int order, const double *x, double kappa, bool coulombOnly, double *d0, double *dk,
-                               int stride) {
-  double G0[PM + 2], Gk[PM + 2];
-  const double r = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+// T = float: the same recursion in FP32 (the mixed energy walk).
+template <int PM, typename T = double>
+__device__ void derivs_inplace(int order, const T *x, T kappa, bool coulombOnly, T *d0, T *dk, int stride) {
+  T G0[PM + 2], Gk[PM + 2];
+  const T r = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
   if (coulombOnly) {
-    const double r2 = -1.0 / (r * r);
-    G0[0] = kFourPiI / r;
-    for (int k = 0; k < order; k++) G0[k + 1] = (2 * k + 1) * r2 * G0[k];
+    const T r2 = (T)-1 / (r * r);
+    G0[0] = (T)kFourPiI / r;
+    for (int k = 0; k < order; k++) G0[k + 1] = (T)(2 * k + 1) * r2 * G0[k];
   } else {
-    const double rexp = exp(-kappa * r), r1 = 1.0 / r, rr2 = r1 * r1, nr2 = -rr2, k2 = kappa * kappa;
-    G0[0] = r1 * kFourPiI;
+    const T rexp = exp(-kappa * r), r1 = (T)1 / r, rr2 = r1 * r1, nr2 = -rr2, k2 = kappa * kappa;
+    G0[0] = r1 * (T)kFourPiI;
     Gk[0] = rexp * G0[0];
     G0[1] = nr2 * G0[0];
     Gk[1] = -Gk[0] * (rr2 + kappa * r1);
     for (int k = 1; k < order; k++) {
-      G0[k + 1] = (2 * k + 1) * nr2 * G0[k];
-      Gk[k + 1] = rr2 * (k2 * Gk[k - 1] - (2 * k + 1) * Gk[k]);
+      G0[k + 1] = (T)(2 * k + 1) * nr2 * G0[k];
+      Gk[k + 1] = rr2 * (k2 * Gk[k - 1] - (T)(2 * k + 1) * Gk[k]);
     }
   }
   d0[0] = G0[order];
@@ -130,7 +130,7 @@ __device__ void derivs_inplace(int order, const double *x, double kappa, bool co
     for (int e = ne - 1; e >= 1; e--) {
       const char4 m = c_mi[e];
       int a, b = -1;
-      double xa, fb = 0.0;
+      T xa, fb = (T)0;
       if (m.x >= 1) {
         a = IDX(m.x - 1, m.y, m.z); xa = x[0];
         if (m.x >= 2) { b = IDX(m.x - 2, m.y, m.z); fb = m.x - 1; }
@@ -141,11 +141,11 @@ __device__ void derivs_inplace(int order, const double *x, double kappa, bool co
         a = IDX(0, 0, m.z - 1); xa = x[2];
         if (m.z >= 2) { b = IDX(0, 0, m.z - 2); fb = m.z - 1; }
       }
-      double v0 = d0[a * stride] * xa;
+      T v0 = d0[a * stride] * xa;
       if (b >= 0) v0 += d0[b * stride] * fb;
       d0[e * stride] = v0;
       if (!coulombOnly) {
-        double vk = dk[a * stride] * xa;
+        T vk = dk[a * stride] * xa;
         if (b >= 0) vk += dk[b * stride] * fb;
         dk[e * stride] = vk;
       }
