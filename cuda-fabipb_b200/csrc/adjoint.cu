@@ -70,59 +70,72 @@ __global__ void energy_weights_kernel(int n, int m, int q, const double *__restr
 }
 
 // Mixed contexts, one-point rule: the same weights with FP32 pair terms
-// (positions relative to the root box centre, MUFU rsqrt/exp2), summed in
-// FP32 over 64 charges at a time and in FP64 above.
+// (positions relative to the root box centre, MUFU rsqrt/exp2) in packed
+// f32x2 arithmetic, two charges per step (charge pairs staged as
+// rhs_direct_f2_kernel stages them), summed in FP32 over 64 charges at a time
+// and in FP64 above.  The pair sums leave out the common factor 1/(4 pi)
+// (and the sign of dG0/dn), which the FP64 epilogue applies:
+//   dpdn: sum q (1 - e)/r,   pot: -sum q (eps (kappa r + 1) e - 1) (n.d)/r^3.
 __global__ void __launch_bounds__(256)
-energy_weights_f32_kernel(int n, int m, const double *__restrict__ vtx, const double *__restrict__ nrm,
-                          const double *__restrict__ area, const float4 *__restrict__ chg, double ox, double oy,
-                          double oz, float kappa, float kexp, float eps, double *out) {
+energy_weights_f2_kernel(int n, int m, const double *__restrict__ vtx, const double *__restrict__ nrm,
+                         const double *__restrict__ area, const float4 *__restrict__ chg, double ox, double oy,
+                         double oz, float kappa, float kexp, float eps, double *out) {
   __shared__ float4 sc[kRhsTileF];
   const int X = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = X < n;
   const int Xs = valid ? X : 0;
   const double *v0 = vtx + 9 * (size_t)Xs;
   const double t = c_tLeg[1][0], wt = c_wLeg[1][0];
-  float px, py, pz;
+  float2 px, py, pz;
   {
     double p[3];
     for (int k = 0; k < 3; k++) p[k] = v0[k] + t * ((v0[3 + k] - v0[k]) + t * (v0[6 + k] - v0[3 + k]));
-    px = (float)(p[0] - ox);
-    py = (float)(p[1] - oy);
-    pz = (float)(p[2] - oz);
+    px = f2((float)(p[0] - ox));
+    py = f2((float)(p[1] - oy));
+    pz = f2((float)(p[2] - oz));
   }
-  const float nx = (float)nrm[3 * (size_t)Xs], ny = (float)nrm[3 * (size_t)Xs + 1], nz = (float)nrm[3 * (size_t)Xs + 2];
-  const float f4 = (float)kFourPiI;
+  const float2 nx = f2((float)nrm[3 * (size_t)Xs]), ny = f2((float)nrm[3 * (size_t)Xs + 1]),
+               nz = f2((float)nrm[3 * (size_t)Xs + 2]);
+  const float2 ek = f2(eps * kappa), ev = f2(eps), m1 = f2(-1.f), ke = f2(kexp);
   double s0 = 0.0, s1 = 0.0;
   for (int base = 0; base < m; base += kRhsTileF) {
-    const int cnt = min(kRhsTileF, m - base);
-    for (int j = threadIdx.x; j < cnt; j += blockDim.x) sc[j] = chg[base + j];
+    const int cnt = min(kRhsTileF, m - base), cnt2 = (cnt + 1) / 2;
+    stage_charge_pairs(chg, base, cnt, sc);
     __syncthreads();
-    for (int j0 = 0; j0 < cnt; j0 += 64) {
-      const int j1 = min(cnt, j0 + 64);
-      float a0 = 0.f, a1 = 0.f;
+    for (int j0 = 0; j0 < cnt2; j0 += 32) {
+      const int j1 = min(cnt2, j0 + 32);
+      float2 a0 = f2(0.f), a1 = f2(0.f);
 #pragma unroll 4
       for (int j = j0; j < j1; j++) {
-        const float4 cj = sc[j];
-        const float dx = px - cj.x, dy = py - cj.y, dz = pz - cj.z;
-        const float r2 = dx * dx + dy * dy + dz * dz;
-        const float ri = rsqrt_t(r2);
-        const float r = r2 * ri;
-        const float e = expneg_t(kexp, r);
-        const float G0 = f4 * ri;
-        const float ip = nx * dx + ny * dy + nz * dz;
-        const float dG0dn = -ip * G0 * ri * ri;
-        a0 += cj.w * (G0 - e * G0);                                 // G0 - Gk
-        a1 += cj.w * ((eps * (kappa * r + 1.f) * e - 1.f) * dG0dn);  // eps dGk/dn - dG0/dn
+        const float4 A = sc[2 * j], B = sc[2 * j + 1];
+        const float2 dx = __fadd2_rn(px, make_float2(A.x, A.y));
+        const float2 dy = __fadd2_rn(py, make_float2(A.z, A.w));
+        const float2 dz = __fadd2_rn(pz, make_float2(B.x, B.y));
+        const float2 q = make_float2(B.z, B.w);
+        const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+        float2 ri;
+        ri.x = rsqrt_t(r2.x);
+        ri.y = rsqrt_t(r2.y);
+        const float2 r = __fmul2_rn(r2, ri);
+        const float2 ea = __fmul2_rn(ke, r);
+        float2 e;
+        e.x = expneg_t(1.f, ea.x);
+        e.y = expneg_t(1.f, ea.y);
+        a0 = __ffma2_rn(q, __ffma2_rn(make_float2(-e.x, -e.y), ri, ri), a0);   // q (G0 - Gk) 4 pi
+        const float2 ip = __ffma2_rn(nz, dz, __ffma2_rn(ny, dy, __fmul2_rn(nx, dx)));
+        const float2 w = __fmul2_rn(ip, __fmul2_rn(__fmul2_rn(ri, ri), ri));
+        const float2 u = __ffma2_rn(__ffma2_rn(ek, r, ev), e, m1);           // eps c - 1
+        a1 = __ffma2_rn(q, __fmul2_rn(u, w), a1);
       }
-      s0 += (double)a0;
-      s1 += (double)a1;
+      s0 += (double)a0.x + (double)a0.y;
+      s1 += (double)a1.x + (double)a1.y;
     }
     __syncthreads();
   }
   if (!valid) return;
-  const double W = 2.0 * area[Xs] * t * wt * wt;
-  out[X] = s1 * W;       // pot slot
-  out[n + X] = s0 * W;   // dpdn slot
+  const double W = 2.0 * area[Xs] * t * wt * wt * kFourPiI;
+  out[X] = -s1 * W;     // pot slot
+  out[n + X] = s0 * W;  // dpdn slot
 }
 
 // Per surface quadrature point: position, normal and the four weights
@@ -149,84 +162,147 @@ __global__ void grad_records_kernel(int n, int q, const double *__restrict__ vtx
 }
 
 // The records of a mixed context, one-point rule, in FP32, with the weights
-// pre-combined for charge_grad_f32_kernel (f = 1/(4 pi), a_i as above):
-//   rp = (x_w - o, f a1),  rn = (n, f a2 eps),
-//   rx = (f a1 + a3, a4 - f a2, f a1 kappa, f a2 eps kappa^2).
-__global__ void grad_records_f32_kernel(int n, const double *__restrict__ vtx, const double *__restrict__ nrm,
-                                        const double *__restrict__ area, const double *__restrict__ sgm,
-                                        const double *__restrict__ lam, double fac, double ox, double oy, double oz,
-                                        double kappa, double eps, float4 *rp, float4 *rn, float4 *rx) {
-  const int X = blockIdx.x * blockDim.x + threadIdx.x;
-  if (X >= n) return;
-  const double *v0 = vtx + 9 * (size_t)X;
+// pre-combined for charge_grad_f2_kernel (f = 1/(4 pi), a_i as above) and two
+// records interleaved per 96-byte pair, so that every packed f32x2 operand of
+// the pair loop is one half of a float4 of the pair:
+//   q[0] = (x0 x1 y0 y1)   position x_w - o
+//   q[1] = (z0 z1 a0 a1)   a  = -f a1
+//   q[2] = (nx0 nx1 ny0 ny1)
+//   q[3] = (nz0 nz1 b0 b1) b  = f a2 eps
+//   q[4] = (u0 u1 v0 v1)   u  = f a1 + a3,  v = a4 - f a2
+//   q[5] = (s0 s1 w0 w1)   s  = f a1 kappa, w = f a2 eps kappa^2.
+// An odd record count pads the last pair with a copy of the last position
+// and zero weights and normal, which adds exactly zero.
+__global__ void grad_records_f2_kernel(int n, const double *__restrict__ vtx, const double *__restrict__ nrm,
+                                       const double *__restrict__ area, const double *__restrict__ sgm,
+                                       const double *__restrict__ lam, double fac, double ox, double oy, double oz,
+                                       double kappa, double eps, float4 *rq) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= (n + 1) / 2) return;
   const double t = c_tLeg[1][0], w = c_wLeg[1][0];
-  double p[3];
-  for (int k = 0; k < 3; k++) p[k] = v0[k] + t * ((v0[3 + k] - v0[k]) + t * (v0[6 + k] - v0[3 + k]));
-  const double a = 2.0 * area[X] * t * w * w;
-  const double f1 = kFourPiI * a * sgm[n + X], f2 = kFourPiI * a * sgm[X];
-  const double a3 = a * fac * lam[X], a4 = a * fac * lam[n + X];
-  rp[X] = make_float4((float)(p[0] - ox), (float)(p[1] - oy), (float)(p[2] - oz), (float)f1);
-  rn[X] = make_float4((float)nrm[3 * (size_t)X], (float)nrm[3 * (size_t)X + 1], (float)nrm[3 * (size_t)X + 2],
-                      (float)(f2 * eps));
-  rx[X] = make_float4((float)(f1 + a3), (float)(a4 - f2), (float)(f1 * kappa), (float)(f2 * eps * kappa * kappa));
+  float v[2][12];
+  for (int h = 0; h < 2; h++) {
+    const int X = min(2 * j + h, n - 1);
+    const double live = 2 * j + h < n ? 1.0 : 0.0;
+    const double *v0 = vtx + 9 * (size_t)X;
+    double p[3];
+    for (int k = 0; k < 3; k++) p[k] = v0[k] + t * ((v0[3 + k] - v0[k]) + t * (v0[6 + k] - v0[3 + k]));
+    const double a = live * 2.0 * area[X] * t * w * w;
+    const double f1 = kFourPiI * a * sgm[n + X], f2v = kFourPiI * a * sgm[X];
+    const double a3 = a * fac * lam[X], a4 = a * fac * lam[n + X];
+    float *o = v[h];
+    o[0] = (float)(p[0] - ox);
+    o[1] = (float)(p[1] - oy);
+    o[2] = (float)(p[2] - oz);
+    o[3] = (float)(-f1);
+    for (int k = 0; k < 3; k++) o[4 + k] = (float)(live * nrm[3 * (size_t)X + k]);
+    o[7] = (float)(f2v * eps);
+    o[8] = (float)(f1 + a3);
+    o[9] = (float)(a4 - f2v);
+    o[10] = (float)(f1 * kappa);
+    o[11] = (float)(f2v * eps * kappa * kappa);
+  }
+  float4 *q = rq + 6 * (size_t)j;
+  for (int s = 0; s < 6; s++) q[s] = make_float4(v[0][2 * s], v[1][2 * s], v[0][2 * s + 1], v[1][2 * s + 1]);
 }
 
-constexpr int kGradCharges = 128;   // charges per block
+constexpr int kGradCharges = 128;   // threads per block (FP64 kernel: charges per block)
 constexpr int kGradTile = 128;      // records staged per step
+constexpr int kGradCpt = 2;         // charges per thread in charge_grad_f2_kernel
 
-// charge_grad_kernel with FP32 pair terms (records and charges relative to
-// the root box centre), FP32 sums over 64 records at a time, FP64 above.  With
-// A = f a1 (1 - e) + a3 and B = f a2 (eps c - 1) + a4 (e = exp(-kappa r),
-// c = (kappa r + 1) e), the record's term and its gradient in x are
+// One record pair against one charge (c = the negated charge position), in
+// packed f32x2 arithmetic.  With A = f a1 (1 - e) + a3 and B = f a2 (eps c - 1)
+// + a4 (e = exp(-kappa r), c = (kappa r + 1) e), the record's term and its
+// gradient in x = x_w - r_k are
 //   phi  = A/r - (n.x) B/r^3,
 //   grad = x [f a1 kappa e/r^2 - A/r^3 + (n.x)/r^3 (3B/r^2 + f a2 eps kappa^2 e)] - n B/r^3.
+__device__ __forceinline__ void grad_pair2(const float4 Q0, const float4 Q1, const float4 Q2, const float4 Q3,
+                                           const float4 Q4, const float4 Q5, float2 cx, float2 cy, float2 cz,
+                                           float kappa, float kexp, float2 &phi, float2 &gx, float2 &gy,
+                                           float2 &gz) {
+  const float2 x = __fadd2_rn(make_float2(Q0.x, Q0.y), cx);
+  const float2 y = __fadd2_rn(make_float2(Q0.z, Q0.w), cy);
+  const float2 z = __fadd2_rn(make_float2(Q1.x, Q1.y), cz);
+  const float2 r2 = __ffma2_rn(z, z, __ffma2_rn(y, y, __fmul2_rn(x, x)));
+  float2 ri;
+  ri.x = rsqrt_t(r2.x);
+  ri.y = rsqrt_t(r2.y);
+  const float2 r = __fmul2_rn(r2, ri), ri2 = __fmul2_rn(ri, ri), ri3 = __fmul2_rn(ri2, ri);
+  const float2 ea = __fmul2_rn(f2(kexp), r);
+  float2 e;
+  e.x = expneg_t(1.f, ea.x);
+  e.y = expneg_t(1.f, ea.y);
+  const float2 c = __fmul2_rn(__ffma2_rn(f2(kappa), r, f2(1.f)), e);
+  const float2 nx = make_float2(Q2.x, Q2.y), ny = make_float2(Q2.z, Q2.w), nz = make_float2(Q3.x, Q3.y);
+  const float2 ip = __ffma2_rn(nz, z, __ffma2_rn(ny, y, __fmul2_rn(nx, x)));
+  const float2 A = __ffma2_rn(make_float2(Q1.z, Q1.w), e, make_float2(Q4.x, Q4.y));
+  const float2 B = __ffma2_rn(make_float2(Q3.z, Q3.w), c, make_float2(Q4.z, Q4.w));
+  const float2 t = __fmul2_rn(ip, ri3);
+  phi = __ffma2_rn(A, ri, phi);
+  phi = __ffma2_rn(make_float2(-t.x, -t.y), B, phi);
+  const float2 u = __ffma2_rn(__fmul2_rn(f2(3.f), ri2), B, __fmul2_rn(make_float2(Q5.z, Q5.w), e));
+  const float2 sxv = __ffma2_rn(__fmul2_rn(make_float2(Q5.x, Q5.y), e), ri2,
+                                __ffma2_rn(make_float2(-A.x, -A.y), ri3, __fmul2_rn(t, u)));
+  const float2 snv = __fmul2_rn(make_float2(-ri3.x, -ri3.y), B);
+  gx = __ffma2_rn(sxv, x, __ffma2_rn(snv, nx, gx));
+  gy = __ffma2_rn(sxv, y, __ffma2_rn(snv, ny, gy));
+  gz = __ffma2_rn(sxv, z, __ffma2_rn(snv, nz, gz));
+}
+
+// charge_grad_kernel with FP32 pair terms (records and charges relative to
+// the root box centre) in packed f32x2 arithmetic: every thread takes two
+// charges (k and k + 128) and every step one record pair, so each staged
+// float4 feeds four pair terms.  FP32 sums over 64 records at a time, FP64
+// above; part[chunk][k] as charge_grad_kernel.
 __global__ void __launch_bounds__(kGradCharges)
-charge_grad_f32_kernel(long long nRec, int m, long long chunkLen, const float4 *__restrict__ rp,
-                       const float4 *__restrict__ rn, const float4 *__restrict__ rx, const float4 *__restrict__ chg,
-                       float kappa, float kexp, double4 *part) {
-  __shared__ float4 sp[kGradTile], sn[kGradTile], sx_[kGradTile];
-  const int k = blockIdx.x * kGradCharges + threadIdx.x;
-  const bool valid = k < m;
-  const float4 ck = valid ? chg[k] : make_float4(0.f, 0.f, 0.f, 0.f);
-  const long long r0 = (long long)blockIdx.y * chunkLen, r1 = min(nRec, r0 + chunkLen);
-  double phi = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;   // gradient with respect to x = x_w - r_k
-  for (long long b = r0; b < r1; b += kGradTile) {
-    const int cnt = (int)min((long long)kGradTile, r1 - b);
-    for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
-      sp[j] = rp[b + j];
-      sn[j] = rn[b + j];
-      sx_[j] = rx[b + j];
-    }
+charge_grad_f2_kernel(long long nPairs, int m, long long chunkPairs, const float4 *__restrict__ rq,
+                      const float4 *__restrict__ chg, float kappa, float kexp, double4 *part) {
+  constexpr int kPairs = kGradTile / 2;
+  __shared__ float4 sq[6 * kPairs];
+  float2 cx[kGradCpt], cy[kGradCpt], cz[kGradCpt];
+  double phi[kGradCpt], gx[kGradCpt], gy[kGradCpt], gz[kGradCpt];
+#pragma unroll
+  for (int h = 0; h < kGradCpt; h++) {
+    const int k = blockIdx.x * (kGradCharges * kGradCpt) + h * kGradCharges + threadIdx.x;
+    const float4 ck = k < m ? chg[k] : make_float4(0.f, 0.f, 0.f, 0.f);
+    cx[h] = f2(-ck.x);
+    cy[h] = f2(-ck.y);
+    cz[h] = f2(-ck.z);
+    phi[h] = gx[h] = gy[h] = gz[h] = 0.0;
+  }
+  const long long p0 = (long long)blockIdx.y * chunkPairs, p1 = min(nPairs, p0 + chunkPairs);
+  for (long long b = p0; b < p1; b += kPairs) {
+    const int cnt = (int)min((long long)kPairs, p1 - b);
+    for (int i = threadIdx.x; i < 6 * cnt; i += blockDim.x) sq[i] = rq[6 * b + i];
     __syncthreads();
-    for (int j0 = 0; j0 < cnt; j0 += 64) {
-      const int j1 = min(cnt, j0 + 64);
-      float fphi = 0.f, fx = 0.f, fy = 0.f, fz = 0.f;
+    for (int j0 = 0; j0 < cnt; j0 += 32) {
+      const int j1 = min(cnt, j0 + 32);
+      float2 fphi[kGradCpt], fx[kGradCpt], fy[kGradCpt], fz[kGradCpt];
+#pragma unroll
+      for (int h = 0; h < kGradCpt; h++) fphi[h] = fx[h] = fy[h] = fz[h] = f2(0.f);
 #pragma unroll 2
       for (int j = j0; j < j1; j++) {
-        const float4 P = sp[j], N = sn[j], R = sx_[j];
-        const float x = P.x - ck.x, y = P.y - ck.y, z = P.z - ck.z;
-        const float r2 = x * x + y * y + z * z;
-        const float ri = rsqrt_t(r2), r = r2 * ri, ri2 = ri * ri, ri3 = ri2 * ri;
-        const float e = expneg_t(kexp, r), c = (kappa * r + 1.f) * e;
-        const float ip = N.x * x + N.y * y + N.z * z;
-        const float A = R.x - P.w * e;          // f a1 (1 - e) + a3
-        const float B = N.w * c + R.y;          // f a2 eps c + a4 - f a2
-        const float t = ip * ri3;
-        fphi += A * ri - t * B;
-        const float sxv = R.z * e * ri2 - A * ri3 + t * (3.f * ri2 * B + R.w * e);
-        const float snv = -ri3 * B;
-        fx += sxv * x + snv * N.x;
-        fy += sxv * y + snv * N.y;
-        fz += sxv * z + snv * N.z;
+        const float4 Q0 = sq[6 * j], Q1 = sq[6 * j + 1], Q2 = sq[6 * j + 2], Q3 = sq[6 * j + 3],
+                     Q4 = sq[6 * j + 4], Q5 = sq[6 * j + 5];
+#pragma unroll
+        for (int h = 0; h < kGradCpt; h++)
+          grad_pair2(Q0, Q1, Q2, Q3, Q4, Q5, cx[h], cy[h], cz[h], kappa, kexp, fphi[h], fx[h], fy[h], fz[h]);
       }
-      phi += (double)fphi;
-      gx += (double)fx;
-      gy += (double)fy;
-      gz += (double)fz;
+#pragma unroll
+      for (int h = 0; h < kGradCpt; h++) {
+        phi[h] += (double)fphi[h].x + (double)fphi[h].y;
+        gx[h] += (double)fx[h].x + (double)fx[h].y;
+        gy[h] += (double)fy[h].x + (double)fy[h].y;
+        gz[h] += (double)fz[h].x + (double)fz[h].y;
+      }
     }
     __syncthreads();
   }
-  if (valid) part[(size_t)blockIdx.y * m + k] = make_double4(phi, -gx, -gy, -gz);   // d/dr_k = -d/dx
+#pragma unroll
+  for (int h = 0; h < kGradCpt; h++) {
+    const int k = blockIdx.x * (kGradCharges * kGradCpt) + h * kGradCharges + threadIdx.x;
+    if (k < m) part[(size_t)blockIdx.y * m + k] = make_double4(phi[h], -gx[h], -gy[h], -gz[h]);   // d/dr_k = -d/dx
+  }
 }
 
 // phi_k and grad_{r_k} phi_k over one chunk of the records, for a tile of
@@ -307,7 +383,8 @@ struct AdjointDev {
   double *d_b = nullptr, *d_sigma = nullptr, *d_e = nullptr, *d_lam = nullptr, *d_out = nullptr;
   double4 *d_rp = nullptr, *d_rn = nullptr, *d_part = nullptr;
   double2 *d_rw = nullptr;
-  long long recCap = 0, partCap = 0;
+  float4 *d_rq = nullptr;
+  long long recCap = 0, rqCap = 0, partCap = 0;
   int outCap = 0;
   bool forwardDone = false;
   double energy = 0.0;
@@ -339,7 +416,7 @@ bool launch_energy_weights(Context &c, double *e) {
   if (c.mixed && c.prm.quad_order == 1) {
     double ox, oy, oz;
     if (!charges_f32(c, &ox, &oy, &oz)) return false;
-    energy_weights_f32_kernel<<<ceil_div(c.n, 256), 256, 0, c.stream>>>(
+    energy_weights_f2_kernel<<<ceil_div(c.n, 256), 256, 0, c.stream>>>(
         c.n, c.nChar, c.d_vtx, c.d_nrm, c.d_area, c.ct->d_chgF, ox, oy, oz, (float)c.prm.kappa,
         (float)(-c.prm.kappa * 1.4426950408889634), (float)c.epsilon, e);
     c.launches += 1;
@@ -386,38 +463,44 @@ bool adjoint_backward(Context &c, double scale, int restart, int maxit, double t
   // records, then per-charge sums over chunks of records
   const int q = c.prm.quad_order, m = c.nChar;
   const long long nRec = (long long)c.n * q * q;
-  if (a.recCap < nRec) {
+  const double fac = c.rhsFac != 0.0 ? c.rhsFac : kFourPiI / c.prm.eps1;
+  const bool f32 = c.mixed && q == 1;   // FP32 pair terms, records interleaved in pairs
+  const long long nPairs = (nRec + 1) / 2;
+  if (f32) {
+    if (a.rqCap < 6 * nPairs) {
+      if (!a.arena.alloc_n(&a.d_rq, (size_t)(6 * nPairs))) return false;
+      a.rqCap = 6 * nPairs;
+    }
+  } else if (a.recCap < nRec) {
     if (!a.arena.alloc_n(&a.d_rp, (size_t)nRec) || !a.arena.alloc_n(&a.d_rn, (size_t)nRec) ||
         !a.arena.alloc_n(&a.d_rw, (size_t)nRec))
       return false;
     a.recCap = nRec;
   }
-  const double fac = c.rhsFac != 0.0 ? c.rhsFac : kFourPiI / c.prm.eps1;
-  const bool f32 = c.mixed && q == 1;   // FP32 pair terms (records of 48 bytes in the FP64 arrays' space)
-  double ox = 0.0, oy = 0.0, oz = 0.0;
   if (f32) {
+    double ox, oy, oz;
     if (!charges_f32(c, &ox, &oy, &oz)) return false;
-    grad_records_f32_kernel<<<ceil_div(nRec, 256), 256, 0, c.stream>>>(
-        c.n, c.d_vtx, c.d_nrm, c.d_area, a.d_sigma, a.d_lam, fac, ox, oy, oz, c.prm.kappa, c.epsilon,
-        (float4 *)a.d_rp, (float4 *)a.d_rn, (float4 *)a.d_rw);
+    grad_records_f2_kernel<<<ceil_div(nPairs, 256), 256, 0, c.stream>>>(
+        c.n, c.d_vtx, c.d_nrm, c.d_area, a.d_sigma, a.d_lam, fac, ox, oy, oz, c.prm.kappa, c.epsilon, a.d_rq);
   } else {
     grad_records_kernel<<<ceil_div(nRec, 256), 256, 0, c.stream>>>(c.n, q, c.d_vtx, c.d_nrm, c.d_area, a.d_sigma,
                                                                    a.d_lam, fac, a.d_rp, a.d_rn, a.d_rw);
   }
   // enough blocks to fill the GPU: chunks of the records times tiles of charges
-  const int tiles = (int)ceil_div(m, kGradCharges);
+  const int perBlock = f32 ? kGradCharges * kGradCpt : kGradCharges;
+  const int tiles = (int)ceil_div(m, perBlock);
   const long long want = (2368LL + tiles - 1) / tiles, most = (nRec + 4095) / 4096;
   const int nChunks = (int)std::max(1LL, std::min(want, most));
-  const long long chunkLen = (nRec + nChunks - 1) / nChunks;
+  const long long chunkPairs = (nPairs + nChunks - 1) / nChunks, chunkLen = (nRec + nChunks - 1) / nChunks;
   if (a.partCap < (long long)nChunks * m) {
     if (!a.arena.alloc_n(&a.d_part, (size_t)nChunks * m)) return false;
     a.partCap = (long long)nChunks * m;
   }
   dim3 grid(tiles, nChunks);
   if (f32)
-    charge_grad_f32_kernel<<<grid, kGradCharges, 0, c.stream>>>(
-        nRec, m, chunkLen, (const float4 *)a.d_rp, (const float4 *)a.d_rn, (const float4 *)a.d_rw, c.ct->d_chgF,
-        (float)c.prm.kappa, (float)(-c.prm.kappa * 1.4426950408889634), a.d_part);
+    charge_grad_f2_kernel<<<grid, kGradCharges, 0, c.stream>>>(nPairs, m, chunkPairs, a.d_rq, c.ct->d_chgF,
+                                                               (float)c.prm.kappa,
+                                                               (float)(-c.prm.kappa * 1.4426950408889634), a.d_part);
   else
     charge_grad_kernel<<<grid, kGradCharges, 0, c.stream>>>(nRec, m, chunkLen, a.d_rp, a.d_rn, a.d_rw,
                                                            c.ct->d_posOrig, c.prm.kappa, c.epsilon, a.d_part);

@@ -237,7 +237,8 @@ __global__ void rhs_direct_kernel(int n, int m, int q, const double *__restrict_
 // panel's quadrature point and the charges are taken relative to the root
 // box centre (differences in FP64, then rounded), the pair terms use the
 // MUFU reciprocal square root, and every 64 charges are summed in FP32 and
-// added to the panel's FP64 totals.
+// added to the panel's FP64 totals.  The pair terms run in packed f32x2
+// arithmetic (sm_100 FFMA2/FMUL2/FADD2), two charges per step.
 constexpr int kRhsTileF = 1024;
 
 __global__ void charges_to_float_kernel(int m, const double *__restrict__ pos, const double *__restrict__ chr,
@@ -248,45 +249,64 @@ __global__ void charges_to_float_kernel(int m, const double *__restrict__ pos, c
                        (float)(pos[3 * (size_t)j + 2] - oz), (float)chr[j]);
 }
 
+// Stages charges [base, base + cnt) as (cnt + 1) / 2 interleaved pairs with
+// negated positions, s[2p] = (-x0 -x1 -y0 -y1), s[2p + 1] = (-z0 -z1 q0 q1),
+// so every packed operand is one half of a staged float4; an odd count pads
+// the last pair with a copy of the last position carrying zero charge.
+__device__ __forceinline__ void stage_charge_pairs(const float4 *__restrict__ chg, int base, int cnt, float4 *s) {
+  for (int p = threadIdx.x; 2 * p < cnt; p += blockDim.x) {
+    const float4 a = chg[base + 2 * p];
+    const float4 b = 2 * p + 1 < cnt ? chg[base + 2 * p + 1] : make_float4(a.x, a.y, a.z, 0.f);
+    s[2 * p] = make_float4(-a.x, -b.x, -a.y, -b.y);
+    s[2 * p + 1] = make_float4(-a.z, -b.z, a.w, b.w);
+  }
+}
+
 __global__ void __launch_bounds__(256)
-rhs_direct_f32_kernel(int n, int m, const double *__restrict__ vtx, const double *__restrict__ nrm,
-                      const double *__restrict__ area, const float4 *__restrict__ chg, double ox, double oy,
-                      double oz, double fac, double *rhs) {
+rhs_direct_f2_kernel(int n, int m, const double *__restrict__ vtx, const double *__restrict__ nrm,
+                     const double *__restrict__ area, const float4 *__restrict__ chg, double ox, double oy,
+                     double oz, double fac, double *rhs) {
   __shared__ float4 sc[kRhsTileF];
   const int X = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = X < n;
   const int Xs = valid ? X : 0;
   const double *v0 = vtx + 9 * (size_t)Xs;
   const double t = c_tLeg[1][0], wt = c_wLeg[1][0];
-  float px, py, pz;
+  float2 px, py, pz;
   {
     double p[3];
     for (int k = 0; k < 3; k++) p[k] = v0[k] + t * ((v0[3 + k] - v0[k]) + t * (v0[6 + k] - v0[3 + k]));
-    px = (float)(p[0] - ox);
-    py = (float)(p[1] - oy);
-    pz = (float)(p[2] - oz);
+    px = f2((float)(p[0] - ox));
+    py = f2((float)(p[1] - oy));
+    pz = f2((float)(p[2] - oz));
   }
-  const float nx = (float)nrm[3 * (size_t)Xs], ny = (float)nrm[3 * (size_t)Xs + 1], nz = (float)nrm[3 * (size_t)Xs + 2];
+  const float2 nx = f2((float)nrm[3 * (size_t)Xs]), ny = f2((float)nrm[3 * (size_t)Xs + 1]),
+               nz = f2((float)nrm[3 * (size_t)Xs + 2]);
   double s0 = 0.0, s1 = 0.0;
   for (int base = 0; base < m; base += kRhsTileF) {
-    const int cnt = min(kRhsTileF, m - base);
-    for (int j = threadIdx.x; j < cnt; j += blockDim.x) sc[j] = chg[base + j];
+    const int cnt = min(kRhsTileF, m - base), cnt2 = (cnt + 1) / 2;
+    stage_charge_pairs(chg, base, cnt, sc);
     __syncthreads();
-    for (int j0 = 0; j0 < cnt; j0 += 64) {   // FP32 sums of 64 charges at a time
-      const int j1 = min(cnt, j0 + 64);
-      float a0 = 0.f, a1 = 0.f;
-#pragma unroll 8
+    for (int j0 = 0; j0 < cnt2; j0 += 32) {   // FP32 sums of 64 charges at a time
+      const int j1 = min(cnt2, j0 + 32);
+      float2 a0 = f2(0.f), a1 = f2(0.f);
+#pragma unroll 4
       for (int j = j0; j < j1; j++) {
-        const float4 cj = sc[j];
-        const float dx = px - cj.x, dy = py - cj.y, dz = pz - cj.z;
-        const float r2 = dx * dx + dy * dy + dz * dz;
-        const float ri = rsqrt_t(r2);
-        const float qr3 = cj.w * (ri * ri * ri);
-        a0 += cj.w * ri;
-        a1 += qr3 * (nx * dx + ny * dy + nz * dz);
+        const float4 A = sc[2 * j], B = sc[2 * j + 1];
+        const float2 dx = __fadd2_rn(px, make_float2(A.x, A.y));
+        const float2 dy = __fadd2_rn(py, make_float2(A.z, A.w));
+        const float2 dz = __fadd2_rn(pz, make_float2(B.x, B.y));
+        const float2 q = make_float2(B.z, B.w);
+        const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+        float2 ri;
+        ri.x = rsqrt_t(r2.x);
+        ri.y = rsqrt_t(r2.y);
+        const float2 qr3 = __fmul2_rn(q, __fmul2_rn(__fmul2_rn(ri, ri), ri));
+        a0 = __ffma2_rn(q, ri, a0);
+        a1 = __ffma2_rn(qr3, __ffma2_rn(nz, dz, __ffma2_rn(ny, dy, __fmul2_rn(nx, dx))), a1);
       }
-      s0 += (double)a0;
-      s1 -= (double)a1;
+      s0 += (double)a0.x + (double)a0.y;
+      s1 -= (double)a1.x + (double)a1.y;
     }
     __syncthreads();
   }
@@ -497,7 +517,7 @@ bool launch_rhs(Context &c, int useTree, double *rhs) {
   if (!useTree && c.mixed && c.prm.quad_order == 1) {
     double ox, oy, oz;
     if (!charges_f32(c, &ox, &oy, &oz)) return false;
-    rhs_direct_f32_kernel<<<ceil_div(c.n, 256), 256, 0, c.stream>>>(
+    rhs_direct_f2_kernel<<<ceil_div(c.n, 256), 256, 0, c.stream>>>(
         c.n, c.nChar, c.d_vtx, c.d_nrm, c.d_area, c.ct->d_chgF, ox, oy, oz,
         c.rhsFac != 0.0 ? c.rhsFac : kFourPiI / c.prm.eps1, rhs);
     FB_CUDA(cudaGetLastError());
