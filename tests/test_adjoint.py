@@ -159,3 +159,38 @@ def test_autograd_function(case_dir, golden_meta):
     dq, dx, _, _, _ = s.backward(1.0, **TIGHT)
     assert np.allclose(q.grad.numpy(), dq * KCAL, rtol=1e-10, atol=0)
     assert np.allclose(pos.grad.numpy(), dx * KCAL, rtol=1e-10, atol=1e-14)
+
+
+def test_mixed_direct_sums_odd_counts(case_dir, golden_meta):
+    """Odd panel and charge counts, a last charge tile of odd length: the
+    packed FP32 kernels of a mixed context pad the last panel record pair and
+    the last charge pair with zero weights.  Mixed direct RHS, energy weights
+    and charge gradients against the FP64 context's, on the 320-panel sphere
+    with its last panel removed (319 panels) and 1,101 seeded charges (one
+    full tile of 1,024 and 77 more)."""
+    name = "sphere320"
+    pan, _ = meshio.load_case(os.path.join(case_dir, name))
+    keep = pan.n - 1
+    pan = meshio.PanelSet(vtx=pan.vtx[:keep], normal=pan.normal[:keep], area=pan.area[:keep],
+                          face_index=pan.face_index[:keep])
+    rng = np.random.default_rng(11)
+    m = 1101
+    d = rng.normal(size=(m, 3))
+    pos = d / np.linalg.norm(d, axis=1)[:, None] * (15.0 * rng.random(m)[:, None] ** (1 / 3))
+    ch = meshio.ChargeSet(pos=pos, q=rng.normal(0.0, 0.5, m), radius=np.full(m, 1.5))
+    out = {}
+    for prec, tol in ((lib.FP64, 1e-10), (lib.MIXED, 1e-6)):
+        s = lib.Surface(pan, lib.params(precision=prec, **case_params(golden_meta[name]["opts"])), ch)
+        rhs, ew = s.rhs(), s.energy_weights()
+        e, it, res, info = s.forward(restart=10, maxit=400, tol=tol)
+        assert info == 0
+        dq, dx, it2, res2, info2 = s.backward(1.0, restart=10, maxit=400, tol=tol)
+        assert info2 == 0
+        out[prec] = (rhs, ew, dq, dx)
+        s.close()
+    a, b = out[lib.FP64], out[lib.MIXED]
+    assert np.all(np.isfinite(np.concatenate([np.ravel(v) for v in b])))
+    assert rel_l2(b[0], a[0]) < 2e-6   # FP32 pair terms, FP64 sums above 64 charges
+    assert rel_l2(b[1], a[1]) < 2e-6
+    assert rel_l2(b[2], a[2]) < 1e-3   # plus the mixed solves' tolerance
+    assert rel_l2(b[3], a[3]) < 1e-3
