@@ -170,8 +170,10 @@ bool setup_geometry(Context &c, const double *vtx, const double *nrm, const doub
   return true;
 }
 
-// pot = beta*pot + alpha*K_part*sgm
+// pot = beta*pot + alpha*K_part*sgm (a direct context has no far part: its
+// near field is every panel pair)
 bool op_apply(Context &c, int part, double alpha, const double *sgm, double beta, double *pot, bool adjoint) {
+  if (c.dense) part &= ~FABIPB_B200_FAR;
   if (part & FABIPB_B200_FAR) {
     if (!launch_far_upward(c, sgm, adjoint)) return false;
     if (!launch_l2p(c, alpha, beta, pot, nullptr, 0.0, 0.0, adjoint)) return false;
@@ -191,6 +193,18 @@ bool op_apply(Context &c, int part, double alpha, const double *sgm, double beta
   return true;
 }
 
+// y = beta*y + s1*A.*x_pot, s2*A.*x_dpdn + add (the direct context's matvec:
+// the diagonal of MtVmain, src/fabipb.c:1257-1265, plus its near term)
+__global__ void direct_combine_kernel(int n, const double *__restrict__ area, const double *__restrict__ x,
+                                      const double *__restrict__ add, double s1, double s2, double beta, double *y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double a = area[i];
+  const double y0 = beta == 0.0 ? 0.0 : beta * y[i], y1 = beta == 0.0 ? 0.0 : beta * y[i + n];
+  y[i] = y0 + s1 * a * x[i] + add[i];
+  y[i + n] = y1 + s2 * a * x[i + n] + add[i + n];
+}
+
 #ifndef FB_FAR_PRIORITY
 #define FB_FAR_PRIORITY 1
 #endif
@@ -198,6 +212,13 @@ bool op_apply(Context &c, int part, double alpha, const double *sgm, double beta
 bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y, bool adjoint, bool fp64) {
   double s1 = (1.0 + c.epsilon) / 2.0 * alpha;
   double s2 = (1.0 + 1.0 / c.epsilon) / 2.0 * alpha;
+  if (c.dense) {   // the direct operator: every panel pair through the near-field kernels
+    if (!launch_near(c, x, -alpha, c.d_nearOut, adjoint, fp64, c.stream, false)) return false;
+    direct_combine_kernel<<<ceil_div(c.n, 256), 256, 0, c.stream>>>(c.n, c.d_area, x, c.d_nearOut, s1, s2, beta, y);
+    c.launches += 1;
+    FB_CUDA(cudaGetLastError());
+    return true;
+  }
   // the near field on the side stream, into d_nearOut, beside the far passes
   FB_CUDA(cudaEventRecord(c.evFork, c.stream));
   FB_CUDA(cudaStreamWaitEvent(c.sideStream, c.evFork, 0));
@@ -360,6 +381,11 @@ const char *fabipb_b200_last_error(void) { return get_error(); }
 int fabipb_b200_create(const fabipb_b200_params *p, int n, const double *vtx, const double *normal,
                        const double *area, void **out) {
   return create_context(p, n, vtx, normal, area, false, out);
+}
+
+int fabipb_b200_create_direct(const fabipb_b200_params *p, int n, const double *vtx, const double *normal,
+                              const double *area, void **out) {
+  return create_context(p, n, vtx, normal, area, true, out);
 }
 
 void fabipb_b200_destroy(void *ctx) {

@@ -9,3 +9,4 @@
 #include "abi.cu"
 #include "adjoint.cu"
 #include "noalloc.cu"
+#include "peak.cu"

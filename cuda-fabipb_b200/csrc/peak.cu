@@ -1,0 +1,75 @@
+// peak.cu -- the FP32 SIMT rate of this device, measured.
+//
+// The near-field P2P and the mixed-precision direct sums are bound by the FP32
+// FMA pipe (not a memory stream, not a tensor-core contraction), so their
+// roofline denominator is the FP32 FMA rate.  It is measured here rather than
+// derived from the clock: every thread runs long chains of independent packed
+// f32x2 FMAs (FFMA2, the instruction the near field issues) on values the
+// compiler cannot fold, timed with CUDA events over a grid of several waves.
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace fb {
+
+constexpr int kPeakChains = 8;     // independent accumulators per thread
+constexpr int kPeakIters = 4096;   // FMA steps per chain
+
+__global__ void __launch_bounds__(256) fp32_peak_kernel(float seed, float *sink) {
+  float2 acc[kPeakChains];
+  const float2 m = make_float2(0.999f + 1e-7f * threadIdx.x, 0.998f);
+  const float2 a = make_float2(seed, -seed);
+#pragma unroll
+  for (int k = 0; k < kPeakChains; k++) acc[k] = make_float2(seed * (k + 1), seed * (k + 2));
+  for (int it = 0; it < kPeakIters; it++) {
+#pragma unroll
+    for (int k = 0; k < kPeakChains; k++) acc[k] = __ffma2_rn(acc[k], m, a);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < kPeakChains; k++) s += acc[k].x + acc[k].y;
+  if (s == 12345.678f) sink[threadIdx.x] = s;   // never true for these inputs; keeps the chains live
+}
+
+// TFLOP/s of the FP32 FMA pipe (2 flop per lane FMA), the best of `reps`
+// event-timed launches after one warm-up launch
+bool measure_fp32_peak(int device, int reps, double *tflops) {
+  FB_CUDA(cudaSetDevice(device));
+  int sms = 0;
+  FB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  float *sink = nullptr;
+  FB_CUDA(cudaMalloc(&sink, 256 * sizeof(float)));
+  cudaStream_t st = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  bool ok = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess;
+  const int blocks = sms * 8 * 4;   // eight resident 256-thread blocks per SM, four waves
+  const double flop = 2.0 * 2.0 * kPeakChains * (double)kPeakIters * 256.0 * blocks;
+  double best = 0.0;
+  for (int r = 0; ok && r <= reps; r++) {
+    ok = cudaEventRecord(e0, st) == cudaSuccess;
+    fp32_peak_kernel<<<blocks, 256, 0, st>>>(1e-3f, sink);
+    ok = ok && cudaGetLastError() == cudaSuccess && cudaEventRecord(e1, st) == cudaSuccess &&
+         cudaEventSynchronize(e1) == cudaSuccess;
+    float ms = 0.f;
+    if (ok && r > 0 && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess && ms > 0.f)
+      best = std::max(best, flop / (ms * 1e-3) / 1e12);
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (st) cudaStreamDestroy(st);
+  cudaFree(sink);
+  FB_CHECK(ok, "FP32 peak measurement failed: %s", cudaGetErrorString(cudaGetLastError()));
+  *tflops = best;
+  return true;
+}
+
+}  // namespace fb
+
+extern "C" int fabipb_b200_fp32_peak(int device, double *tflops) {
+  if (tflops == nullptr) {
+    fb::set_error("fabipb_b200_fp32_peak: null output");
+    return 0;
+  }
+  return fb::measure_fp32_peak(device, 5, tflops) ? 1 : 0;
+}

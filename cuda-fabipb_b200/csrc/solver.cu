@@ -49,12 +49,16 @@ struct PrecondDev {
   int restart = 0;
   double *d_V = nullptr, *d_r = nullptr, *d_av = nullptr, *d_w = nullptr;
   double *d_h = nullptr, *d_part = nullptr, *d_y = nullptr;
+  double *d_H = nullptr, *d_sv = nullptr;   // Hessenberg (+ cs, sn columns) and rotated residual vector
+  void *d_status = nullptr;                 // GmresStatus on the device
+  void *h_status = nullptr;                 // pinned host copy (and two host-read norms)
   int partCap = 0;
 };
 
 void free_precond(Context &c) {
   if (c.pc) {
     c.pc->arena.release();
+    if (c.pc->h_status) cudaFreeHost(c.pc->h_status);
     delete c.pc;
     c.pc = nullptr;
   }
@@ -615,7 +619,7 @@ static bool factor_cusolver(Context &c, PrecondDev &p, const std::vector<int> &b
 #ifndef FB_PC_GJ_MAXM
 #define FB_PC_GJ_MAXM 11000
 #endif
-// CTAs per block for blocks of 385-768 rows (1 or 2; 1600+ rows use 8)
+// CTAs per block for blocks of 385-768 rows (1 or 2; larger blocks use 8)
 #ifndef FB_PC_GJ_MIDCS
 #define FB_PC_GJ_MIDCS 2
 #endif
@@ -624,6 +628,14 @@ template <typename TV, int NB, int CS>
 static bool launch_gj_t(int nList, int maxM, cudaStream_t st, const int *d_list, PrecondDev &p, const long long *d_yOff,
                         TV *inv, TV *d_y, int *d_info) {
   const size_t shm = gj_smem_bytes<TV, NB>(maxM);
+  cudaFuncAttributes fa{};
+  FB_CUDA(cudaFuncGetAttributes(&fa, pc_gj_invert_kernel<TV, NB, CS>));
+  int dev = 0, optin = 0;
+  FB_CUDA(cudaGetDevice(&dev));
+  FB_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  FB_CHECK(shm + fa.sharedSizeBytes <= (size_t)optin,
+           "Gauss-Jordan class NB=%d: %d rows need %zu + %zu bytes of shared memory, above the %d available", NB,
+           maxM, shm, (size_t)fa.sharedSizeBytes, optin);
   FB_CUDA(cudaFuncSetAttribute(pc_gj_invert_kernel<TV, NB, CS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)shm));
   cudaLaunchConfig_t cfg = {};
@@ -665,7 +677,9 @@ static const GjCls *gj_classes(int *count) {
   // FP64 stops at 3200 rows: above it cuSOLVER's factorisation of a single
   // large block (all SMs) beats the kernel's narrow panels (measured on a
   // 2.1M-panel surface: 7.9 s against 9.8 s for the whole inversion)
-  static const GjCls d64[4] = {{384, 16, 1}, {768, 16, FB_PC_GJ_MIDCS}, {1600, 16, 8}, {3200, 8, 8}};
+  // (the NB = 16 FP64 panel of 1536 rows plus the kernel's static shared
+  // memory is the largest that fits in the 227 KiB a block may use)
+  static const GjCls d64[4] = {{384, 16, 1}, {768, 16, FB_PC_GJ_MIDCS}, {1536, 16, 8}, {3200, 8, 8}};
   static const GjCls d32[5] = {{384, 16, 1}, {768, 16, FB_PC_GJ_MIDCS}, {3200, 16, 8}, {6000, 8, 8}, {11000, 4, 8}};
   *count = sizeof(TV) == 8 ? 4 : 5;
   return sizeof(TV) == 8 ? d64 : d32;
@@ -1007,59 +1021,162 @@ bool dot_to_host(Context &c, long long n, const double *x, const double *y, doub
   return true;
 }
 
-static bool nrm2_host(Context &c, long long n, const double *x, double *out) {
-  if (!dot_dev(c, n, x, x, c.pc->d_part + kRedBlocks, true)) return false;
-  FB_CUDA(cudaMemcpyAsync(out, c.pc->d_part + kRedBlocks, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
-  FB_CUDA(cudaStreamSynchronize(c.stream));
-  return true;
+// ---------------------------------------------------------------------------
+// GMRES state on the device.  The Hessenberg matrix, the Givens rotations
+// (cs, sn), the rotated residual vector s and the residual estimate live in
+// device memory; one single-warp kernel per Arnoldi step applies the previous
+// rotations to the new column, forms the next rotation (netlib drotg, the
+// BLAS the reference calls at src/gmres.c:281-293), rotates s and decides
+// whether the cycle ends.  The host reads back only the small GmresStatus
+// record (pinned) after each step, to know whether to queue another one; the
+// triangular solve and the x update of src/gmres.c:364-373 are kernels too.
+// Every product and sum of the rotations is rounded separately (no fused
+// multiply-add), as the reference's BLAS calls compute them.
+// ---------------------------------------------------------------------------
+struct GmresStatus {
+  double resid;   // |s_i| / ||b|| after the last step, or the restart residual
+  double rnorm;   // norm of the preconditioned residual at the cycle start
+  int i;          // columns of the current cycle
+  int iters;      // Arnoldi steps so far
+  int state;      // 0 running, 1 converged, 2 cycle full (i == restart or iters == maxit), 3 zero/NaN residual
+  int pad;
+};
+
+__device__ __forceinline__ void drot_d(double *x, double *y, double cc, double ss) {
+  const double xv = *x, yv = *y;
+  *x = __dadd_rn(__dmul_rn(cc, xv), __dmul_rn(ss, yv));
+  *y = __dsub_rn(__dmul_rn(cc, yv), __dmul_rn(ss, xv));
 }
 
-// drotg of the reference BLAS: r takes the sign of the larger input
-static void drotg_h(double *a, double *b, double *cc, double *ss) {
-  double aa = *a, bb = *b, roe = (fabs(aa) > fabs(bb)) ? aa : bb, scale = fabs(aa) + fabs(bb), r, z;
+__device__ void drotg_d(double *a, double *b, double *cc, double *ss) {
+  const double aa = *a, bb = *b;
+  const double roe = (fabs(aa) > fabs(bb)) ? aa : bb;
+  const double scale = __dadd_rn(fabs(aa), fabs(bb));
+  double r, z;
   if (scale == 0.0) {
     *cc = 1.0; *ss = 0.0; r = 0.0; z = 0.0;
   } else {
-    r = scale * sqrt((aa / scale) * (aa / scale) + (bb / scale) * (bb / scale));
+    const double ua = __ddiv_rn(aa, scale), ub = __ddiv_rn(bb, scale);
+    r = __dmul_rn(scale, __dsqrt_rn(__dadd_rn(__dmul_rn(ua, ua), __dmul_rn(ub, ub))));
     if (roe < 0.0) r = -r;
-    *cc = aa / r;
-    *ss = bb / r;
+    *cc = __ddiv_rn(aa, r);
+    *ss = __ddiv_rn(bb, r);
     z = 1.0;
     if (fabs(aa) > fabs(bb)) z = *ss;
-    if (fabs(bb) >= fabs(aa) && *cc != 0.0) z = 1.0 / (*cc);
+    if (fabs(bb) >= fabs(aa) && *cc != 0.0) z = __ddiv_rn(1.0, *cc);
   }
   *a = r;
   *b = z;
 }
 
-static void rot_h(double *x, double *y, double cc, double ss) {
-  double xv = *x, yv = *y;
-  *x = cc * xv + ss * yv;
-  *y = cc * yv - ss * xv;
+// Cycle start: rnorm = sqrt(sum of the dot partials of r.r); the restart
+// residual test of src/gmres.c:225-232 / :352-356 (strict < tol at the very
+// first test, <= at a restart); s = (rnorm, 0, ...).
+__global__ void gmres_cycle_start_kernel(const double *__restrict__ part, int nPart, double bnrm2, double tol,
+                                         int first, int restrt, double *sv, GmresStatus *st) {
+  __shared__ double red[kRedThreads];
+  double s = 0.0;
+  for (int k = threadIdx.x; k < nPart; k += blockDim.x) s += part[k];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int m = blockDim.x / 2; m > 0; m >>= 1) {
+    if ((int)threadIdx.x < m) red[threadIdx.x] += red[threadIdx.x + m];
+    __syncthreads();
+  }
+  const double rn = sqrt(red[0]);
+  for (int k = threadIdx.x; k < restrt + 2; k += blockDim.x) sv[k] = (k == 0) ? rn : 0.0;
+  if (threadIdx.x == 0) {
+    const double res = rn / bnrm2;
+    st->rnorm = rn;
+    st->resid = res;
+    st->i = 0;
+    if (first ? (res < tol) : (res <= tol)) st->state = 1;
+    else if (!(rn > 0.0) || rn != rn) st->state = 3;
+    else st->state = 0;
+  }
 }
 
-static bool gmres_update_dev(Context &c, int it, std::vector<double> &H, int ldh, const std::vector<double> &sv,
-                             double *x) {
-  PrecondDev &p = *c.pc;
-  std::vector<double> y(sv.begin(), sv.begin() + it);
-  for (int j = it - 1; j >= 0; j--) {  // dtrsv upper, no transpose
+// One Givens step for column i (1-based, as src/gmres.c): H(:, i-1) = h,
+// previous rotations, the new rotation, s rotated, residual estimate.  A step
+// queued after the cycle ended (state != 0) changes nothing.
+__global__ void gmres_givens_kernel(const double *__restrict__ h, double *H, int ldh, int restrt, double *sv,
+                                    int i, int iters, int maxit, double bnrm2, double tol, GmresStatus *st) {
+  if (threadIdx.x != 0 || st->state != 0) return;
+  double *cs = H + (size_t)restrt * ldh, *sn = H + (size_t)(restrt + 1) * ldh;
+  double *hc = H + (size_t)(i - 1) * ldh;
+  for (int k = 0; k <= i; k++) hc[k] = h[k];
+  for (int k = 0; k < i - 1; k++) drot_d(&hc[k], &hc[k + 1], cs[k], sn[k]);
+  double aa = hc[i - 1], bb = hc[i];
+  drotg_d(&aa, &bb, &cs[i - 1], &sn[i - 1]);
+  drot_d(&hc[i - 1], &hc[i], cs[i - 1], sn[i - 1]);
+  drot_d(&sv[i - 1], &sv[i], cs[i - 1], sn[i - 1]);
+  const double res = fabs(sv[i]) / bnrm2;
+  st->resid = res;
+  st->i = i;
+  st->iters = iters;
+  if (res <= tol) st->state = 1;
+  else if (iters == maxit || i >= restrt) st->state = 2;
+}
+
+// y = H(0:k, 0:k)^-1 s (upper triangular, netlib dtrsv order), k = st->i
+__global__ void gmres_trsv_kernel(const double *__restrict__ H, int ldh, const double *__restrict__ sv, double *y,
+                                  const GmresStatus *st) {
+  if (threadIdx.x != 0) return;
+  const int k = st->i;
+  for (int j = 0; j < k; j++) y[j] = sv[j];
+  for (int j = k - 1; j >= 0; j--) {
     if (y[j] != 0.0) {
-      y[j] /= H[(size_t)j * ldh + j];
-      for (int i = j - 1; i >= 0; i--) y[i] -= y[j] * H[(size_t)j * ldh + i];
+      y[j] = __ddiv_rn(y[j], H[(size_t)j * ldh + j]);
+      const double t = y[j];
+      for (int r = j - 1; r >= 0; r--) y[r] = __dsub_rn(y[r], __dmul_rn(t, H[(size_t)j * ldh + r]));
     }
   }
-  const long long n2 = 2LL * c.n;
-  FB_CUDA(cudaMemcpyAsync(p.d_y, y.data(), it * sizeof(double), cudaMemcpyHostToDevice, c.stream));
-  update_kernel<<<kRedBlocks * 4, 256, 0, c.stream>>>(n2, it, p.d_V, n2, p.d_y, x);
-  c.launches += 1;
-  FB_CUDA(cudaGetLastError());
-  FB_CUDA(cudaStreamSynchronize(c.stream));  // y (host) must outlive the copy
+}
+
+// x += V y over the first st->i columns
+__global__ void gmres_update_kernel(long long n, const double *__restrict__ V, long long ldv,
+                                    const double *__restrict__ y, const GmresStatus *st, double *x) {
+  const int k = st->i;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    double s = x[i];
+    for (int j = 0; j < k; j++) s += y[j] * V[(size_t)j * ldv + i];
+    x[i] = s;
+  }
+}
+
+static bool gmres_log_enabled() {
+  static const bool on = [] {
+    const char *e = getenv("FABIPB_GMRES_LOG_RESID");
+    return e != nullptr && atoi(e) > 0;
+  }();
+  return on;
+}
+
+// the status record to the host (pinned), after everything queued so far
+static bool read_status(Context &c, const GmresStatus *d_st, GmresStatus *h_st) {
+  FB_CUDA(cudaMemcpyAsync(h_st, d_st, sizeof(GmresStatus), cudaMemcpyDeviceToHost, c.stream));
+  FB_CUDA(cudaStreamSynchronize(c.stream));
   return true;
 }
 
+// x := x + V y with y from the device triangular solve
+static bool gmres_update_dev(Context &c, int ldh, const GmresStatus *d_st, double *x) {
+  PrecondDev &p = *c.pc;
+  const long long n2 = 2LL * c.n;
+  gmres_trsv_kernel<<<1, 32, 0, c.stream>>>(p.d_H, ldh, p.d_sv, p.d_y, d_st);
+  gmres_update_kernel<<<kRedBlocks * 4, 256, 0, c.stream>>>(n2, p.d_V, n2, p.d_y, d_st, x);
+  c.launches += 2;
+  FB_CUDA(cudaGetLastError());
+  return true;
+}
+
+// Restarted, left-preconditioned GMRES of src/gmres.c:153-362 with every
+// vector and the Hessenberg/Givens state on the device.  Residual measure:
+// ||P^-1 (b - A x)|| / ||b||, estimated by |s_i| / ||b|| inside a cycle.
 bool gmres_solve(Context &c, const double *b, double *x, int restrt, int maxit, double tol, int *iters, double *resid,
                  int *info, bool adjoint) {
   FB_CHECK(c.pc != nullptr, "call fabipb_b200_precond_setup before solving (mode -1 for none)");
+  FB_CHECK(restrt >= 1, "GMRES restart must be at least 1");
   PrecondDev &p = *c.pc;
   const long long n2 = 2LL * c.n;
   const int ldh = restrt + 1;
@@ -1069,42 +1186,69 @@ bool gmres_solve(Context &c, const double *b, double *x, int restrt, int maxit, 
     if (!p.arena.alloc_n(&p.d_V, (size_t)n2 * (restrt + 1)) || !p.arena.alloc_n(&p.d_r, (size_t)n2) ||
         !p.arena.alloc_n(&p.d_av, (size_t)n2) || !p.arena.alloc_n(&p.d_w, (size_t)n2) ||
         !p.arena.alloc_n(&p.d_h, (size_t)ldh + 1) || !p.arena.alloc_n(&p.d_part, 2 * (size_t)kRedBlocks + 2) ||
-        !p.arena.alloc_n(&p.d_y, (size_t)restrt + 1))
+        !p.arena.alloc_n(&p.d_y, (size_t)restrt + 1) || !p.arena.alloc_n(&p.d_H, (size_t)ldh * (restrt + 2)) ||
+        !p.arena.alloc_n(&p.d_sv, (size_t)restrt + 2) || !p.arena.alloc(&p.d_status, sizeof(GmresStatus)))
       return false;
+    if (!p.h_status) FB_CUDA(cudaMallocHost(&p.h_status, 4 * sizeof(GmresStatus)));
   }
-  std::vector<double> H((size_t)ldh * (restrt + 2), 0.0), sv(restrt + 2, 0.0), hcol(ldh, 0.0);
-  double *cs = &H[(size_t)restrt * ldh], *sn = &H[(size_t)(restrt + 1) * ldh];
-  double bnrm2, rnorm, xn;
+  GmresStatus *d_st = static_cast<GmresStatus *>(p.d_status);
+  GmresStatus *h_st = static_cast<GmresStatus *>(p.h_status);
+  const bool logResid = gmres_log_enabled();
   *info = 0;
   *iters = maxit;
   *resid = tol;
-  // av = b (- A x when x != 0); r = P^-1 av
+  // ||x0|| decides whether b - A x0 needs the operator; ||b|| scales the test
+  double *norms = static_cast<double *>(p.h_status) + 2 * sizeof(GmresStatus) / sizeof(double);
+  if (!dot_dev(c, n2, x, x, p.d_part + kRedBlocks, true)) return false;
+  if (!dot_dev(c, n2, b, b, p.d_part + kRedBlocks + 1, true)) return false;
+  FB_CUDA(cudaMemcpyAsync(norms, p.d_part + kRedBlocks, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  FB_CUDA(cudaStreamSynchronize(s));
+  const double xn = norms[0];
+  double bnrm2 = norms[1];
+  if (bnrm2 == 0.0) bnrm2 = 1.0;
   FB_CUDA(cudaMemcpyAsync(p.d_av, b, n2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  if (!nrm2_host(c, n2, x, &xn)) return false;
   if (xn != 0.0) {
     if (!op_matvec(c, -1.0, x, 1.0, p.d_av, adjoint)) return false;
   }
   if (!precond_apply(c, p.d_av, p.d_r, adjoint)) return false;
-  if (!nrm2_host(c, n2, b, &bnrm2)) return false;
-  if (bnrm2 == 0.0) bnrm2 = 1.0;
-  if (!nrm2_host(c, n2, p.d_r, &rnorm)) return false;
-  if (rnorm / bnrm2 < tol) return true;
-  *iters = 0;
+  int it = 0;
+  bool first = true;
   for (;;) {
-    int i = 0;
-    if (!nrm2_host(c, n2, p.d_r, &rnorm)) return false;
-    if (!(rnorm > 0.0) || rnorm != rnorm) {
-      *resid = (rnorm != rnorm) ? rnorm : 0.0;
-      *info = (rnorm != rnorm) ? 2 : 0;
+    // cycle start: rnorm, the restart residual test, v_0 = r / rnorm
+    dot_partial_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(n2, p.d_r, p.d_r, p.d_part);
+    gmres_cycle_start_kernel<<<1, kRedThreads, 0, s>>>(p.d_part, kRedBlocks, bnrm2, tol, first ? 1 : 0, restrt,
+                                                       p.d_sv, d_st);
+    c.launches += 2;
+    FB_CUDA(cudaGetLastError());
+    if (!read_status(c, d_st, h_st)) return false;
+    if (first && h_st->state == 1) return true;   // converged at x0: iters and resid keep their entry values
+    *resid = h_st->resid;
+    if (!first && logResid) printf("GMRES residual: iter=%d resid=%e\n", it, h_st->resid);
+    if (h_st->state == 1) {
+      *iters = it;
       return true;
     }
-    scale_copy_kernel<<<kRedBlocks * 4, 256, 0, s>>>(n2, 1.0 / rnorm, p.d_r, p.d_V);
+    if (first) {
+      *iters = 0;
+      first = false;
+    } else if (it == maxit) {
+      *iters = it;
+      *info = 1;
+      return true;
+    }
+    if (h_st->state == 3) {
+      const double rn = h_st->rnorm;
+      *resid = (rn != rn) ? rn : 0.0;
+      *info = (rn != rn) ? 2 : 0;
+      *iters = it;
+      return true;
+    }
+    scale_copy_dev_kernel<<<kRedBlocks * 4, 256, 0, s>>>(n2, &d_st->rnorm, p.d_r, p.d_V);
     c.launches += 1;
-    sv.assign(restrt + 2, 0.0);
-    sv[0] = rnorm;
+    int i = 0;
     for (;;) {
       ++i;
-      ++(*iters);
+      ++it;
       if (!op_matvec(c, 1.0, p.d_V + (size_t)(i - 1) * n2, 0.0, p.d_av, adjoint)) return false;
       if (!precond_apply(c, p.d_av, p.d_w, adjoint)) return false;
       // modified Gram-Schmidt: h[k] = w.v_k; w -= h[k] v_k, one launch per
@@ -1119,32 +1263,24 @@ bool gmres_solve(Context &c, const double *b, double *x, int restrt, int maxit, 
       }
       mgs_norm_scale_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(n2, partA, p.d_h + i, p.d_w,
                                                                p.d_V + (size_t)i * n2);
-      c.launches += i + 2;
+      gmres_givens_kernel<<<1, 32, 0, s>>>(p.d_h, p.d_H, ldh, restrt, p.d_sv, i, it, maxit, bnrm2, tol, d_st);
+      c.launches += i + 3;
       FB_CUDA(cudaGetLastError());
-      FB_CUDA(cudaMemcpyAsync(hcol.data(), p.d_h, (i + 1) * sizeof(double), cudaMemcpyDeviceToHost, s));
-      FB_CUDA(cudaStreamSynchronize(s));
-      double *hc = &H[(size_t)(i - 1) * ldh];
-      for (int k = 0; k <= i; k++) hc[k] = hcol[k];
-      for (int k = 0; k < i - 1; k++) rot_h(&hc[k], &hc[k + 1], cs[k], sn[k]);
-      double aa = hc[i - 1], bb = hc[i];
-      drotg_h(&aa, &bb, &cs[i - 1], &sn[i - 1]);
-      rot_h(&hc[i - 1], &hc[i], cs[i - 1], sn[i - 1]);
-      rot_h(&sv[i - 1], &sv[i], cs[i - 1], sn[i - 1]);
-      *resid = fabs(sv[i]) / bnrm2;
-      if (*resid <= tol) return gmres_update_dev(c, i, H, ldh, sv, x);
-      if (*iters == maxit || i >= restrt) break;
+      if (!read_status(c, d_st, h_st)) return false;
+      *resid = h_st->resid;
+      if (logResid) printf("GMRES residual: iter=%d resid=%e\n", it, h_st->resid);
+      if (h_st->state == 1) {
+        *iters = it;
+        return gmres_update_dev(c, ldh, d_st, x);
+      }
+      if (h_st->state != 0) break;
     }
-    if (!gmres_update_dev(c, i, H, ldh, sv, x)) return false;
+    // end of a cycle: x += V y, r = P^-1 (b - A x)
+    if (!gmres_update_dev(c, ldh, d_st, x)) return false;
     FB_CUDA(cudaMemcpyAsync(p.d_av, b, n2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
     if (!op_matvec(c, -1.0, x, 1.0, p.d_av, adjoint)) return false;
     if (!precond_apply(c, p.d_av, p.d_r, adjoint)) return false;
-    if (!nrm2_host(c, n2, p.d_r, &sv[i])) return false;
-    *resid = sv[i] / bnrm2;
-    if (*resid <= tol) return true;
-    if (*iters == maxit) {
-      *info = 1;
-      return true;
-    }
+    *iters = it;
   }
 }
 

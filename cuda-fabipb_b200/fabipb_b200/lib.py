@@ -49,6 +49,7 @@ def load():
     vp = C.c_void_p
     L.fabipb_b200_default_params.argtypes = [C.POINTER(Params)]
     L.fabipb_b200_create.argtypes = [C.POINTER(Params), C.c_int, vp, vp, vp, C.POINTER(vp)]
+    L.fabipb_b200_create_direct.argtypes = [C.POINTER(Params), C.c_int, vp, vp, vp, C.POINTER(vp)]
     L.fabipb_b200_set_charges.argtypes = [vp, C.c_int, vp, vp]
     L.fabipb_b200_destroy.argtypes = [vp]
     L.fabipb_b200_set_stream.argtypes = [vp, vp]
@@ -82,6 +83,15 @@ def load():
     return L
 
 
+def fp32_peak_tflops(device=0) -> float:
+    """Measured FP32 FMA rate of `device` (TFLOP/s)."""
+    L = load()
+    L.fabipb_b200_fp32_peak.argtypes = [C.c_int, C.c_void_p]
+    v = np.zeros(1)
+    _check(L.fabipb_b200_fp32_peak(int(device), _ptr(v)), "fp32_peak")
+    return float(v[0])
+
+
 def last_error() -> str:
     return load().fabipb_b200_last_error().decode(errors="replace")
 
@@ -113,14 +123,16 @@ def params(order=3, depth=5, height=2, sep_ratio=0.8, quad_order=1, kappa=0.1257
 class Surface:
     """One panel mesh resident on the GPU (see include/fabipb_b200.h)."""
 
-    def __init__(self, panels, prm: Params, charges=None):
+    def __init__(self, panels, prm: Params, charges=None, direct=False):
+        """direct=True: the dense direct operator (every panel pair, no FMM)."""
         L = load()
         self._vtx = np.ascontiguousarray(panels.vtx.reshape(-1), dtype=np.float64)
         self._nrm = np.ascontiguousarray(panels.normal.reshape(-1), dtype=np.float64)
         self._area = np.ascontiguousarray(panels.area, dtype=np.float64)
         h = C.c_void_p()
-        _check(L.fabipb_b200_create(C.byref(prm), int(panels.n), _ptr(self._vtx), _ptr(self._nrm),
-                                    _ptr(self._area), C.byref(h)), "fabipb_b200_create")
+        make = L.fabipb_b200_create_direct if direct else L.fabipb_b200_create
+        _check(make(C.byref(prm), int(panels.n), _ptr(self._vtx), _ptr(self._nrm), _ptr(self._area), C.byref(h)),
+               "fabipb_b200_create")
         self.h = h
         self.params = prm
         self.n = int(panels.n)
@@ -319,7 +331,16 @@ class Surface:
         _check(load().fabipb_b200_precond_apply(self.h, _ptr(b), _ptr(x), 0), "precond_apply")
         return x
 
-    def solve(self, b, x0, restart=10, maxit=100, tol=1e-4):
+    def solve(self, b, x0, restart=10, maxit=100, tol=1e-4, on_device=0):
+        """GMRES from x0; on_device=1: b and x0 are device pointers and x0 is
+        overwritten with the solution (returned as is)."""
+        it = np.zeros(1, np.int32)
+        res = np.zeros(1)
+        info = np.zeros(1, np.int32)
+        if on_device:
+            _check(load().fabipb_b200_solve(self.h, _ptr(b), _ptr(x0), int(restart), int(maxit), float(tol),
+                                            _ptr(it), _ptr(res), _ptr(info), 1), "solve")
+            return x0, int(it[0]), float(res[0]), int(info[0])
         b = np.ascontiguousarray(b, dtype=np.float64)
         x = np.array(x0, dtype=np.float64)
         it = np.zeros(1, np.int32)

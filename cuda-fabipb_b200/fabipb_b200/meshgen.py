@@ -23,6 +23,9 @@ convention ``nrCommonVtx`` in ``src/numQuad.c:312-353`` relies on).
 """
 from __future__ import annotations
 
+import os
+from concurrent.futures import ThreadPoolExecutor
+
 import numpy as np
 from scipy.special import sph_harm_y, spherical_kn, eval_legendre
 
@@ -127,27 +130,44 @@ def real_sph_harm(l, m, theta, phi):
     return np.sqrt(2.0) * ((-1) ** m) * (np.real(y) if m > 0 else np.imag(y))
 
 
+def _harmonic_sum(coeffs, unit, chunk=32768):
+    """1 + sum over coeffs (l, m, a) of a * Y_lm(unit), in the listed order.
+
+    Each point's sum depends on that point alone, so the points are split into
+    chunks summed on a thread pool (scipy's harmonics release the GIL); every
+    chunk adds the terms in the same order, so the result does not depend on
+    the split or the thread count.
+    """
+    n = unit.shape[0]
+
+    def part(lo):
+        u = unit[lo:lo + chunk]
+        theta = np.arccos(np.clip(u[:, 2], -1.0, 1.0))
+        phi = np.arctan2(u[:, 1], u[:, 0])
+        f = np.ones(u.shape[0])
+        for l, m, a in coeffs:
+            f += a * real_sph_harm(l, m, theta, phi)
+        return f
+
+    starts = list(range(0, n, chunk))
+    if len(starts) <= 1:
+        return part(0) if n else np.ones(0)
+    workers = min(len(starts), os.cpu_count() or 1)
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        return np.concatenate(list(ex.map(part, starts)))
+
+
 def radial_perturbation(unit, lmin, lmax, sigma, rng):
     """1 + sum_{l,m} a_lm Y_lm(unit) with a_lm ~ N(0, sigma^2)."""
-    theta = np.arccos(np.clip(unit[:, 2], -1.0, 1.0))
-    phi = np.arctan2(unit[:, 1], unit[:, 0])
-    f = np.ones(unit.shape[0])
     coeffs = []
     for l in range(lmin, lmax + 1):
         for m in range(-l, l + 1):
-            a = rng.normal(0.0, sigma)
-            coeffs.append((l, m, a))
-            f += a * real_sph_harm(l, m, theta, phi)
-    return f, coeffs
+            coeffs.append((l, m, rng.normal(0.0, sigma)))
+    return _harmonic_sum(coeffs, unit), coeffs
 
 
 def eval_perturbation(coeffs, unit):
-    theta = np.arccos(np.clip(unit[:, 2], -1.0, 1.0))
-    phi = np.arctan2(unit[:, 1], unit[:, 0])
-    f = np.ones(unit.shape[0])
-    for l, m, a in coeffs:
-        f += a * real_sph_harm(l, m, theta, phi)
-    return f
+    return _harmonic_sum(coeffs, unit)
 
 
 def vertex_normals(pos, faces):

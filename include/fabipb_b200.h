@@ -67,12 +67,23 @@ void fabipb_b200_default_params(fabipb_b200_params *p);
 
 int fabipb_b200_create(const fabipb_b200_params *p, int n_panels, const double *vtx,
                        const double *normal, const double *area, void **ctx);
+/* The direct operator of the reference's -r modes (MtVmain's direct branch,
+   src/fabipb.c:1250-1265, src/direct_backend.c:172): every panel pair through
+   the near-field rules, no FMM.  The context takes every call a
+   fabipb_b200_create context takes; its matvec, solves and adjoint use the
+   O(N^2) sum (an FP64 direct-summation oracle in FP64 precision). */
+int fabipb_b200_create_direct(const fabipb_b200_params *p, int n_panels, const double *vtx,
+                              const double *normal, const double *area, void **ctx);
 int fabipb_b200_set_charges(void *ctx, int n_charges, const double *pos, const double *q);
 void fabipb_b200_destroy(void *ctx);
 int fabipb_b200_set_stream(void *ctx, void *cuda_stream);
 /* number of CUDA kernels this context has launched so far */
 long long fabipb_b200_launch_count(void *ctx);
 const char *fabipb_b200_last_error(void);
+/* Measured FP32 FMA rate of a device in TFLOP/s (packed f32x2 FMA chains,
+   best of five event-timed launches): the roofline denominator of the
+   FP32-bound near field.  No counterpart in the reference. */
+int fabipb_b200_fp32_peak(int device, double *tflops);
 
 /* tree queries, for parity checks against the reference layouts */
 int fabipb_b200_info_get(void *ctx, fabipb_b200_info *out);

@@ -12,6 +12,9 @@
  *   rhs     setupRHS (fabipb.c:744)
  *   energy  applyPanelChargeTreeEnergy (treecode.c:927) on a given density
  *   time    wall time of K calls of MtVmain, printed as one JSON line
+ *   sample  estimated MtVmain time of a mesh too large to time in full: the
+ *           FMM passes timed whole, the near field timed on a leaf sample and
+ *           scaled by panel pairs (one JSON line)
  *
  * The setup sequence mirrors main() in fabipb.c:830-1047: defaults, options,
  * loadPanel, the auto policy, gkInit, setupFMM.
@@ -227,6 +230,74 @@ int main(int argc, char **argv) {
     t1 = now();
     printf("{\"panels\": %d, \"reps\": %d, \"seconds\": %.6f, \"matvec_per_s\": %.6g}\n",
            sys->nPnls, reps, t1 - t0, reps / (t1 - t0));
+    return 0;
+  }
+
+  /*
+   * sample: the matvec of a mesh too large to time in full on the host, as
+   * `reps` estimated steps.  Each step times one whole MtVmain with the near
+   * field switched off (nLeafCubesFlat = 0 only shortens the destination-leaf
+   * loop of applyNearfield1CPU, fmm.c:631; the FMM passes and the diagonal
+   * run in full) and the near field alone (applyNearfield1, fmm.c:679) over
+   * the first L destination leaves, and adds that near-field time scaled by
+   * (all near panel pairs) / (panel pairs of the L leaves).  L is chosen from
+   * a first probe so that the sample takes about --budget seconds per step.
+   */
+  if (strcmp(mode, "sample") == 0) {
+    int n2 = 2 * sys->nPnls, r, nLeaves = sys->nLeafCubesFlat, L = 0, leaf;
+    double *sgm = (double *)malloc((size_t)n2 * sizeof(double));
+    double *pot = (double *)calloc((size_t)n2, sizeof(double));
+    double alpha = 1.0, beta = 0.0, tFar = 0.0, tNear = 0.0, est = 0.0, probe;
+    double *cum = (double *)calloc((size_t)nLeaves + 1, sizeof(double));
+    unsigned long long s = 12345ULL;
+    for (i = 0; i < n2; i++) {
+      s = s * 6364136223846793005ULL + 1442695040888963407ULL;
+      sgm[i] = (double)(s >> 11) / 9007199254740992.0 - 0.5;
+    }
+    for (leaf = 0; leaf < nLeaves; leaf++) {
+      double src = 0.0;
+      int k;
+      for (k = sys->nearLeafPairOffset[leaf]; k < sys->nearLeafPairOffset[leaf + 1]; k++)
+        src += sys->leafPanelCount[sys->nearPairSrc[k]];
+      cum[leaf + 1] = cum[leaf] + src * sys->leafPanelCount[leaf];
+    }
+    if (budget <= 0.0) budget = 5.0;
+    /* probe: leaves up to 2e7 panel pairs, for the rate */
+    for (L = 1; L < nLeaves && cum[L] < 2e7; L++) {}
+    {
+      double t0;
+      sys->nLeafCubesFlat = L;
+      t0 = now();
+      applyNearfield1(sys, &alpha, sgm, &beta, pot);
+      probe = now() - t0;
+      sys->nLeafCubesFlat = nLeaves;
+    }
+    {
+      double rate = cum[L] / (probe > 1e-6 ? probe : 1e-6), want = rate * budget;
+      for (L = 1; L < nLeaves && cum[L] < want; L++) {}
+    }
+    for (r = 0; r < warmup + reps; r++) {
+      double t0, tf, tn;
+      sys->nLeafCubesFlat = 0;
+      t0 = now();
+      MtVmain(&alpha, sgm, &beta, pot);
+      tf = now() - t0;
+      sys->nLeafCubesFlat = L;
+      t0 = now();
+      applyNearfield1(sys, &alpha, sgm, &beta, pot);
+      tn = now() - t0;
+      sys->nLeafCubesFlat = nLeaves;
+      if (r >= warmup) {
+        tFar += tf;
+        tNear += tn;
+        est += tf + tn * (cum[nLeaves] / cum[L]);
+      }
+    }
+    printf("{\"panels\": %d, \"reps\": %d, \"seconds\": %.6f, \"matvec_per_s\": %.6g, "
+           "\"far_s\": %.6f, \"near_sample_s\": %.6f, \"sample_leaves\": %d, \"leaves\": %d, "
+           "\"sample_pairs\": %.0f, \"near_pairs\": %.0f}\n",
+           sys->nPnls, reps, tFar + tNear, reps / est, tFar / reps, tNear / reps, L, nLeaves, cum[L],
+           cum[nLeaves]);
     return 0;
   }
 

@@ -1,6 +1,7 @@
 """Generate the golden fixtures under tests/golden/ from the reference itself.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # the small cases (cases.json, *.npz)
+    python tests/golden/make_golden.py --large    # solve-only goldens (solve_cases.json)
 
 Needs the reference CPU solver compiled from its own sources
 (``make -C oracle ref``, which reads the read-only reference mount).  For each
@@ -48,8 +49,27 @@ CASES = {
 }
 
 
+# Larger seeded cases (the benchmark configurations' meshes, and the
+# two-shell geometry at a coarse resolution) for which only the full CLI solve
+# is recorded: solvation energy, GMRES iterations, final residual.  "P" selects
+# the reference's preconditioner (-P=3 diagonal); without it the reference's
+# auto policy picks block LU for eps1 <= 2 and eps2/eps1 >= 40.
+SOLVE_CASES = {
+    "sphere20480": ("sphere", dict(nsub=5, radius=20.0, n_charges=500, seed=0),
+                    dict(p=3, t=3, S=0.8, a=10, o=1e-4, eps1=1.0, eps2=80.0)),
+    "shell16384": ("shell", dict(freq=32, r_in=200.0, r_out=230.0, n_charges=5000, seed=2),
+                   dict(p=5, t=4, S=0.6, a=10, o=1e-6, eps1=2.0, eps2=80.0, P=3)),
+    "star204800": ("star", dict(freq=160, radius=25.0, n_charges=20000, seed=1),
+                   dict(p=4, t=5, S=0.7, a=10, o=1e-5, eps1=2.0, eps2=80.0)),
+}
+# Golden cases also solved with the reference's dense direct operator (-r=2:
+# every panel pair by panelIA0 on the CPU, no FMM), the counterpart of the
+# library's dense context (-r=1 through the plugin ABI).
+DIRECT_CASES = ("sphere320", "sphere1280", "star2048")
+
+
 def generate_mesh(name, directory):
-    kind, kw, _ = CASES[name]
+    kind, kw, _ = CASES[name] if name in CASES else SOLVE_CASES[name]
     base = os.path.join(directory, name)
     fn = {"sphere": meshgen.sphere_case, "star": meshgen.star_case, "shell": meshgen.shell_case}[kind]
     fn(base, **kw)
@@ -69,6 +89,8 @@ def ref_opts(opts, with_solver=False):
            "-eps2=%g" % opts["eps2"]]
     if with_solver:
         out += ["-a=%d" % opts["a"], "-o=%g" % opts["o"]]
+        if "P" in opts:
+            out.append("-P=%d" % opts["P"])
     return out
 
 
@@ -76,10 +98,39 @@ def seeded_sigma(n, seed=0):
     return np.random.default_rng(seed).standard_normal(2 * n)
 
 
+def main_large():
+    """Solve-only goldens of SOLVE_CASES (minutes of reference CPU time) and the
+    dense direct solves of DIRECT_CASES, into solve_cases.json."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        raise SystemExit("build the reference first: make -C oracle ref")
+    out = {}
+    threads = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory() as tmp:
+        for name, (_, _, opts) in SOLVE_CASES.items():
+            base = generate_mesh(name, tmp)
+            e, it, res, _ = O.run_ref_solve(base, ref_opts(opts, True), threads=threads)
+            out[name] = {"opts": opts, "digest": mesh_digest(base),
+                         "solve": {"energy": e, "iterations": it, "residual": res}}
+            print(name, "energy", e, "its", it, "resid", res, flush=True)
+        direct = {}
+        for name in DIRECT_CASES:
+            opts = CASES[name][2]
+            base = generate_mesh(name, tmp)
+            e, it, res, _ = O.run_ref_solve(base, ref_opts(opts, True) + ["-r=2"], threads=threads)
+            direct[name] = {"energy": e, "iterations": it, "residual": res}
+            print(name, "direct (-r=2) energy", e, "its", it, "resid", res, flush=True)
+        out["direct"] = direct
+    with open(os.path.join(HERE, "solve_cases.json"), "w") as fp:
+        json.dump(out, fp, indent=1, sort_keys=True)
+
+
 def main():
     from oracle import oracle as O
     if not O.ref_available():
         raise SystemExit("build the reference first: make -C oracle ref")
+    if "--large" in sys.argv:
+        return main_large()
     meta = {}
     with tempfile.TemporaryDirectory() as tmp:
         for name, (_, _, opts) in CASES.items():
