@@ -1,33 +1,44 @@
-"""Benchmark of the FABIPB GMRES matvec on B200.
+"""Benchmark of the FABIPB GMRES matvec and solve on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision mixed|fp64] [--case star204800|star2097152|sphere20480]
+                    [--precision mixed|fp64] [--case shell2097152|star204800|...]
 
-Workload (one "step" = one operator application y = (D - K)x, the GMRES
-matvec of src/fabipb.c:1237): the star-shaped globular surface of 204,800
-flat triangles (octahedral geodesic, frequency 160, radius 25 A perturbed by
-l=2..6 harmonics), Taylor order p=4, MAC ratio 0.7, octree depth 5 (mean
-leaf 46 panels), eps 2/80, kappa 0.1257, synthetic seeded inputs.
---case star2097152 runs the same measurement on the 2,097,152-panel star
-(frequency 512, radius 50 A, depth 7: mean leaf 31 panels, 100,000 charges),
---case star8388608 on the 8,388,608-panel star (frequency 1024, radius 100 A,
-depth 8, 2,000,000 charges; with --solve-reps 1 --no-adjoint for a short run).
+Default workload, the capsid-scale two-shell configuration: a spherical shell
+of inner radius 200 A and outer radius 230 A as two closed octahedral
+geodesic spheres of frequency 362 (2,096,704 flat triangles; inner normals
+into the cavity), both perturbed by seeded l <= 12 harmonics of amplitude 2%,
+500,000 charges uniform in the shell at least 1.4 A from both surfaces
+(q ~ N(0, 0.4^2) e, net 0), eps 2/80, kappa 0.1257, Taylor order p=5, MAC
+0.6, octree depth 5 (mean leaf 254 panels, the depth nearest a 200-panel
+leaf), GMRES restart 10, tol 1e-6, diagonal preconditioner (the reference's
+-P=3: its block-LU policy stagnates on the two-shell surface, see the
+design notes).  One "step" = one operator application y = (D - K)x, the GMRES
+matvec of src/fabipb.c:1237.  Inputs are synthetic and seeded.
+--case star204800 runs the 204,800-panel star surface (p=4, MAC 0.7, depth 5,
+20,000 charges), where the FP64 direct-summation oracle (every panel pair,
+no FMM) is also solved; sphere20480 the 20,480-panel Kirkwood sphere.
 
 Reported:
-  value      matvec/s with x, y resident in HBM (device time, CUDA events on
-             the library's stream), L2 flushed between steps outside the
-             timed intervals;
+  value      matvec/s of the FP32-mixed operator with x, y resident in HBM
+             (CUDA events on the library's stream), L2 flushed between steps
+             outside the timed intervals;
   e2e        matvec/s through the C ABI with host buffers (H2D of x and D2H
-             of y inside the timed region, pinned host memory);
+             of y inside the timed region, pinned host memory); e2e_dropin
+             the same through the reference host's MtVmain on this library's
+             plugin ABI (src/gpu_backend.h), host wall time;
   roofline   the near-field P2P kernel (the dominant kernel): algorithmic
              FLOPs (60 per panel pair) per launch / its event-timed duration,
-             against the FP32 SIMT peak of the measured SM clock;
+             against the FP32 FMA rate measured on this GPU;
+  fp64       matvec/s of the FP64 operator (the plain FP64 GPU path);
+  solve      GMRES, refined and FP64 solves (every run), energies and their
+             errors, the adjoint's backward/forward cost;
   cpu_baseline  the reference CPU solver compiled from its own sources
-             (oracle/_ref), timed on a bounded sample of matvecs on this
-             host's cores;
-  ref_gpu_baseline  (--ref-gpu) the reference's own CUDA backend compiled
-             from its sources for sm_100a (oracle/_ref/ref_harness_gpu), the
-             same matvec with -g=1 on this GPU.
+             (oracle/_ref), on this host's cores: whole matvecs, or on the
+             large meshes the FMM passes whole plus the near field on a leaf
+             sample scaled by panel pairs;
+  ref_gpu_baseline  the reference's own CUDA backend compiled from its
+             sources for sm_100a (oracle/_ref/ref_harness_gpu), -g=1 on this
+             GPU.
 With --impl reference the line times that reference CPU matvec itself.
 N>1 GPUs run independent replicas (the path does not shard: replicas only);
 value is the sum over replicas, timed as the max over ranks.
@@ -51,21 +62,33 @@ sys.path.insert(0, os.path.join(ROOT, "cuda-fabipb_b200"))
 sys.path.insert(0, ROOT)
 
 CASES = {
-    # name: (generator, kwargs, solver options)
+    # name: (generator, kwargs, solver options); precond 2 = block LU, 3 = diagonal (the reference's -P)
+    # the capsid-scale two-shell surface: 2,096,704 triangles, 500,000 charges
+    "shell2097152": ("shell", dict(freq=362, r_in=200.0, r_out=230.0, n_charges=500000, seed=2),
+                     dict(order=5, depth=5, sep_ratio=0.6, eps1=2.0, eps2=80.0, tol=1e-6, restart=10, maxit=100,
+                          precond=3)),
     "star204800": ("star", dict(freq=160, radius=25.0, n_charges=20000, seed=1),
-                   dict(order=4, depth=5, sep_ratio=0.7, eps1=2.0, eps2=80.0, tol=1e-5, restart=10)),
-    # the 2.1M-panel size: 2,097,152 triangles (octahedral freq 512, radius 50 A), 100,000 charges
+                   dict(order=4, depth=5, sep_ratio=0.7, eps1=2.0, eps2=80.0, tol=1e-5, restart=10, maxit=100,
+                        precond=2)),
+    # a 2.1M-panel star (octahedral freq 512, radius 50 A), 100,000 charges
     "star2097152": ("star", dict(freq=512, radius=50.0, n_charges=100000, seed=7),
-                    dict(order=4, depth=7, sep_ratio=0.7, eps1=2.0, eps2=80.0, tol=1e-6, restart=10)),
-    # the scale-stress size: 8,388,608 triangles (freq 1024, radius 100 A), 2,000,000 charges
-    "star8388608": ("star", dict(freq=1024, radius=100.0, n_charges=2000000, seed=11),
-                    dict(order=4, depth=8, sep_ratio=0.7, eps1=2.0, eps2=80.0, tol=1e-6, restart=10)),
+                    dict(order=4, depth=7, sep_ratio=0.7, eps1=2.0, eps2=80.0, tol=1e-6, restart=10, maxit=100,
+                         precond=2)),
+    # the scale-stress shell: radii 400/440 A, 8,386,816 triangles, 2,000,000 charges
+    "shell8388608": ("shell", dict(freq=724, r_in=400.0, r_out=440.0, n_charges=2000000, seed=4),
+                     dict(order=5, depth=6, sep_ratio=0.6, eps1=2.0, eps2=80.0, tol=1e-6, restart=10, maxit=100,
+                          precond=3)),
     "sphere20480": ("sphere", dict(nsub=5, radius=20.0, n_charges=500, seed=0),
-                    dict(order=3, depth=3, sep_ratio=0.8, eps1=1.0, eps2=80.0, tol=1e-4, restart=10)),
+                    dict(order=3, depth=3, sep_ratio=0.8, eps1=1.0, eps2=80.0, tol=1e-4, restart=10, maxit=100,
+                         precond=2)),
 }
-PANELS = {"star204800": 204800, "star2097152": 2097152, "star8388608": 8388608, "sphere20480": 20480}
+PANELS = {"shell2097152": 2096704, "star204800": 204800, "star2097152": 2097152, "shell8388608": 8386816,
+          "sphere20480": 20480}
+DEFAULT_CASE = "shell2097152"
 METRIC = "matvec/s"
 FLOP_PER_PAIR = 60.0   # algorithmic count per near panel pair (KER4 + apply)
+DIRECT_ORACLE_MAX = 300000   # panels up to which the FP64 direct-summation oracle is solved
+SAMPLE_ABOVE = 500000        # panels above which the CPU reference matvec is sampled
 
 
 def case_base(name):
@@ -87,20 +110,46 @@ def ref_opts(opts):
             "-eps1=%g" % opts["eps1"], "-eps2=%g" % opts["eps2"]]
 
 
-def cpu_reference_rate(base, opts, reps, warmup=1, budget=60.0):
-    """matvec/s of the reference CPU solver (oracle/_ref) or, if it is absent,
-    of the FP64 restatement oracle; returns (value, kind, cores, sample).
-    At most `reps` timed matvecs, fewer if the warm-up matvec shows they would
-    exceed `budget` seconds (at least one is always timed)."""
+def case_config(name, opts, extra=None):
+    """The `config` object both arms report (same keys for the same case)."""
+    cfg = {"workload": name, "panels": PANELS[name], "charges": CASES[name][1]["n_charges"],
+           "order": opts["order"], "depth": opts["depth"], "sep_ratio": opts["sep_ratio"],
+           "eps1": opts["eps1"], "eps2": opts["eps2"], "kappa": 0.1257, "tol": opts["tol"],
+           "restart": opts["restart"], "precond": {2: "block LU (-P=2)", 3: "diagonal (-P=3)"}[opts["precond"]],
+           "l2": "256 MiB buffer written between steps, outside the timed intervals"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def cpu_reference_rate(base, name, opts, reps, warmup=1, budget=60.0):
+    """matvec/s of the reference CPU solver (oracle/_ref) on every host core,
+    or of the FP64 restatement oracle when that build is absent; returns
+    (value, kind, cores, sample, steps_timed).  Meshes up to SAMPLE_ABOVE
+    panels: whole MtVmain calls, at most `reps`, fewer when the warm-up shows
+    they would exceed `budget` seconds.  Larger meshes: `reps` estimated
+    steps, each the FMM passes timed whole plus the near field timed on a
+    leaf sample of about budget/reps seconds and scaled by panel pairs."""
     from oracle import oracle as O
     cores = os.cpu_count() or 1
     if O.ref_available():
         pre = os.path.join(tempfile.gettempdir(), "fabipb_ref_time")
+        if PANELS[name] > SAMPLE_ABOVE:
+            out = O.run_ref_harness("sample", base, pre, ref_opts(opts), threads=cores, reps=reps, warmup=warmup,
+                                    budget=max(budget / max(reps + warmup, 1) * 0.5, 1.0))
+            r = json.loads(out.strip().splitlines()[-1])
+            sample = ("%d estimated matvecs (MtVmain) after %d warm-up: the FMM passes and diagonal timed whole "
+                      "(%.2f s each), the near field timed on the first %d of %d leaves (%.3g of %.3g panel pairs, "
+                      "%.2f s) and scaled by panel pairs" %
+                      (r["reps"], warmup, r["far_s"], r["sample_leaves"], r["leaves"], r["sample_pairs"],
+                       r["near_pairs"], r["near_sample_s"]))
+            return r["matvec_per_s"], "reference", cores, sample, r["reps"]
         out = O.run_ref_harness("time", base, pre, ref_opts(opts), threads=cores, reps=reps,
                                 warmup=max(warmup, 1), budget=budget)
         r = json.loads(out.strip().splitlines()[-1])
         return (r["matvec_per_s"], "reference", cores,
-                "%d timed matvecs (MtVmain) of the full mesh after %d warm-up" % (r["reps"], max(warmup, 1)))
+                "%d timed matvecs (MtVmain) of the full mesh after %d warm-up" % (r["reps"], max(warmup, 1)),
+                r["reps"])
     from fabipb_b200 import meshio
     pan, _ = meshio.load_case(base)
     orc = O.Oracle(pan, O.make_params(order=opts["order"], depth=opts["depth"], sep_ratio=opts["sep_ratio"],
@@ -114,26 +163,49 @@ def cpu_reference_rate(base, opts, reps, warmup=1, budget=60.0):
     for _ in range(reps):
         orc.matvec(x)
     dt = time.perf_counter() - t0
-    return reps / dt, "port", cores, "%d timed matvecs of the full mesh (FP64 restatement)" % reps
+    return reps / dt, "port", cores, "%d timed matvecs of the full mesh (FP64 restatement)" % reps, reps
 
 
-def ref_gpu_rate(base, opts, reps=10):
+def ref_gpu_rate(base, name, opts, reps=10, timeout=900):
     """matvec/s of the reference's own CUDA backend (src/gpu_backend_cuda.cu,
     compiled from its sources into oracle/_ref by `make -C oracle refgpu`):
     MtVmain with -g=1 on this GPU, host wall time of `reps` calls after two
-    warm-up calls.  None when that build is absent or the run fails."""
+    warm-up calls.  None when that build is absent."""
     from oracle import oracle as O
     if not os.path.exists(O.REF_HARNESS_GPU):
         return None
     try:
         pre = os.path.join(tempfile.gettempdir(), "fabipb_refgpu_time")
         out = O.run_ref_harness("time", base, pre, ref_opts(opts), threads=os.cpu_count() or 1, reps=reps,
-                                warmup=2, gpu=True, timeout=900)
+                                warmup=2, gpu=True, timeout=timeout, budget=60.0)
         r = json.loads(out.strip().splitlines()[-1])
     except Exception as e:   # a baseline, not the product: report the failure, keep the line
-        return {"value": None, "error": str(e)[:200]}
+        return {"value": None, "error": str(e)[-300:]}
     return {"value": r["matvec_per_s"], "unit": "matvec/s", "kind": "reference CUDA backend (-g=1, FP64)",
             "sample": "%d timed MtVmain calls after 2 warm-up, host wall time" % r["reps"]}
+
+
+def dropin_rate(base, opts, reps=10, timeout=900):
+    """matvec/s end to end through the plugin ABI: the reference host's
+    MtVmain (its host M2M/L2L, host vectors) with this library behind
+    gpu_backend.h (oracle/_ref/ref_harness_dropin, -g=1), host wall time."""
+    from oracle import oracle as O
+    exe = os.path.join(os.path.dirname(O.REF_HARNESS), "ref_harness_dropin")
+    if not os.path.exists(exe):
+        return None
+    try:
+        pre = os.path.join(tempfile.gettempdir(), "fabipb_dropin_time")
+        cmd = [exe, "time", base, pre] + ref_opts(opts) + ["-g=1", "--reps=%d" % reps, "--warmup=2",
+                                                         "--budget=60"]
+        r = subprocess.run(cmd, env=O.ref_env(os.cpu_count() or 1), capture_output=True, text=True,
+                           timeout=timeout, check=True)
+        v = json.loads(r.stdout.strip().splitlines()[-1])
+    except Exception as e:
+        return {"value": None, "error": str(e)[-300:]}
+    n2 = 2 * v["panels"]
+    return {"value": v["matvec_per_s"], "unit": "matvec/s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+            "path": "reference host MtVmain on gpu_backend.h (host M2M/L2L, per-stage copies of the %d-vector)" % n2,
+            "sample": "%d timed MtVmain calls after 2 warm-up, host wall time" % v["reps"]}
 
 
 class ClockSampler:
@@ -222,6 +294,9 @@ def replica_value(world, steps, total_s):
 
 
 def run_reference(args):
+    """The reference arm: the reference's own CPU implementation of the
+    matvec (oracle/_ref, compiled from its sources), every host core, on this
+    arm's case, metric and config; rank 0 alone under torchrun."""
     rank, world, local, pg = dist_setup(args)
     name = args.case
     opts = CASES[name][2]
@@ -231,18 +306,19 @@ def run_reference(args):
         return
     base = case_base(name)
     t0 = time.perf_counter()
-    # one process: setup once, `warmup` untimed matvecs, then `steps` timed ones
-    value, kind, cores, sample = cpu_reference_rate(base, opts, args.steps, 1, budget=args.ref_budget)
+    value, kind, cores, sample, timed = cpu_reference_rate(base, name, opts, args.steps, args.warmup,
+                                                           budget=args.ref_budget)
     wall = time.perf_counter() - t0
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "matvec/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
+            "steps": timed, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded %s surface, %d panels)" % (CASES[name][0], PANELS[name]),
-            "config": {"workload": name, "panels": PANELS[name],
-                       "order": opts["order"], "depth": opts["depth"], "sep_ratio": opts["sep_ratio"]},
+            "data": "synthetic (seeded %s surface, %d panels, %d charges)" %
+                    (CASES[name][0], PANELS[name], CASES[name][1]["n_charges"]),
+            "config": case_config(name, opts, {"precision": "fp64 (reference CPU)",
+                                               "parallelism": "host threads"}),
             "cpu_baseline": {"value": value, "unit": "matvec/s", "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": "matvec/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "wall_s": wall}
+            "steps_requested": args.steps, "wall_s": wall}
     if pg:
         pg.destroy_process_group()
     print(json.dumps(line))
@@ -257,7 +333,7 @@ def measured_hbm_gbs():
         return 6650.0, "fallback"
 
 
-def pass_report(surf, info, x_ptr, flush, reps, prec_is_mixed, sm_mhz, n_sm):
+def pass_report(surf, info, x_ptr, flush, reps, prec_is_mixed, fp32, fp64):
     """Per-pass device times (CUDA events between the passes of one matvec,
     L2 flushed before every matvec) against each pass's bound: algorithmic
     FLOPs for the near field and M2L, algorithmic bytes for the rest."""
@@ -273,8 +349,6 @@ def pass_report(surf, info, x_ptr, flush, reps, prec_is_mixed, sm_mhz, n_sm):
     nmom = lambda q: (q + 1) * (q + 2) * (q + 3) // 6
     from math import comb
     hbm, hbm_src = measured_hbm_gbs()
-    fp32 = n_sm * 128 * 2 * sm_mhz * 1e6 / 1e12
-    fp64 = n_sm * 64 * 2 * sm_mhz * 1e6 / 1e12
     near_peak = fp32 if prec_is_mixed else fp64
     qb = 4.0 if prec_is_mixed else 8.0   # bytes per leaf-matrix entry (FP32 copies in a mixed context)
     work = {
@@ -292,7 +366,7 @@ def pass_report(surf, info, x_ptr, flush, reps, prec_is_mixed, sm_mhz, n_sm):
             ach = amount / t / 1e12
             out[k] = {"ms": ms[k], "bound": ("fp32" if peak == fp32 else "fp64"),
                       "achieved": ach, "unit": "TFLOP/s", "peak": peak, "frac": ach / peak,
-                      "algorithmic": amount}
+                      "algorithmic": amount, "peak_source": "measured FMA rate of this GPU"}
         else:
             ach = amount / t / 1e9
             out[k] = {"ms": ms[k], "bound": "hbm", "achieved": ach, "unit": "GB/s", "peak": peak,
@@ -302,103 +376,161 @@ def pass_report(surf, info, x_ptr, flush, reps, prec_is_mixed, sm_mhz, n_sm):
     return out
 
 
-def solve_report(pan, ch, opts, device, st, reps=3, adjoint=True):
-    """Full solves of the same case in both precisions: RHS (direct, or the
-    charge-tree treecode above 2e11 panel-charge pairs as the reference), block-LU
-    preconditioner, device GMRES from x0 = b (as the reference CLI), energy.
-    Times are CUDA-event times on the library's stream (the calls are
-    synchronous); setup = context (tree, near field, FMM lists) + RHS +
-    preconditioner."""
+def _ev():
+    import torch
+    return torch.cuda.Event(enable_timing=True)
+
+
+def solve_report(pan, ch, name, opts, device, st, reps=3, adjoint=True):
+    """Full solves of the case in both precisions, every vector on the device:
+    RHS (direct, or the charge-tree treecode above 2e11 panel-charge pairs as
+    the reference's GPU policy), the case's preconditioner, GMRES from x0 = b
+    (as the reference CLI), the panel-tree energy; the mixed context also
+    solves by iterative refinement (FP64 residuals) to the same tolerance.
+    Each precision runs 1 + reps times on a fresh context; the first run is
+    not reported (it pays the one-time module loading).  Every timed interval
+    is CUDA events on the library's stream around library calls only: setup
+    = context (tree, near field, FMM lists) + RHS + preconditioner."""
     import torch
     from fabipb_b200 import lib
-    out = {}
-    runs = {"mixed": [], "fp64": []}
-    mem_peak = {"mixed": 0.0, "fp64": 0.0}   # device memory in use after the solver set-up, GiB
     kcal = 2.0 * np.pi * 332.0716
-    # each precision runs 1 + reps times: the first pays the one-time loading
-    # of the kernels it is the first to use and is not reported; every time
-    # reported is the median over the other reps runs
-    seq = [("mixed", lib.MIXED)] * (1 + reps) + [("fp64", lib.FP64)] * (1 + reps)
-    # the reference's RHS policy on the GPU path: direct sums up to 2e11
-    # panel-charge pairs, the charge-tree treecode above (src/fabipb_options.c:15-16)
     use_tree = pan.n * len(ch.q) > 2e11
+    n2 = 2 * pan.n
+    runs = {"mixed": [], "fp64": []}
+    mem_peak = {"mixed": 0.0, "fp64": 0.0}
+    seq = [("mixed", lib.MIXED)] * (1 + reps) + [("fp64", lib.FP64)] * (1 + reps)
+    b = torch.empty(n2, dtype=torch.float64, device="cuda")
+    x = torch.empty_like(b)
     for tag, prec in seq:
-        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         torch.cuda.synchronize()
         w0 = time.perf_counter()
+        ev = [_ev() for _ in range(4)]
         ev[0].record(st)
         prm = lib.params(order=opts["order"], depth=opts["depth"], sep_ratio=opts["sep_ratio"], eps1=opts["eps1"],
                          eps2=opts["eps2"], precision=prec, device=device)
         s = lib.Surface(pan, prm, ch)
         s.set_stream(st.cuda_stream)
-        b = s.rhs(use_tree=use_tree)
-        s.precond_setup(2)
+        s.rhs(use_tree=use_tree, out=b.data_ptr(), on_device=1)
+        s.precond_setup(opts["precond"])
         ev[1].record(st)
         torch.cuda.synchronize()
         free, total = torch.cuda.mem_get_info()
         mem_peak[tag] = max(mem_peak[tag], (total - free) / 2**30)
-        x, it, res, info = s.solve(b, b.copy(), restart=opts["restart"], maxit=100, tol=opts["tol"])
+        x.copy_(b)
         ev[2].record(st)
-        e = s.energy_raw(x) * kcal
+        _, it, res, info = s.solve(b.data_ptr(), x.data_ptr(), restart=opts["restart"], maxit=opts["maxit"],
+                                   tol=opts["tol"], on_device=1)
         ev[3].record(st)
+        ee = [_ev(), _ev()]
+        ee[0].record(st)
+        e = s.energy_raw(x.data_ptr(), on_device=1) * kcal
+        ee[1].record(st)
         torch.cuda.synchronize()
         wall = time.perf_counter() - w0
-        # iterative refinement to the same tolerance (FP64 residuals; in the
-        # mixed context the corrections use the FP32 near field)
-        rf = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
-        rf[0].record(st)
-        xr, outer, itr, resr, infr = s.solve_refined(b, b.copy(), restart=opts["restart"], maxit=200,
-                                                     tol_inner=opts["tol"], tol=opts["tol"], max_outer=10)
-        rf[1].record(st)
-        torch.cuda.synchronize()
-        refined = {"gmres_s": rf[0].elapsed_time(rf[1]) / 1000.0, "outer": outer, "iterations": itr,
-                   "residual_fp64": resr, "info": infr, "energy_kcal_mol": s.energy_raw(xr) * kcal}
-        out[tag] = {"gmres_s": ev[1].elapsed_time(ev[2]) / 1000.0, "setup_s": ev[0].elapsed_time(ev[1]) / 1000.0,
-                    "energy_s": ev[2].elapsed_time(ev[3]) / 1000.0, "wall_s": wall, "iterations": it,
-                    "residual": res, "info": info, "energy_kcal_mol": e, "refined": refined}
-        if not adjoint:
-            s.close()
-            runs[tag].append(out.pop(tag))
-            continue
-        # gradients of the (direct) energy: forward = RHS + GMRES + energy,
-        # backward = adjoint GMRES + dE/dq, dE/dx of every charge
-        ag = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-        torch.cuda.synchronize()
-        ag[0].record(st)
-        ef, itf, resf, inff = s.forward(restart=opts["restart"], maxit=100, tol=opts["tol"])
-        ag[1].record(st)
-        dq, dx, itb, resb, infb = s.backward(1.0, restart=opts["restart"], maxit=100, tol=opts["tol"])
-        ag[2].record(st)
-        torch.cuda.synchronize()
-        fs, bs = ag[0].elapsed_time(ag[1]) / 1000.0, ag[1].elapsed_time(ag[2]) / 1000.0
-        out[tag]["adjoint"] = {"forward_s": fs, "backward_s": bs, "backward_over_forward": bs / fs,
-                               "forward_iterations": itf, "backward_iterations": itb, "info": [inff, infb],
-                               "charges": int(len(ch.q)), "energy_direct_kcal_mol": ef * kcal}
+        r = {"setup_s": ev[0].elapsed_time(ev[1]) / 1000.0, "gmres_s": ev[2].elapsed_time(ev[3]) / 1000.0,
+             "energy_s": ee[0].elapsed_time(ee[1]) / 1000.0, "iterations": it, "residual": res, "info": info,
+             "energy_kcal_mol": e, "wall_s": wall}
+        r["solve_s"] = r["setup_s"] + r["gmres_s"] + r["energy_s"]
+        if tag == "mixed":
+            # FP32-FMM corrections with FP64 residuals, to the same tolerance
+            x.copy_(b)
+            rf = [_ev(), _ev()]
+            rf[0].record(st)
+            _, outer, itr, resr, infr = s.solve_refined(b.data_ptr(), x.data_ptr(), restart=opts["restart"],
+                                                        maxit=2 * opts["maxit"], tol_inner=opts["tol"],
+                                                        tol=opts["tol"], max_outer=10, on_device=1)
+            rf[1].record(st)
+            torch.cuda.synchronize()
+            er = s.energy_raw(x.data_ptr(), on_device=1) * kcal
+            r["refined"] = {"gmres_s": rf[0].elapsed_time(rf[1]) / 1000.0, "outer": outer, "iterations": itr,
+                            "residual_fp64": resr, "info": infr, "energy_kcal_mol": er}
+            r["refined"]["solve_s"] = r["setup_s"] + r["refined"]["gmres_s"] + r["energy_s"]
+        if adjoint:
+            # gradients of the (direct) energy: forward = direct RHS + GMRES +
+            # direct energy, backward = adjoint GMRES + dE/dq, dE/dx of every charge
+            ag = [_ev() for _ in range(3)]
+            torch.cuda.synchronize()
+            ag[0].record(st)
+            ef, itf, resf, inff = s.forward(restart=opts["restart"], maxit=opts["maxit"], tol=opts["tol"])
+            ag[1].record(st)
+            dq, dx, itb, resb, infb = s.backward(1.0, restart=opts["restart"], maxit=opts["maxit"], tol=opts["tol"])
+            ag[2].record(st)
+            torch.cuda.synchronize()
+            fs, bs = ag[0].elapsed_time(ag[1]) / 1000.0, ag[1].elapsed_time(ag[2]) / 1000.0
+            r["adjoint"] = {"forward_s": fs, "backward_s": bs, "backward_over_forward": bs / fs,
+                            "forward_iterations": itf, "backward_iterations": itb, "info": [inff, infb],
+                            "charges": int(len(ch.q)), "energy_direct_kcal_mol": ef * kcal}
         s.close()
-        runs[tag].append(out.pop(tag))
+        runs[tag].append(r)
     med = lambda v: float(np.median(v))
+    out = {}
     for tag, rs in runs.items():
         rs = rs[1:]
         r = dict(rs[-1])
-        for k in ("gmres_s", "setup_s", "energy_s", "wall_s"):
+        for k in ("setup_s", "gmres_s", "energy_s", "solve_s", "wall_s"):
             r[k] = med([q[k] for q in rs])
-        r["wall_s_runs"] = [q["wall_s"] for q in rs]
-        r["refined"] = dict(rs[-1]["refined"], gmres_s=med([q["refined"]["gmres_s"] for q in rs]))
+            r[k + "_runs"] = [q[k] for q in rs]
+        if "refined" in r:
+            r["refined"] = dict(rs[-1]["refined"])
+            for k in ("gmres_s", "solve_s"):
+                r["refined"][k] = med([q["refined"][k] for q in rs])
+                r["refined"][k + "_runs"] = [q["refined"][k] for q in rs]
         if adjoint:
             a = dict(rs[-1]["adjoint"])
-            a["forward_s"] = med([q["adjoint"]["forward_s"] for q in rs])
-            a["backward_s"] = med([q["adjoint"]["backward_s"] for q in rs])
+            for k in ("forward_s", "backward_s"):
+                a[k] = med([q["adjoint"][k] for q in rs])
+                a[k + "_runs"] = [q["adjoint"][k] for q in rs]
             a["backward_over_forward"] = a["backward_s"] / a["forward_s"]
             r["adjoint"] = a
         r["runs"] = len(rs)
         r["device_mem_gib"] = mem_peak[tag]
         out[tag] = r
     m, f = out["mixed"], out["fp64"]
-    out["energy_rel_err_mixed_vs_fp64"] = abs(m["energy_kcal_mol"] - f["energy_kcal_mol"]) / abs(f["energy_kcal_mol"])
+    rel = lambda a, b: abs(a - b) / abs(b)
+    out["energy_rel_err_mixed_vs_fp64"] = rel(m["energy_kcal_mol"], f["energy_kcal_mol"])
+    out["energy_rel_err_refined_vs_fp64"] = rel(m["refined"]["energy_kcal_mol"], f["energy_kcal_mol"])
     out["gmres_speedup_mixed_vs_fp64"] = f["gmres_s"] / m["gmres_s"]
+    out["gmres_speedup_refined_vs_fp64"] = f["gmres_s"] / m["refined"]["gmres_s"]
+    out["solve_speedup_refined_vs_fp64"] = f["solve_s"] / m["refined"]["solve_s"]
     out["rhs"] = "charge tree" if use_tree else "direct"
     out["tol"] = opts["tol"]
     out["restart"] = opts["restart"]
+    out["precond"] = opts["precond"]
+    return out
+
+
+def direct_oracle_report(pan, ch, opts, device, st, energies):
+    """The FP64 direct-summation oracle: the dense direct operator (every
+    panel pair through the near-field rules, no FMM), solved in FP64 with the
+    case's preconditioner to 1e-8, its panel-tree energy; the relative error
+    of each FMM energy in `energies` (tag -> kcal/mol) against it."""
+    import torch
+    from fabipb_b200 import lib
+    kcal = 2.0 * np.pi * 332.0716
+    prm = lib.params(order=opts["order"], depth=opts["depth"], sep_ratio=opts["sep_ratio"], eps1=opts["eps1"],
+                     eps2=opts["eps2"], precision=lib.FP64, device=device)
+    ev = [_ev() for _ in range(3)]
+    ev[0].record(st)
+    s = lib.Surface(pan, prm, ch, direct=True)
+    s.set_stream(st.cuda_stream)
+    n2 = 2 * pan.n
+    b = torch.empty(n2, dtype=torch.float64, device="cuda")
+    s.rhs(use_tree=False, out=b.data_ptr(), on_device=1)
+    s.precond_setup(opts["precond"])
+    ev[1].record(st)
+    x = b.clone()
+    _, it, res, info = s.solve(b.data_ptr(), x.data_ptr(), restart=opts["restart"], maxit=300, tol=1e-8,
+                               on_device=1)
+    ev[2].record(st)
+    e = s.energy_raw(x.data_ptr(), on_device=1) * kcal
+    torch.cuda.synchronize()
+    pairs = s.info()["near_panel_pairs"]
+    s.close()
+    out = {"energy_kcal_mol": e, "iterations": it, "residual": res, "info": info, "tol": 1e-8,
+           "panel_pairs_per_matvec": pairs, "setup_s": ev[0].elapsed_time(ev[1]) / 1000.0,
+           "gmres_s": ev[1].elapsed_time(ev[2]) / 1000.0}
+    for tag, v in energies.items():
+        out["energy_rel_err_" + tag] = abs(v - e) / abs(e)
     return out
 
 
@@ -414,7 +546,15 @@ def run_ours(args):
     pan, ch = meshio.load_case(base)
     # the reference's CUDA backend first, in its own process, while this
     # process holds no device memory yet
-    ref_gpu = ref_gpu_rate(base, opts) if (args.ref_gpu and rank == 0) else None
+    ref_gpu = None
+    if rank == 0 and not args.no_ref_gpu:
+        if PANELS[name] <= DIRECT_ORACLE_MAX or args.ref_gpu:
+            ref_gpu = ref_gpu_rate(base, name, opts)
+        else:
+            ref_gpu = {"value": None, "skipped": "not run by default above %d panels (--ref-gpu runs it)" %
+                       DIRECT_ORACLE_MAX}
+    fp32_peak = lib.simt_peak_tflops(local, fp64=False)
+    fp64_peak = lib.simt_peak_tflops(local, fp64=True)
     prec = lib.MIXED if args.precision == "mixed" else lib.FP64
     prm = lib.params(order=opts["order"], depth=opts["depth"], sep_ratio=opts["sep_ratio"], eps1=opts["eps1"],
                      eps2=opts["eps2"], precision=prec, device=local)
@@ -427,6 +567,16 @@ def run_ours(args):
     y = torch.zeros(n2, dtype=torch.float64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
+    def timed_steps(fn, k):
+        st_, en_ = [_ev() for _ in range(k)], [_ev() for _ in range(k)]
+        for i in range(k):
+            flush.zero_()
+            st_[i].record(stream)
+            fn()
+            en_[i].record(stream)
+        torch.cuda.synchronize()
+        return [a.elapsed_time(b) for a, b in zip(st_, en_)]
+
     def step():
         surf.matvec(x.data_ptr(), 1.0, 0.0, y.data_ptr(), on_device=1)
 
@@ -436,32 +586,17 @@ def run_ours(args):
     for _ in range(max(args.warmup, 3)):
         step()
     torch.cuda.synchronize()
-
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     launches0 = surf.launch_count()
     with ClockSampler(local) as clk:
         if pg:
             pg.barrier()
         torch.cuda.synchronize()
-        for i in range(args.steps):
-            flush.zero_()
-            starts[i].record(stream)
-            step()
-            ends[i].record(stream)
-        torch.cuda.synchronize()
+        step_ms = timed_steps(step, args.steps)
         if pg:
             pg.barrier()
         launches = surf.launch_count() - launches0
         # the dominant kernel alone, same stream, for the roofline
-        nstarts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-        nends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-        for i in range(args.steps):
-            flush.zero_()
-            nstarts[i].record(stream)
-            near_only()
-            nends[i].record(stream)
-        torch.cuda.synchronize()
+        near_ms = timed_steps(near_only, args.steps)
         # e2e: host buffers through the C ABI (pinned), copies inside the region
         xh = torch.from_numpy(np.random.default_rng(rank + 7).standard_normal(n2)).pin_memory()
         yh = torch.zeros(n2, dtype=torch.float64).pin_memory()
@@ -471,13 +606,10 @@ def run_ours(args):
         for _ in range(args.steps):
             surf.matvec(xh_np, 1.0, 0.0, out=yh_np)
         e2e_s = time.perf_counter() - t0
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    near_ms = [s.elapsed_time(e) for s, e in zip(nstarts, nends)]
     total_s = sum(step_ms) / 1000.0
-    e2e_rate = args.steps / e2e_s
     if pg:
         total_s, e2e_s = replica_times(pg, total_s, e2e_s)
-        e2e_rate = args.steps / e2e_s
+    e2e_rate = args.steps / e2e_s
     value = replica_value(world, args.steps, total_s)
     if rank != 0:
         if pg:
@@ -487,15 +619,12 @@ def run_ours(args):
     near_s = float(np.mean(near_ms)) / 1000.0
     pairs = float(info["near_panel_pairs"])
     achieved = FLOP_PER_PAIR * pairs / near_s / 1e12
-    sm_mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
-    props = torch.cuda.get_device_properties(local)
-    n_sm = props.multi_processor_count
     if prec == lib.MIXED:
-        peak = n_sm * 128 * 2 * sm_mhz * 1e6 / 1e12
-        peak_src = "FP32 SIMT FMA pipe: %d SMs x 128 lanes x 2 flop x %.0f MHz (median SM clock sampled)" % (n_sm, sm_mhz)
+        peak, bound = fp32_peak, "fp32"
+        peak_src = "measured FP32 FMA rate of this GPU (packed f32x2 FMA chains, fabipb_b200_simt_peak)"
     else:
-        peak = n_sm * 64 * 2 * sm_mhz * 1e6 / 1e12
-        peak_src = "FP64 SIMT FMA pipe: %d SMs x 64 lanes x 2 flop x %.0f MHz (median SM clock sampled)" % (n_sm, sm_mhz)
+        peak, bound = fp64_peak, "fp64"
+        peak_src = "measured FP64 FMA rate of this GPU (DFMA chains, fabipb_b200_simt_peak)"
     traffic = None
     # DRAM bytes per launch from the committed ncu summary of this kernel and workload
     kname = "near_apply_f2_kernel<0>" if prec == lib.MIXED else "near_apply_kernel<double,0>"
@@ -505,39 +634,60 @@ def run_ours(args):
         with open(prof) as fp:
             m = re.search(r"dram_bytes_per_launch \| (\d+)", fp.read())
         traffic = int(m.group(1)) if m else None
-    passes = pass_report(surf, info, x.data_ptr(), flush, args.steps, prec == lib.MIXED, sm_mhz, n_sm)
-    mem_ctx = None
-    if not args.no_solve:   # the matvec context is not needed any more: free it before the solves
-        free, total = torch.cuda.mem_get_info()
-        mem_ctx = (total - free) / 2**30
-        surf.close()
+    passes = pass_report(surf, info, x.data_ptr(), flush, args.steps, prec == lib.MIXED, fp32_peak, fp64_peak)
+    free, total = torch.cuda.mem_get_info()
+    mem_ctx = (total - free) / 2**30
+    surf.close()
+    # the plain FP64 operator on the same case (a second context)
+    fp64_rate = None
+    if prec == lib.MIXED and not args.no_fp64:
+        s64 = lib.Surface(pan, lib.params(order=opts["order"], depth=opts["depth"], sep_ratio=opts["sep_ratio"],
+                                          eps1=opts["eps1"], eps2=opts["eps2"], precision=lib.FP64, device=local), ch)
+        s64.set_stream(stream.cuda_stream)
+        for _ in range(2):
+            s64.matvec(x.data_ptr(), 1.0, 0.0, y.data_ptr(), on_device=1)
+        k64 = max(3, args.steps // 2)
+        ms64 = timed_steps(lambda: s64.matvec(x.data_ptr(), 1.0, 0.0, y.data_ptr(), on_device=1), k64)
+        fp64_rate = {"value": 1000.0 * k64 / sum(ms64), "unit": "matvec/s", "steps": k64,
+                     "ms_per_step": sum(ms64) / k64}
+        s64.close()
+    del flush
+    torch.cuda.empty_cache()
     solve = None
     if not args.no_solve:
         with ClockSampler(local) as clk2:   # the clocks during the solves too
-            solve = solve_report(pan, ch, opts, local, stream, reps=args.solve_reps, adjoint=not args.no_adjoint)
+            solve = solve_report(pan, ch, name, opts, local, stream, reps=args.solve_reps,
+                                 adjoint=not args.no_adjoint)
+            if PANELS[name] <= DIRECT_ORACLE_MAX and not args.no_direct_oracle:
+                en = {"mixed": solve["mixed"]["energy_kcal_mol"], "refined": solve["mixed"]["refined"]["energy_kcal_mol"],
+                      "fp64": solve["fp64"]["energy_kcal_mol"]}
+                solve["direct_oracle"] = direct_oracle_report(pan, ch, opts, local, stream, en)
         solve["clocks"] = clk2.summary()
+    dropin = None if args.no_dropin else dropin_rate(base, opts)
     cpu = None
     if not args.no_cpu_baseline:
-        v, kind, cores, sample = cpu_reference_rate(base, opts, args.cpu_reps, 1, budget=30.0)
+        v, kind, cores, sample, _ = cpu_reference_rate(base, name, opts, args.cpu_reps, 1, budget=30.0)
         cpu = {"value": v, "unit": "matvec/s", "cores": cores, "kind": kind, "sample": sample}
     line = {
         "metric": METRIC, "value": value, "unit": "matvec/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 * total_s / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32" if prec == lib.MIXED else "f64",
-        "data": "synthetic (seeded %s surface, %d seeded charges)" % (CASES[name][0], CASES[name][1]["n_charges"]),
-        "config": {"workload": name, "panels": surf.n, "order": opts["order"], "depth": opts["depth"],
-                   "sep_ratio": opts["sep_ratio"], "eps1": opts["eps1"], "eps2": opts["eps2"],
-                   "precision": args.precision, "parallelism": "replicas" if world > 1 else "single",
-                   "leaves": info["leaves"], "near_panel_pairs": info["near_panel_pairs"],
-                   "m2l_pairs": info["m2l_pairs"], "special_pairs": info["special_pairs"],
-                   "l2": "256 MiB buffer written between steps, outside the timed intervals"},
+        "data": "synthetic (seeded %s surface, %d panels, %d charges)" %
+                (CASES[name][0], surf.n, CASES[name][1]["n_charges"]),
+        "config": case_config(name, opts, {"precision": args.precision,
+                                           "parallelism": "replicas" if world > 1 else "single"}),
+        "tree": {"leaves": info["leaves"], "max_leaf": info["max_leaf"], "mean_leaf": surf.n / info["leaves"],
+                 "near_panel_pairs": info["near_panel_pairs"], "m2l_pairs": info["m2l_pairs"],
+                 "special_pairs": info["special_pairs"]},
         "e2e": {"value": e2e_rate * world, "unit": "matvec/s", "h2d_bytes_per_step": n2 * 8,
-                "d2h_bytes_per_step": n2 * 8},
-        "roofline": {"kernel": kname,
-                     "bound": "fp32" if prec == lib.MIXED else "fp64", "achieved": achieved, "peak": peak,
+                "d2h_bytes_per_step": n2 * 8, "path": "fabipb_b200_matvec, pinned host x and y"},
+        "e2e_dropin": dropin,
+        "roofline": {"kernel": kname, "bound": bound, "achieved": achieved, "peak": peak,
                      "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
                      "peak_source": peak_src, "flop_per_pair": FLOP_PER_PAIR,
                      "pairs_per_launch": pairs, "launch_ms": near_s * 1000.0},
+        "peaks": {"fp32_tflops": fp32_peak, "fp64_tflops": fp64_peak, "hbm_gbs": measured_hbm_gbs()[0]},
+        "fp64": fp64_rate,
         "cpu_baseline": cpu,
         "ref_gpu_baseline": ref_gpu,
         "gpu_launches": launches,
@@ -559,15 +709,19 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
-    ap.add_argument("--case", default="star204800", choices=sorted(CASES))
+    ap.add_argument("--case", default=DEFAULT_CASE, choices=sorted(CASES))
     ap.add_argument("--cpu-reps", type=int, default=2)
-    ap.add_argument("--ref-budget", type=float, default=90.0,
-                    help="seconds of timed reference matvecs at most (--impl reference)")
+    ap.add_argument("--ref-budget", type=float, default=150.0,
+                    help="seconds of timed reference work at most (--impl reference)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-gpu", action="store_true",
-                    help="also time the reference's own CUDA backend (oracle/_ref/ref_harness_gpu, -g=1)")
+                    help="time the reference's own CUDA backend also on meshes above %d panels" % DIRECT_ORACLE_MAX)
+    ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference's CUDA backend")
+    ap.add_argument("--no-dropin", action="store_true", help="skip the plugin-ABI end-to-end timing")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 operator's matvec rate")
+    ap.add_argument("--no-direct-oracle", action="store_true", help="skip the FP64 direct-summation oracle solve")
     ap.add_argument("--no-solve", action="store_true", help="skip the mixed/FP64 solve report")
-    ap.add_argument("--solve-reps", type=int, default=3, help="reported runs per precision (after one warm-up run)")
+    ap.add_argument("--solve-reps", type=int, default=2, help="reported runs per precision (after one warm-up run)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the forward/backward gradient timing")
     args = ap.parse_args()
     if args.impl == "reference":

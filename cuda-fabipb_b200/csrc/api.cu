@@ -297,6 +297,12 @@ int create_context(const fabipb_b200_params *p, int n, const double *vtx, const 
   tm.mark("near_setup");
   ok = ok && setup_fmm(*c);
   tm.mark("fmm_setup");
+  // the geometry-only tables of the adjoint operator (the transposed special
+  // pairs and M2L lists) and, in a mixed context, the FP64 near-field records
+  // of the refinement residuals: built here, once, so that no solve, backward
+  // pass or refinement pays for them on its first call
+  ok = ok && setup_near_adjoint(*c) && setup_m2l_adjoint(*c) && (!c->mixed || setup_near_fp64(*c));
+  tm.mark("adjoint_and_refinement_tables");
   if (ok && cudaStreamSynchronize(c->stream) != cudaSuccess) {
     set_error("setup kernels failed: %s", cudaGetErrorString(cudaGetLastError()));
     ok = false;

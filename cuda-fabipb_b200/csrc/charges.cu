@@ -460,12 +460,21 @@ __global__ void tree_walk_kernel(int mode, int n, int q, const double *__restric
   }
 }
 
-__global__ void sum_partials_kernel(int k, const double *__restrict__ p, double *out) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    double s = 0.0;
-    for (int i = 0; i < k; i++) s += p[i];
-    *out = s;
+// out = sum of the k partials, in a fixed order whatever k: thread t adds
+// p[t], p[t + 256], ... in turn, then a fixed shared-memory tree adds the 256
+// thread sums (one block of kSumThreads threads)
+constexpr int kSumThreads = 256;
+__global__ void __launch_bounds__(kSumThreads) sum_partials_kernel(int k, const double *__restrict__ p, double *out) {
+  __shared__ double red[kSumThreads];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < k; i += kSumThreads) s += p[i];
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int m = kSumThreads / 2; m > 0; m >>= 1) {
+    if ((int)threadIdx.x < m) red[threadIdx.x] += red[threadIdx.x + m];
+    __syncthreads();
   }
+  if (threadIdx.x == 0) *out = red[0];
 }
 
 template <int PM>
@@ -548,7 +557,7 @@ bool launch_energy_mode(Context &c, const double *sgm, int mode, double *raw_hos
   }
   FB_DISPATCH_WALK(c.P, c, mode, sgm, nullptr, d.d_partial);
   c.launches += 2;
-  sum_partials_kernel<<<1, 32, 0, c.stream>>>(blocks, d.d_partial, d.d_partial + blocks);
+  sum_partials_kernel<<<1, kSumThreads, 0, c.stream>>>(blocks, d.d_partial, d.d_partial + blocks);
   FB_CUDA(cudaGetLastError());
   FB_CUDA(cudaMemcpyAsync(raw_host, d.d_partial + blocks, sizeof(double), cudaMemcpyDeviceToHost, c.stream));
   FB_CUDA(cudaStreamSynchronize(c.stream));
@@ -582,7 +591,7 @@ bool abi_coulomb_dot(Context &c, const double *rhs, const double *sgm, double ep
   double *part = nullptr;
   FB_CUDA(cudaMallocAsync((void **)&part, (blocks + 1) * sizeof(double), c.stream));
   coulomb_dot_kernel<<<blocks, 256, 0, c.stream>>>(c.n, eps1, rhs, sgm, part);
-  sum_partials_kernel<<<1, 32, 0, c.stream>>>(blocks, part, part + blocks);
+  sum_partials_kernel<<<1, kSumThreads, 0, c.stream>>>(blocks, part, part + blocks);
   c.launches += 2;
   cudaError_t e = cudaMemcpyAsync(dot, part + blocks, sizeof(double), cudaMemcpyDeviceToHost, c.stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);

@@ -44,7 +44,7 @@ struct Context {
   long long nSpecial = 0;
   int *d_spOff = nullptr, *d_spSrc = nullptr;  // CSR by destination panel
   double4 *d_spK = nullptr;                    // exact minus one-point coefficient
-  double4 *d_spKT = nullptr;                   // the same for the transposed operator (built on first use)
+  double4 *d_spKT = nullptr;                   // the same for the transposed operator
   void *d_tgtP64 = nullptr, *d_tgtN64 = nullptr;   // FP64 records of a mixed context (refinement residuals)
   void *d_srcA64 = nullptr, *d_srcB64 = nullptr;
 
@@ -70,7 +70,7 @@ struct Context {
   long long nM2LPairs = 0;
   double2 *d_m2lTens = nullptr;                // [nMom][pairs] (D G0, D Gk) per M2L pair
   float2 *d_m2lTensF = nullptr;                // the same in FP32 (mixed contexts, orders <= 5)
-  // transposed M2L lists (adjoint operator, built on first use)
+  // transposed M2L lists (adjoint operator)
   bool m2lAdjReady = false;
   std::vector<int> h_m2lDstT;
   int *d_m2lDstT = nullptr, *d_m2lOffT = nullptr, *d_m2lSrcT = nullptr, *d_m2lPairT = nullptr;
@@ -134,8 +134,10 @@ bool launch_energy(Context &c, const double *sgm, double *raw_host);
 bool precond_setup(Context &c, int mode);
 // (adjoint: the transposed preconditioner and operator, for A^T lambda = e)
 bool precond_apply(Context &c, const double *b, double *x, bool adjoint = false);
+// (steps: the Arnoldi steps actually taken; *iters follows the reference and
+// keeps maxit when x already meets tol)
 bool gmres_solve(Context &c, const double *b, double *x, int restart, int maxit, double tol,
-                 int *iters, double *resid, int *info, bool adjoint = false);
+                 int *iters, double *resid, int *info, bool adjoint = false, int *steps = nullptr);
 // iterative refinement: FP64 residuals, corrections by GMRES on the context's operator
 bool refined_solve(Context &c, const double *b, double *x, int restart, int maxit, double tolInner, double tol,
                    int maxOuter, int *outer, int *iters, double *resid, int *info);

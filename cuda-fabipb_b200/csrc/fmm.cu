@@ -1002,7 +1002,7 @@ bool setup_fmm(Context &c) {
   return true;
 }
 
-// Transposed M2L lists (built on the first adjoint apply): for every cube s
+// Transposed M2L lists (built at context set-up): for every cube s
 // the forward pairs (f <- s) as entries (source f, forward pair index), f
 // ascending.
 static bool setup_m2l_adjoint(Context &c) {

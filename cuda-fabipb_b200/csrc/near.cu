@@ -855,7 +855,7 @@ static void launch_near_t(Context &c, const void *tgtP, const void *tgtN, void *
 }
 
 // FP64 records in a mixed context, for the FP64 residuals of iterative
-// refinement (built on first use)
+// refinement (built at context set-up)
 static bool setup_near_fp64(Context &c) {
   if (c.d_tgtP64) return true;
   const int n = c.n;

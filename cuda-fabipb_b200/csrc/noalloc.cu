@@ -14,50 +14,38 @@
 // The scratch: g_energyScratch, kNoAllocMaxBlocks doubles (128 KiB), one per
 // 256-panel block of the tree walk, so surfaces of up to 4,194,304 panels.
 // Every GPU that loads this library holds the array until the process exits.
-// Its device address is looked up once per device (cudaGetSymbolAddress with
-// that device current) by the first call on that device; that first call
-// should therefore come before any stream capture.  Every call on a device
-// shares the one array, which keeps the last call's partial sums; each block
-// of the walk writes its entry before the final sum reads it, so nothing needs
-// clearing.  Calls that overlap on the GPU (two streams, two contexts on one
-// device) race on the array: serialise them.
-
-#include <mutex>
+// The array's name in host code is only a host-side stand-in, so its device
+// address is looked up with cudaGetSymbolAddress, which allocates nothing, on
+// every call with the context's device current: the address always belongs to
+// the CUDA context current on the calling thread (after a cudaDeviceReset, or
+// under another context, the module and its array are loaded anew there).  The
+// first call in a process may load the library's device image; make it before
+// any stream capture.  Each CUDA context holds its own copy of the array; all
+// calls in one context share it, and it keeps the last call's partial sums.
+// Each block of the walk writes its entry before the final sum reads it, so
+// nothing needs clearing.  Calls in one context that overlap on the GPU (two
+// streams, two library contexts on one device) race on the array: serialise
+// them.
 
 namespace fb {
 
 constexpr int kNoAllocMaxBlocks = 16384;
-constexpr int kNoAllocMaxDevices = 64;
-
 static __device__ __align__(256) double g_energyScratch[kNoAllocMaxBlocks];
 
-// host-side table of the array's address on each device; the array's name in
-// host code is only a stand-in, so the device address has to be looked up
-static double *g_scratchAddr[kNoAllocMaxDevices] = {nullptr};
-static std::mutex g_scratchMu;
-
+// the array's device address in the current context (device `device`)
 static double *noalloc_scratch(int device) {
-  if (device < 0 || device >= kNoAllocMaxDevices) {
-    set_error("device %d outside 0..%d", device, kNoAllocMaxDevices - 1);
+  int cur = -1;
+  if (cudaGetDevice(&cur) != cudaSuccess || cur != device) {
+    set_error("scratch look-up: device %d is not current", device);
     return nullptr;
   }
-  std::lock_guard<std::mutex> lk(g_scratchMu);
-  if (g_scratchAddr[device] == nullptr) {
-    int cur = -1;
-    cudaGetDevice(&cur);
-    if (cur != device) {
-      set_error("scratch set-up: device %d is not current", device);
-      return nullptr;
-    }
-    void *p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_energyScratch);
-    if (e != cudaSuccess || p == nullptr) {
-      set_error("scratch set-up on device %d failed: %s", device, cudaGetErrorString(e));
-      return nullptr;
-    }
-    g_scratchAddr[device] = (double *)p;
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_energyScratch);
+  if (e != cudaSuccess || p == nullptr) {
+    set_error("scratch look-up on device %d failed: %s", device, cudaGetErrorString(e));
+    return nullptr;
   }
-  return g_scratchAddr[device];
+  return (double *)p;
 }
 
 }  // namespace fb
@@ -88,7 +76,7 @@ extern "C" int fabipb_b200_energy_noalloc(void *ctx, const double *sgm, double *
   if (scratch == nullptr) return 0;
   // the same walk as fabipb_b200_energy (mode 1), partial sums into the fixed array
   FB_DISPATCH_WALK(c->P, *c, 1, sgm, nullptr, scratch);
-  sum_partials_kernel<<<1, 32, 0, c->stream>>>((int)blocks, scratch, raw);
+  sum_partials_kernel<<<1, kSumThreads, 0, c->stream>>>((int)blocks, scratch, raw);
   c->launches += 2;
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {

@@ -83,12 +83,12 @@ def load():
     return L
 
 
-def fp32_peak_tflops(device=0) -> float:
-    """Measured FP32 FMA rate of `device` (TFLOP/s)."""
+def simt_peak_tflops(device=0, fp64=False) -> float:
+    """Measured FMA rate of `device`'s FP32 (or FP64) pipe in TFLOP/s."""
     L = load()
-    L.fabipb_b200_fp32_peak.argtypes = [C.c_int, C.c_void_p]
+    L.fabipb_b200_simt_peak.argtypes = [C.c_int, C.c_int, C.c_void_p]
     v = np.zeros(1)
-    _check(L.fabipb_b200_fp32_peak(int(device), _ptr(v)), "fp32_peak")
+    _check(L.fabipb_b200_simt_peak(int(device), int(bool(fp64)), _ptr(v)), "simt_peak")
     return float(v[0])
 
 
@@ -264,18 +264,22 @@ class Surface:
         _check(load().fabipb_b200_pass_times(self.h, _ptr(x), int(reps), _ptr(ms), int(on_device)), "pass_times")
         return dict(zip(self.PASSES, ms.tolist()))
 
-    def solve_refined(self, b, x0, restart=10, maxit=200, tol_inner=1e-5, tol=1e-10, max_outer=20):
+    def solve_refined(self, b, x0, restart=10, maxit=200, tol_inner=1e-5, tol=1e-10, max_outer=20, on_device=0):
         """Iterative refinement (FP64 residuals, corrections by GMRES on this
-        context's operator); returns (x, outer, iters, resid, info)."""
-        b = np.ascontiguousarray(b, dtype=np.float64)
-        x = np.array(x0, dtype=np.float64)
+        context's operator); returns (x, outer, iters, resid, info).
+        on_device=1: b and x0 are device pointers, x0 is overwritten."""
+        if on_device:
+            x = x0
+        else:
+            b = np.ascontiguousarray(b, dtype=np.float64)
+            x = np.array(x0, dtype=np.float64)
         ou = np.zeros(1, np.int32)
         it = np.zeros(1, np.int32)
         res = np.zeros(1)
         info = np.zeros(1, np.int32)
         _check(load().fabipb_b200_solve_refined(self.h, _ptr(b), _ptr(x), int(restart), int(maxit), float(tol_inner),
                                                 float(tol), int(max_outer), _ptr(ou), _ptr(it), _ptr(res), _ptr(info),
-                                                0), "solve_refined")
+                                                int(bool(on_device))), "solve_refined")
         return x, int(ou[0]), int(it[0]), float(res[0]), int(info[0])
 
     def energy_weights(self):

@@ -80,10 +80,11 @@ int fabipb_b200_set_stream(void *ctx, void *cuda_stream);
 /* number of CUDA kernels this context has launched so far */
 long long fabipb_b200_launch_count(void *ctx);
 const char *fabipb_b200_last_error(void);
-/* Measured FP32 FMA rate of a device in TFLOP/s (packed f32x2 FMA chains,
-   best of five event-timed launches): the roofline denominator of the
-   FP32-bound near field.  No counterpart in the reference. */
-int fabipb_b200_fp32_peak(int device, double *tflops);
+/* Measured FMA rate of a device's FP32 (fp64 = 0: packed f32x2 FMA chains)
+   or FP64 (fp64 = 1) pipe in TFLOP/s, best of five event-timed launches: the
+   roofline denominators of the FMA-bound near field.  No counterpart in the
+   reference. */
+int fabipb_b200_simt_peak(int device, int fp64, double *tflops);
 
 /* tree queries, for parity checks against the reference layouts */
 int fabipb_b200_info_get(void *ctx, fabipb_b200_info *out);
@@ -138,10 +139,12 @@ int fabipb_b200_energy(void *ctx, const double *sgm, double *raw, int on_device)
    ready when that stream reaches it.  Per-block partial sums go to a fixed
    128 KiB array in the library's device image (limit 4,194,304 panels); the
    charge tree must already exist (one fabipb_b200_energy or tree
-   fabipb_b200_rhs call builds it).  The first call on a device looks up the
-   array's address and should come before any stream capture; calls that
-   overlap on one GPU share the array and race.  No counterpart in the
-   reference, whose energy path allocates per call. */
+   fabipb_b200_rhs call builds it).  Every call looks the array's address up
+   in the current CUDA context (no allocation); the first call in a process
+   may load the device image and should come before any stream capture.
+   Calls in one CUDA context share the array: calls that overlap on the GPU
+   race.  No counterpart in the reference, whose energy path allocates per
+   call. */
 int fabipb_b200_energy_noalloc(void *ctx, const double *sgm, double *raw);
 /* gradients of the solvation energy with respect to the charges, surface
    fixed (no counterpart in the reference).  The energy here is the direct

@@ -27,6 +27,13 @@ def golden_meta():
 
 
 @pytest.fixture(scope="session")
+def solve_meta():
+    """Solve-only goldens of the larger cases and the reference's -r=2 direct solves."""
+    with open(os.path.join(GOLDEN, "solve_cases.json")) as fp:
+        return json.load(fp)
+
+
+@pytest.fixture(scope="session")
 def case_dir(tmp_path_factory):
     """All golden meshes, generated once per session from their seeds."""
     import make_golden

@@ -64,13 +64,33 @@ def test_dropin_debug_compare(case_dir, golden_meta):
 
 
 @pytest.mark.skipif(not os.path.exists(DROPIN), reason="drop-in binary not built (make -C oracle dropin)")
-def test_dropin_direct_mode_and_gpu_precond(case_dir, golden_meta):
-    """-r=1 (dense direct matvec through gpuDirectApply) and the GPU
-    preconditioner block builder both run without a CPU fallback."""
+@pytest.mark.parametrize("name", list(make_golden.DIRECT_CASES))
+def test_dropin_direct_mode_matches_reference_direct(name, case_dir, golden_meta, solve_meta):
+    """-r=1 (the dense direct matvec through gpuDirectApply) against the
+    reference's own CPU direct mode -r=2 (cpuDirectApply,
+    src/direct_backend.c:172) on the same mesh: the same GMRES iteration count
+    and the printed energy to its last digit."""
+    meta = golden_meta[name]
+    ref = solve_meta["direct"][name]
+    out = run_dropin(os.path.join(case_dir, name), meta["opts"], extra=["-r=1"])
+    assert "unavailable" not in out and "CPU fallback" not in out, out
+    e, it = parse(out)
+    assert it == ref["iterations"]
+    assert abs(e - ref["energy"]) <= 2e-6 + 1e-8 * abs(e)
+
+
+@pytest.mark.skipif(not os.path.exists(DROPIN), reason="drop-in binary not built (make -C oracle dropin)")
+def test_dropin_direct_mode_with_gpu_precond(case_dir, golden_meta, solve_meta):
+    """-r=1 with the reference's GPU preconditioner block builder
+    (gpuBuildPrecondDisjointBlock, which evaluates the transposed disjoint
+    pairs, so the preconditioner differs slightly from the host's): no CPU
+    fallback, and the energy of the direct solve within the solver tolerance
+    of the reference's -r=2 energy."""
     name = "sphere320"
     meta = golden_meta[name]
     out = run_dropin(os.path.join(case_dir, name), meta["opts"], extra=["-r=1"],
                      env_extra={"FABIPB_GPU_PRECOND_BUILD_DISJOINT": "1"})
-    assert "unavailable" not in out, out
+    assert "unavailable" not in out and "CPU fallback" not in out, out
     e, it = parse(out)
-    assert e is not None and abs(e - meta["solve"]["energy"]) < 2e-2 * abs(meta["solve"]["energy"])
+    ref = solve_meta["direct"][name]["energy"]
+    assert e is not None and abs(e - ref) <= 1e-4 * abs(ref)

@@ -105,3 +105,11 @@ def test_oracle_matches_live_reference(case_dir, golden_meta, oracles, tmp_path)
     O.run_ref_harness("matvec", os.path.join(case_dir, name), pre,
                       make_golden.ref_opts(golden_meta[name]["opts"]), sigma=sg)
     assert np.array_equal(O.read_bin(pre, "pot", np.float64), orc.matvec(sg))
+
+
+@pytest.mark.parametrize("name", ["sphere20480", "shell16384"])
+def test_large_case_meshes_match_golden_digests(name, tmp_path, solve_meta):
+    """The generator still writes the meshes the reference solved for the
+    solve-only goldens (a generator change shows here, not as a solver diff)."""
+    base = make_golden.generate_mesh(name, str(tmp_path))
+    assert make_golden.mesh_digest(base) == solve_meta[name]["digest"]
