@@ -78,15 +78,22 @@ CASES = {
     "shell8388608": ("shell", dict(freq=724, r_in=400.0, r_out=440.0, n_charges=2000000, seed=4),
                      dict(order=5, depth=6, sep_ratio=0.6, eps1=2.0, eps2=80.0, tol=1e-6, restart=10, maxit=100,
                           precond=3)),
+    # the two-shell configuration's leaf structure at a quarter of its size (radii 100/115 A,
+    # 524,176 triangles, depth 4: mean leaf 300, max 1219), for kernel profiles
+    "shell524176": ("shell", dict(freq=181, r_in=100.0, r_out=115.0, n_charges=125000, seed=13),
+                    dict(order=5, depth=4, sep_ratio=0.6, eps1=2.0, eps2=80.0, tol=1e-6, restart=10, maxit=100,
+                         precond=3)),
     "sphere20480": ("sphere", dict(nsub=5, radius=20.0, n_charges=500, seed=0),
                     dict(order=3, depth=3, sep_ratio=0.8, eps1=1.0, eps2=80.0, tol=1e-4, restart=10, maxit=100,
                          precond=2)),
 }
 PANELS = {"shell2097152": 2096704, "star204800": 204800, "star2097152": 2097152, "shell8388608": 8386816,
-          "sphere20480": 20480}
+          "shell524176": 524176, "sphere20480": 20480}
 DEFAULT_CASE = "shell2097152"
 METRIC = "matvec/s"
 FLOP_PER_PAIR = 60.0   # algorithmic count per near panel pair (KER4 + apply)
+# a workload too large for a full ncu capture -> (the captured case, panel ratio)
+PROFILE_PROXY = {"shell2097152": (("shell524176", 2096704 / 524176),)}
 DIRECT_ORACLE_MAX = 300000   # panels up to which the FP64 direct-summation oracle is solved
 SAMPLE_ABOVE = 500000        # panels above which the CPU reference matvec is sampled
 
@@ -625,15 +632,21 @@ def run_ours(args):
     else:
         peak, bound = fp64_peak, "fp64"
         peak_src = "measured FP64 FMA rate of this GPU (DFMA chains, fabipb_b200_simt_peak)"
-    traffic = None
-    # DRAM bytes per launch from the committed ncu summary of this kernel and workload
+    # DRAM bytes per launch from the committed ncu summary of this kernel and
+    # workload, or of the smaller capture that stands in for it, scaled by panels
     kname = "near_apply_f2_kernel<0>" if prec == lib.MIXED else "near_apply_kernel<double,0>"
-    tname = "%s_%s.md" % ("near_apply_f2_kernel" if prec == lib.MIXED else "near_apply_kernel_double", args.case)
-    prof = os.path.join(ROOT, "profiles", tname)
-    if os.path.exists(prof):
-        with open(prof) as fp:
-            m = re.search(r"dram_bytes_per_launch \| (\d+)", fp.read())
-        traffic = int(m.group(1)) if m else None
+    kfile = "near_apply_f2_kernel" if prec == lib.MIXED else "near_apply_kernel_double"
+    traffic, traffic_src = None, None
+    for case, scale in ((args.case, 1.0),) + tuple(PROFILE_PROXY.get(args.case, ())):
+        prof = os.path.join(ROOT, "profiles", "%s_%s.md" % (kfile, case))
+        if os.path.exists(prof):
+            with open(prof) as fp:
+                m = re.search(r"dram_bytes_per_launch \| (\d+)", fp.read())
+            if m:
+                traffic = int(int(m.group(1)) * scale)
+                traffic_src = "ncu capture of %s%s" % (case, "" if scale == 1.0 else
+                                                       ", scaled by panels (x%.2f)" % scale)
+                break
     passes = pass_report(surf, info, x.data_ptr(), flush, args.steps, prec == lib.MIXED, fp32_peak, fp64_peak)
     free, total = torch.cuda.mem_get_info()
     mem_ctx = (total - free) / 2**30
@@ -683,7 +696,7 @@ def run_ours(args):
                 "d2h_bytes_per_step": n2 * 8, "path": "fabipb_b200_matvec, pinned host x and y"},
         "e2e_dropin": dropin,
         "roofline": {"kernel": kname, "bound": bound, "achieved": achieved, "peak": peak,
-                     "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+                     "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_src,
                      "peak_source": peak_src, "flop_per_pair": FLOP_PER_PAIR,
                      "pairs_per_launch": pairs, "launch_ms": near_s * 1000.0},
         "peaks": {"fp32_tflops": fp32_peak, "fp64_tflops": fp64_peak, "hbm_gbs": measured_hbm_gbs()[0]},
@@ -721,7 +734,7 @@ def main():
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 operator's matvec rate")
     ap.add_argument("--no-direct-oracle", action="store_true", help="skip the FP64 direct-summation oracle solve")
     ap.add_argument("--no-solve", action="store_true", help="skip the mixed/FP64 solve report")
-    ap.add_argument("--solve-reps", type=int, default=2, help="reported runs per precision (after one warm-up run)")
+    ap.add_argument("--solve-reps", type=int, default=3, help="reported runs per precision (after one warm-up run)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the forward/backward gradient timing")
     args = ap.parse_args()
     if args.impl == "reference":
