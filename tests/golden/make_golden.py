@@ -2,6 +2,7 @@
 
     python tests/golden/make_golden.py            # the small cases (cases.json, *.npz)
     python tests/golden/make_golden.py --large    # solve-only goldens (solve_cases.json)
+    python tests/golden/make_golden.py --fd       # the reference's energy gradient by FD (fd_star2048.json)
 
 Needs the reference CPU solver compiled from its own sources
 (``make -C oracle ref``, which reads the read-only reference mount).  For each
@@ -125,12 +126,75 @@ def main_large():
         json.dump(out, fp, indent=1, sort_keys=True)
 
 
+# Central finite differences of the reference CLI's own energy on star2048:
+# every charge-tree cluster opened (FABIPB_ENERGY_TREE_THETA=1e-9, so the
+# energy is the direct panel-charge sum), GMRES to 1e-12, the charges written
+# with ten decimals.  Step 1e-5 e for a charge, 1e-4 A for a position (the
+# configuration's steps); the printed energy has six decimals (kcal/mol).
+FD_CASE = "star2048"
+FD_CHARGES = 4
+FD_SEED = 21
+FD_HQ, FD_HX = 1e-5, 1e-4
+
+
+def write_pqr(path, ch):
+    with open(path, "w") as fp:
+        for i, (p, c, r) in enumerate(zip(ch.pos, ch.q, ch.radius)):
+            fp.write("ATOM %d C ALA A 1 %.10f %.10f %.10f %.10f %.4f\n" % (i + 1, p[0], p[1], p[2], c, r))
+
+
+def fd_charges(n_charges):
+    return sorted(int(k) for k in np.random.default_rng(FD_SEED).choice(n_charges, size=FD_CHARGES, replace=False))
+
+
+def main_fd():
+    """fd_star2048.json: the reference's central differences of its energy."""
+    from fabipb_b200 import meshio
+    from oracle import oracle as O
+    opts = dict(CASES[FD_CASE][2], o=1e-12)
+    env = {"FABIPB_ENERGY_TREE_THETA": "1e-9"}
+    out = {"case": FD_CASE, "hq": FD_HQ, "hx": FD_HX, "charges": {}}
+    with tempfile.TemporaryDirectory() as tmp:
+        base = generate_mesh(FD_CASE, tmp)
+        pan, ch = meshio.load_case(base)
+        write_pqr(base + ".pqr", ch)   # ten decimals: the perturbed files below differ only in one value
+
+        def energy(c):
+            write_pqr(base + ".pqr", c)
+            e, it, res, _ = O.run_ref_solve(base, ref_opts(opts, True), threads=os.cpu_count(), extra_env=env)
+            return e
+
+        out["energy"] = energy(ch)
+        for k in fd_charges(len(ch.q)):
+            rec = {}
+            q = ch.q.copy()
+            q[k] += FD_HQ
+            ep = energy(meshio.ChargeSet(ch.pos, q, ch.radius))
+            q[k] -= 2 * FD_HQ
+            em = energy(meshio.ChargeSet(ch.pos, q, ch.radius))
+            rec["dq"] = (ep - em) / (2 * FD_HQ)
+            rec["dx"] = []
+            for a in range(3):
+                pos = ch.pos.copy()
+                pos[k, a] += FD_HX
+                ep = energy(meshio.ChargeSet(pos, ch.q, ch.radius))
+                pos[k, a] -= 2 * FD_HX
+                em = energy(meshio.ChargeSet(pos, ch.q, ch.radius))
+                rec["dx"].append((ep - em) / (2 * FD_HX))
+            out["charges"][str(k)] = rec
+            print(k, rec, flush=True)
+    with open(os.path.join(HERE, "fd_star2048.json"), "w") as fp:
+        json.dump(out, fp, indent=1, sort_keys=True)
+
+
 def main():
     from oracle import oracle as O
     if not O.ref_available():
         raise SystemExit("build the reference first: make -C oracle ref")
     if "--large" in sys.argv:
         return main_large()
+    if "--fd" in sys.argv:
+        return main_fd()
     meta = {}
     with tempfile.TemporaryDirectory() as tmp:
         for name, (_, _, opts) in CASES.items():
