@@ -388,7 +388,7 @@ def _ev():
     return torch.cuda.Event(enable_timing=True)
 
 
-def solve_report(pan, ch, name, opts, device, st, reps=3, adjoint=True):
+def solve_report(pan, ch, name, opts, device, st, reps=3, adjoint=True, fp64_adjoint=True):
     """Full solves of the case in both precisions, every vector on the device:
     RHS (direct, or the charge-tree treecode above 2e11 panel-charge pairs as
     the reference's GPU policy), the case's preconditioner, GMRES from x0 = b
@@ -452,7 +452,7 @@ def solve_report(pan, ch, name, opts, device, st, reps=3, adjoint=True):
             r["refined"] = {"gmres_s": rf[0].elapsed_time(rf[1]) / 1000.0, "outer": outer, "iterations": itr,
                             "residual_fp64": resr, "info": infr, "energy_kcal_mol": er}
             r["refined"]["solve_s"] = r["setup_s"] + r["refined"]["gmres_s"] + r["energy_s"]
-        if adjoint:
+        if adjoint and (fp64_adjoint or tag == "mixed"):
             # gradients of the (direct) energy: forward = direct RHS + GMRES +
             # direct energy, backward = adjoint GMRES + dE/dq, dE/dx of every charge
             ag = [_ev() for _ in range(3)]
@@ -467,6 +467,11 @@ def solve_report(pan, ch, name, opts, device, st, reps=3, adjoint=True):
             r["adjoint"] = {"forward_s": fs, "backward_s": bs, "backward_over_forward": bs / fs,
                             "forward_iterations": itf, "backward_iterations": itb, "info": [inff, infb],
                             "charges": int(len(ch.q)), "energy_direct_kcal_mol": ef * kcal}
+        # the pool keeps freed blocks (release threshold at its maximum), so memory in use
+        # at the end of the run is the high-water mark of the run's allocations
+        torch.cuda.synchronize()
+        free, total = torch.cuda.mem_get_info()
+        r["device_mem_high_water_gib"] = (total - free) / 2**30
         s.close()
         runs[tag].append(r)
     med = lambda v: float(np.median(v))
@@ -482,7 +487,7 @@ def solve_report(pan, ch, name, opts, device, st, reps=3, adjoint=True):
             for k in ("gmres_s", "solve_s"):
                 r["refined"][k] = med([q["refined"][k] for q in rs])
                 r["refined"][k + "_runs"] = [q["refined"][k] for q in rs]
-        if adjoint:
+        if "adjoint" in rs[-1]:
             a = dict(rs[-1]["adjoint"])
             for k in ("forward_s", "backward_s"):
                 a[k] = med([q["adjoint"][k] for q in rs])
@@ -491,6 +496,7 @@ def solve_report(pan, ch, name, opts, device, st, reps=3, adjoint=True):
             r["adjoint"] = a
         r["runs"] = len(rs)
         r["device_mem_gib"] = mem_peak[tag]
+        r["device_mem_high_water_gib"] = max(q["device_mem_high_water_gib"] for q in rs)
         out[tag] = r
     m, f = out["mixed"], out["fp64"]
     rel = lambda a, b: abs(a - b) / abs(b)
@@ -670,7 +676,7 @@ def run_ours(args):
     if not args.no_solve:
         with ClockSampler(local) as clk2:   # the clocks during the solves too
             solve = solve_report(pan, ch, name, opts, local, stream, reps=args.solve_reps,
-                                 adjoint=not args.no_adjoint)
+                                 adjoint=not args.no_adjoint, fp64_adjoint=not args.no_fp64_adjoint)
             if PANELS[name] <= DIRECT_ORACLE_MAX and not args.no_direct_oracle:
                 en = {"mixed": solve["mixed"]["energy_kcal_mol"], "refined": solve["mixed"]["refined"]["energy_kcal_mol"],
                       "fp64": solve["fp64"]["energy_kcal_mol"]}
@@ -736,6 +742,7 @@ def main():
     ap.add_argument("--no-solve", action="store_true", help="skip the mixed/FP64 solve report")
     ap.add_argument("--solve-reps", type=int, default=3, help="reported runs per precision (after one warm-up run)")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the forward/backward gradient timing")
+    ap.add_argument("--no-fp64-adjoint", action="store_true", help="time the gradients of the mixed context only")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
