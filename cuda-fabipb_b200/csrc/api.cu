@@ -125,18 +125,29 @@ Context::~Context() {
   if (ownStream && stream) cudaStreamDestroy(stream);
 }
 
+bool build_panel_tree_device(Context &c, const double *vtxIn, const double *nrmIn, const double *areaIn);
+
+// The panel tree on the device (tree_dev.cu), which also leaves the panels in
+// tree order on the device; FABIPB_B200_HOST_TREE=1 builds it on the host
+// threads instead (tree.cpp; the tests compare the two).
 bool setup_geometry(Context &c, const double *vtx, const double *nrm, const double *area) {
   const int n = c.n;
   StageTimer tm("create", c.stream);
-  if (!build_panel_tree(c.pt, n, vtx, c.prm.depth, c.prm.height, c.prm.sep_ratio, c.prm.order,
-                        c.prm.order_mom))
-    return false;
-  tm.mark("octree_host");
+  const bool hostTree = getenv("FABIPB_B200_HOST_TREE") != nullptr;
+  if (!hostTree) {
+    if (!build_panel_tree_device(c, vtx, nrm, area)) return false;
+    tm.mark("octree_device");
+  } else {
+    if (!build_panel_tree(c.pt, n, vtx, c.prm.depth, c.prm.height, c.prm.sep_ratio, c.prm.order,
+                          c.prm.order_mom))
+      return false;
+    tm.mark("octree_host");
+  }
   const PanelTree &pt = c.pt;
-  c.h_vtx.resize(9 * (size_t)n);
-  c.h_nrm.resize(3 * (size_t)n);
-  c.h_area.resize(n);
-  {   // the panels in tree order, gathered on host threads
+  if (hostTree) {   // the panels in tree order, gathered on host threads
+    c.h_vtx.resize(9 * (size_t)n);
+    c.h_nrm.resize(3 * (size_t)n);
+    c.h_area.resize(n);
     auto gather = [&](int i0, int i1) {
       for (int i = i0; i < i1; i++) {
         int o = pt.order[i];
@@ -158,8 +169,10 @@ bool setup_geometry(Context &c, const double *vtx, const double *nrm, const doub
     for (int k = 0; k < 3; k++) leafCtr[3 * (size_t)L + k] = pt.t.x[3 * (size_t)pt.leafCube[L] + k];
   }
   cudaStream_t s = c.stream;
-  if (!c.arena.upload(&c.d_vtx, c.h_vtx, s) || !c.arena.upload(&c.d_nrm, c.h_nrm, s) ||
-      !c.arena.upload(&c.d_area, c.h_area, s) || !c.arena.upload(&c.d_leafStart, pt.leafStart, s) ||
+  if (hostTree && (!c.arena.upload(&c.d_vtx, c.h_vtx, s) || !c.arena.upload(&c.d_nrm, c.h_nrm, s) ||
+                   !c.arena.upload(&c.d_area, c.h_area, s)))
+    return false;
+  if (!c.arena.upload(&c.d_leafStart, pt.leafStart, s) ||
       !c.arena.upload(&c.d_leafCount, pt.leafCount, s) || !c.arena.upload(&c.d_leafOfPanel, leafOf, s) ||
       !c.arena.upload(&c.d_nearOff, pt.nearOff, s) || !c.arena.upload(&c.d_nearSrc, pt.nearSrc, s) ||
       !c.arena.upload(&c.d_leafCtr, leafCtr, s))
@@ -208,6 +221,10 @@ __global__ void direct_combine_kernel(int n, const double *__restrict__ area, co
 #ifndef FB_FAR_PRIORITY
 #define FB_FAR_PRIORITY 1
 #endif
+// the far chain queued before the near field (1) or after it (0)
+#ifndef FB_FAR_FIRST
+#define FB_FAR_FIRST 0
+#endif
 // y = alpha*(D - K)x + beta*y, D = diag(s1*A, s2*A) (MtVmain); adjoint: (D - K^T)
 bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y, bool adjoint, bool fp64) {
   double s1 = (1.0 + c.epsilon) / 2.0 * alpha;
@@ -222,8 +239,10 @@ bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y
   // the near field on the side stream, into d_nearOut, beside the far passes
   FB_CUDA(cudaEventRecord(c.evFork, c.stream));
   FB_CUDA(cudaStreamWaitEvent(c.sideStream, c.evFork, 0));
+#if !FB_FAR_FIRST
   if (!launch_near(c, x, -alpha, c.d_nearOut, adjoint, fp64, c.sideStream, false)) return false;
   FB_CUDA(cudaEventRecord(c.evJoin, c.sideStream));
+#endif
 #if FB_FAR_PRIORITY
   // the far passes on the high-priority stream (the launch helpers use c.stream)
   FB_CUDA(cudaStreamWaitEvent(c.farStream, c.evFork, 0));
@@ -236,6 +255,12 @@ bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y
   FB_CUDA(cudaStreamWaitEvent(c.stream, c.evFar, 0));
 #else
   if (!launch_far_upward(c, x, adjoint, nullptr, fp64)) return false;
+#endif
+#if FB_FAR_FIRST
+  // queued after the far chain, so the chain's first blocks take SMs before
+  // the near field's grid fills them
+  if (!launch_near(c, x, -alpha, c.d_nearOut, adjoint, fp64, c.sideStream, false)) return false;
+  FB_CUDA(cudaEventRecord(c.evJoin, c.sideStream));
 #endif
   FB_CUDA(cudaStreamWaitEvent(c.stream, c.evJoin, 0));
   if (!launch_l2p(c, -alpha, beta, y, x, s1, s2, adjoint, c.d_nearOut, fp64)) return false;

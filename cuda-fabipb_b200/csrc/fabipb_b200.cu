@@ -5,6 +5,7 @@
 #include "fmm.cu"
 #include "charges.cu"
 #include "solver.cu"
+#include "tree_dev.cu"
 #include "api.cu"
 #include "abi.cu"
 #include "adjoint.cu"

@@ -555,11 +555,15 @@ struct Vec2<float> {
 // the per-coefficient sums across batches are always FP64.
 // TSMEM (order 5): the tensors of the batch's 32 pairs are staged in shared
 // memory next to the moments instead of being held in registers.
+// FP32 order-5 tensors held in registers (1) or staged in shared memory (0)
+#ifndef FB_M2L_TREG_F32
+#define FB_M2L_TREG_F32 0
+#endif
 template <int PM, typename TV = double>
 struct M2LUnrolledShape {
   typedef typename Vec2<TV>::t V2;
   static constexpr int NMP = nmom_c(PM);
-  static constexpr bool TSMEM = PM >= 5;
+  static constexpr bool TSMEM = PM >= 5 && !(FB_M2L_TREG_F32 && sizeof(TV) == 4);
   static constexpr int W = TSMEM ? (sizeof(TV) == 8 ? 1 : 2) : 4;   // warps per block
   static constexpr size_t colBytes = (size_t)NMP * 32 * sizeof(V2);   // moment columns (and tensor columns)
   static constexpr size_t warpBytes = (TSMEM ? 2 : 1) * colBytes + 4 * NMP * sizeof(double);   // + [4][NMP] sums

@@ -731,6 +731,11 @@ static bool special_pairs_host(Context &c, const std::vector<int> &nearSortedFla
   const PanelTree &pt = c.pt;
   const int n = c.n;
   cudaStream_t s = c.stream;
+  if (c.h_vtx.size() != 9 * (size_t)n) {   // the device tree keeps the tree-order panels on the device only
+    c.h_vtx.resize(9 * (size_t)n);
+    FB_CUDA(cudaMemcpyAsync(c.h_vtx.data(), c.d_vtx, 9 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    FB_CUDA(cudaStreamSynchronize(s));
+  }
   std::unordered_map<VKey, int, VKeyHash> vid;
   vid.reserve((size_t)n * 2);
   std::vector<int> pv(3 * (size_t)n);

@@ -309,7 +309,14 @@ bool build_panel_tree(PanelTree &pt, int n, const double *vtx, int depth, int he
   ht.mark("boxes");
   octree_neighbours(pt.t, sep_ratio);
   ht.mark("neighbours");
+  if (!finish_panel_tree(pt, order, order_mom)) return false;
+  ht.mark("layouts");
+  return true;
+}
+
+bool finish_panel_tree(PanelTree &pt, int order, int order_mom) {
   Octree &t = pt.t;
+  const int depth = t.depth, height = t.height;
 
   // getOrders (gkSetup.c:42-81)
   pt.ordMom.assign(depth + 1, 0);
@@ -394,7 +401,6 @@ bool build_panel_tree(PanelTree &pt, int n, const double *vtx, int depth, int he
     }
   }
   pt.m2lOff[pt.nFmm] = (int)pt.m2lSrc.size();
-  ht.mark("layouts");
   return true;
 }
 

@@ -58,5 +58,8 @@ struct PanelTree {
 
 bool build_panel_tree(PanelTree &pt, int n, const double *vtx, int depth, int height,
                       double sep_ratio, int order, int order_mom);
+// the expansion orders and the flattened layouts (near pairs by leaf, FMM
+// cube order, M2L lists) from a finished octree and panel order
+bool finish_panel_tree(PanelTree &pt, int order, int order_mom);
 
 }  // namespace fb

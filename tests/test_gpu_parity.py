@@ -55,6 +55,31 @@ def test_tree_matches_reference(name, case_dir, golden_meta):
     assert np.array_equal(lev, g["cubeLevel"]) and np.array_equal(ctr.reshape(-1), g["cubeCtr"])
 
 
+def _tree_arrays(s):
+    lev, ctr = s.cube_data()
+    return [s.panel_order(), *s.leaf_layout(), *s.near_pairs(), *s.m2l_pairs(), lev, ctr]
+
+
+@pytest.mark.parametrize("name", CASES + ["star204800", "shell16384"])
+def test_device_tree_matches_host_tree(name, case_dir, golden_meta, tmp_path, monkeypatch):
+    """The octree built on the device (cell keys, stable radix sort, key-prefix
+    cubes, boxes, MAC lists) equals the host build bit for bit: panel order,
+    leaves, near and M2L lists, box centres and radii -- on the golden cases
+    and on two larger meshes (the 204,800-panel star, the 16,384-panel
+    two-shell surface)."""
+    if name in golden_meta:
+        base, opts = os.path.join(case_dir, name), golden_meta[name]["opts"]
+    else:
+        base, opts = make_golden.generate_mesh(name, str(tmp_path)), make_golden.SOLVE_CASES[name][2]
+    pan, _ = meshio.load_case(base)
+    prm = lib.params(precision=lib.FP64, **case_params(opts))
+    dev = _tree_arrays(lib.Surface(pan, prm))
+    monkeypatch.setenv("FABIPB_B200_HOST_TREE", "1")
+    host = _tree_arrays(lib.Surface(pan, prm))
+    for a, b in zip(dev, host):
+        assert a.shape == b.shape and np.array_equal(a, b)
+
+
 @pytest.mark.parametrize("name", CASES)
 @pytest.mark.parametrize("precision,tol", [(lib.FP64, 1e-12), (lib.MIXED, 5e-6)])
 def test_near_field(name, precision, tol, case_dir, golden_meta):
