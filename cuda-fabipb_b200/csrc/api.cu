@@ -221,10 +221,6 @@ __global__ void direct_combine_kernel(int n, const double *__restrict__ area, co
 #ifndef FB_FAR_PRIORITY
 #define FB_FAR_PRIORITY 1
 #endif
-// the far chain queued before the near field (1) or after it (0)
-#ifndef FB_FAR_FIRST
-#define FB_FAR_FIRST 0
-#endif
 // y = alpha*(D - K)x + beta*y, D = diag(s1*A, s2*A) (MtVmain); adjoint: (D - K^T)
 bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y, bool adjoint, bool fp64) {
   double s1 = (1.0 + c.epsilon) / 2.0 * alpha;
@@ -239,10 +235,8 @@ bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y
   // the near field on the side stream, into d_nearOut, beside the far passes
   FB_CUDA(cudaEventRecord(c.evFork, c.stream));
   FB_CUDA(cudaStreamWaitEvent(c.sideStream, c.evFork, 0));
-#if !FB_FAR_FIRST
   if (!launch_near(c, x, -alpha, c.d_nearOut, adjoint, fp64, c.sideStream, false)) return false;
   FB_CUDA(cudaEventRecord(c.evJoin, c.sideStream));
-#endif
 #if FB_FAR_PRIORITY
   // the far passes on the high-priority stream (the launch helpers use c.stream)
   FB_CUDA(cudaStreamWaitEvent(c.farStream, c.evFork, 0));
@@ -255,12 +249,6 @@ bool op_matvec(Context &c, double alpha, const double *x, double beta, double *y
   FB_CUDA(cudaStreamWaitEvent(c.stream, c.evFar, 0));
 #else
   if (!launch_far_upward(c, x, adjoint, nullptr, fp64)) return false;
-#endif
-#if FB_FAR_FIRST
-  // queued after the far chain, so the chain's first blocks take SMs before
-  // the near field's grid fills them
-  if (!launch_near(c, x, -alpha, c.d_nearOut, adjoint, fp64, c.sideStream, false)) return false;
-  FB_CUDA(cudaEventRecord(c.evJoin, c.sideStream));
 #endif
   FB_CUDA(cudaStreamWaitEvent(c.stream, c.evJoin, 0));
   if (!launch_l2p(c, -alpha, beta, y, x, s1, s2, adjoint, c.d_nearOut, fp64)) return false;

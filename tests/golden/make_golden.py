@@ -128,9 +128,12 @@ def main_large():
 
 # Central finite differences of the reference CLI's own energy on star2048:
 # every charge-tree cluster opened (FABIPB_ENERGY_TREE_THETA=1e-9, so the
-# energy is the direct panel-charge sum), GMRES to 1e-12, the charges written
-# with ten decimals.  Step 1e-5 e for a charge, 1e-4 A for a position (the
-# configuration's steps); the printed energy has six decimals (kcal/mol).
+# panel-tree energy is the direct panel-charge sum), GMRES to 1e-12, the
+# charges written with ten decimals, the raw energy read at full precision
+# from the CLI's energy-compare line (FABIPB_ENERGY_MODE=compare,
+# src/fabipb.c:1172-1181).  Step 1e-5 e for a charge, 1e-4 A for a position
+# (the configuration's steps); values in raw energy units (kcal/mol over
+# 2 pi 332.0716).
 FD_CASE = "star2048"
 FD_CHARGES = 4
 FD_SEED = 21
@@ -152,8 +155,8 @@ def main_fd():
     from fabipb_b200 import meshio
     from oracle import oracle as O
     opts = dict(CASES[FD_CASE][2], o=1e-12)
-    env = {"FABIPB_ENERGY_TREE_THETA": "1e-9"}
-    out = {"case": FD_CASE, "hq": FD_HQ, "hx": FD_HX, "charges": {}}
+    env = {"FABIPB_ENERGY_TREE_THETA": "1e-9", "FABIPB_ENERGY_MODE": "compare"}
+    out = {"case": FD_CASE, "hq": FD_HQ, "hx": FD_HX, "units": "raw energy", "charges": {}}
     with tempfile.TemporaryDirectory() as tmp:
         base = generate_mesh(FD_CASE, tmp)
         pan, ch = meshio.load_case(base)
@@ -161,10 +164,11 @@ def main_fd():
 
         def energy(c):
             write_pqr(base + ".pqr", c)
-            e, it, res, _ = O.run_ref_solve(base, ref_opts(opts, True), threads=os.cpu_count(), extra_env=env)
-            return e
+            _, _, _, out = O.run_ref_solve(base, ref_opts(opts, True), threads=os.cpu_count(), extra_env=env)
+            line = [l for l in out.splitlines() if l.startswith("Energy compare:")][0]
+            return float(line.split("panel-tree raw=")[1].split()[0])
 
-        out["energy"] = energy(ch)
+        out["energy_raw"] = energy(ch)
         for k in fd_charges(len(ch.q)):
             rec = {}
             q = ch.q.copy()

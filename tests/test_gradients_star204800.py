@@ -13,8 +13,8 @@ reference's own finite differences.
   truncation only (p=4, MAC 0.7: energy 1.7e-4, dE/dq 1.7e-3 relative).
 * On star2048, the library's gradients against central differences of the
   reference CLI's own energy (tests/golden/fd_star2048.json, written by
-  make_golden.py --fd: direct energy, GMRES to 1e-12, printed to 1e-6
-  kcal/mol, hence the looser tolerance).
+  make_golden.py --fd: direct energy, GMRES to 1e-12, raw energies at full
+  precision).
 
 The energy differentiated is the direct panel-charge sum E = e(q, r) . sigma
 with (D - K) sigma = b(q, r) (fabipb_b200_forward / _backward).
@@ -138,13 +138,14 @@ def test_gradients_match_reference_finite_differences(case_dir, golden_meta):
     s.precond_setup(2)
     e, it, res, info = s.forward(**TIGHT)
     assert info == 0
-    assert abs(e * KCAL - fd["energy"]) <= 2e-6 + 1e-8 * abs(fd["energy"])
+    assert abs(e - fd["energy_raw"]) <= 1e-10 * abs(fd["energy_raw"])
     dq, dx, it2, res2, info2 = s.backward(1.0, **TIGHT)
     assert info2 == 0
     for k, rec in fd["charges"].items():
         k = int(k)
-        # printed energies resolve 1e-6 kcal/mol: 0.05 (charge) and 5e-3 (position) in the differences
-        assert abs(dq[k] * KCAL - rec["dq"]) <= 1e-4 * abs(rec["dq"]) + 0.1, (k, dq[k] * KCAL, rec["dq"])
+        # E is quadratic in q: the charge differences are exact up to rounding;
+        # positions: O(h^2) truncation and the solves' rounding over h
+        assert abs(dq[k] - rec["dq"]) <= 1e-7 * abs(rec["dq"]), (k, dq[k], rec["dq"])
+        scale = max(abs(v) for v in rec["dx"])
         for a in range(3):
-            assert abs(dx[k, a] * KCAL - rec["dx"][a]) <= 1e-3 * abs(rec["dx"][a]) + 1e-2, \
-                (k, a, dx[k, a] * KCAL, rec["dx"][a])
+            assert abs(dx[k, a] - rec["dx"][a]) <= 1e-4 * scale, (k, a, dx[k, a], rec["dx"][a])
