@@ -345,7 +345,8 @@ near_apply_f2_kernel(int nWork, const int2 *__restrict__ work, const int *__rest
                      const float4 *__restrict__ srcA, const float4 *__restrict__ srcB,
                      const int *__restrict__ spOff, const int *__restrict__ spSrc, const double4 *__restrict__ spK,
                      const double *__restrict__ sgm, const double *__restrict__ area, int n, float kappa, float kexp,
-                     float eps, float ieps, float kap2, double coef, int accumulate, double *out) {
+                     float eps, float ieps, float kap2, double coef, int accumulate, double *out,
+                     const int *__restrict__ symOff, const float2 *__restrict__ symScr) {
   __shared__ float4 sP[kNearWarps][16][4];
   __shared__ float sR[kNearWarps][2][32];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -367,6 +368,17 @@ near_apply_f2_kernel(int nWork, const int2 *__restrict__ work, const int *__rest
   float *pf = reinterpret_cast<float *>(&sP[warp][lane >> 1][0]) + (lane & 1);
   const int p1 = nearOff[L + 1];
   for (int p = nearOff[L]; p < p1; p++) {
+    if (symOff) {   // a leaf pair of the symmetric kernel: its sums for this target are in the scratch
+      const int o = symOff[p];
+      if (o >= 0) {   // warp-uniform
+        if (valid && sub == 0) {
+          const float2 v = symScr[o + (X - base)];
+          acc0.x += v.x;
+          acc1.x += v.y;
+        }
+        continue;
+      }
+    }
     const int S = nearSrc[p];
     const int sb = leafStart[S], sc = leafCount[S];
     const float2 tx = f2(tp.x + (float)(cx - leafCtr[3 * S]));
@@ -417,6 +429,145 @@ near_apply_f2_kernel(int nWork, const int2 *__restrict__ work, const int *__rest
   const double v0 = coef * (AX * (double)s0 + e0), v1 = coef * (AX * (double)s1 + e1);
   out[X] = accumulate ? out[X] + v0 : v0;   // each output has exactly one writer
   out[X + n] = accumulate ? out[X + n] + v1 : v1;
+}
+
+// ---------------------------------------------------------------------------
+// Symmetric near field (FP32, packed f32x2; mixed contexts, forward operator).
+// The one-point pair term of K(X, Y) and that of K(Y, X) share r, 1/r,
+// e^{-kappa r}, (kappa r + 1) e^{-kappa r}, n_X.n_Y and the double-layer
+// factors; with d = x_X - x_Y, swapping the panels negates d, so
+//   t1(Y,X) = -t2(X,Y),  t2(Y,X) = -t1(X,Y),  u, dd, y0, y3 unchanged,
+//   K(Y,X): out_pot  += y0 wa_X - t2 (eps c - 1) wb_X,
+//           out_dpdn += -t1 (c/eps - 1) wa_X + y3 wb_X.
+// So every unordered pair of distinct near leaves (R, T) is evaluated once
+// for both directions.  One warp per leaf pair: the 32-panel groups of R in
+// registers (lane = target), T in tiles of 32 staged in shared memory.  In
+// step s of a tile, lane t takes the tile's sources (t + s) and (t + s + 16)
+// (mod 32), so at every step the 32 lanes hold 32 distinct sources and each
+// source's contribution from the lane's target goes to the lane that owns that
+// source by two shuffles; after 16 steps every source has had all 32 targets.
+// The sums go to a scratch slot per (ordered leaf pair, panel); the ordered
+// near-field kernel adds them, in its near-list order, to its own FP32 sums
+// (deterministic: no atomics).  Self pairs and pairs with a small leaf stay in
+// the ordered kernel.
+// ---------------------------------------------------------------------------
+#ifndef FB_NEAR_SYM_MIN_BLOCKS
+#define FB_NEAR_SYM_MIN_BLOCKS 6
+#endif
+// leaf pairs whose smaller leaf has fewer panels stay in the ordered kernel
+#ifndef FB_NEAR_SYM_MIN_LEAF
+#define FB_NEAR_SYM_MIN_LEAF 24
+#endif
+constexpr int kSymWarps = 4;
+
+__device__ __forceinline__ void near_sym_pair2(const float4 A, const float4 B, const float4 C, const float4 D,
+                                               float2 tx, float2 ty, float2 tz, float2 tnx, float2 tny, float2 tnz,
+                                               float2 wat, float2 wbt, float2 watn, float2 wbtn, float kappa,
+                                               float kexp, float eps, float ieps, float kap2, float2 &acc0,
+                                               float2 &acc1, float2 &s0, float2 &s1) {
+  const float2 one = f2(1.f), m1 = f2(-1.f);
+  const float2 dx = __fadd2_rn(tx, make_float2(A.x, A.y));
+  const float2 dy = __fadd2_rn(ty, make_float2(A.z, A.w));
+  const float2 dz = __fadd2_rn(tz, make_float2(B.x, B.y));
+  const float2 wa = make_float2(B.z, B.w), wb = make_float2(D.z, D.w);
+  const float2 nx = make_float2(C.x, C.y), ny = make_float2(C.z, C.w), nz = make_float2(D.x, D.y);
+  const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+  float2 g;   // distinct leaves: distinct panel centroids, r > 0
+  g.x = rsqrt_t(r2.x);
+  g.y = rsqrt_t(r2.y);
+  const float2 r = __fmul2_rn(r2, g);
+  const float2 ea = __fmul2_rn(f2(kexp), r);
+  float2 e;
+  e.x = expneg_t(1.f, ea.x);
+  e.y = expneg_t(1.f, ea.y);
+  const float2 c = __fmul2_rn(__ffma2_rn(f2(kappa), r, one), e);    // (kappa r + 1) e^{-kappa r}
+  const float2 g2 = __fmul2_rn(g, g), h = __fmul2_rn(g2, g);
+  const float2 ipX = __ffma2_rn(tnz, dz, __ffma2_rn(tny, dy, __fmul2_rn(tnx, dx)));   // n_X.d
+  const float2 ipY = __ffma2_rn(nz, dz, __ffma2_rn(ny, dy, __fmul2_rn(nx, dx)));      // n_Y.d
+  const float2 ip0 = __ffma2_rn(tnz, nz, __ffma2_rn(tny, ny, __fmul2_rn(tnx, nx)));   // n_X.n_Y
+  const float2 t1 = __fmul2_rn(ipY, h), t2 = __fmul2_rn(ipX, h), u = __fmul2_rn(ipX, t1);
+  const float2 y0 = __ffma2_rn(make_float2(-e.x, -e.y), g, g);                       // G0 - Gk
+  const float2 dd = __fmul2_rn(__ffma2_rn(u, f2(-3.f), __fmul2_rn(ip0, g)), g2);     // d2 G0
+  const float2 y3 = __ffma2_rn(dd, __fadd2_rn(c, m1), __fmul2_rn(__fmul2_rn(f2(-kap2), e), u));
+  const float2 fe = __ffma2_rn(f2(eps), c, m1), fi = __ffma2_rn(f2(ieps), c, m1);    // eps c - 1, c/eps - 1
+  const float2 t1fe = __fmul2_rn(t1, fe), t2fi = __fmul2_rn(t2, fi);
+  const float2 t2fe = __fmul2_rn(t2, fe), t1fi = __fmul2_rn(t1, fi);
+  // K(X, Y): the target X of this lane, sources Y
+  acc0 = __ffma2_rn(y0, wa, acc0);
+  acc0 = __ffma2_rn(t1fe, wb, acc0);
+  acc1 = __ffma2_rn(t2fi, wa, acc1);
+  acc1 = __ffma2_rn(y3, wb, acc1);
+  // K(Y, X): the two sources as targets of this lane's panel
+  s0 = __ffma2_rn(t2fe, wbtn, __fmul2_rn(y0, wat));
+  s1 = __ffma2_rn(t1fi, watn, __fmul2_rn(y3, wbt));
+}
+
+__global__ void __launch_bounds__(kSymWarps * 32, FB_NEAR_SYM_MIN_BLOCKS)
+near_sym_f2_kernel(int nTasks, const int4 *__restrict__ tasks, const int *__restrict__ leafStart,
+                   const int *__restrict__ leafCount, const double *__restrict__ leafCtr,
+                   const float4 *__restrict__ recA, const float4 *__restrict__ recB, float kappa, float kexp,
+                   float eps, float ieps, float kap2, float2 *scr) {
+  // per warp, component-major: sQ[k][m] holds component k of the tile's sources m and (m + 16) mod 32,
+  // interleaved (first, second, first, second), read by lane t at step s from slot (t + s) mod 32
+  __shared__ float4 sQ[kSymWarps][4][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int task = blockIdx.x * kSymWarps + warp;
+  if (task >= nTasks) return;  // warp-uniform
+  const int4 tk = tasks[task];
+  const int R = tk.x, T = tk.y;
+  const int rb = leafStart[R], rc = leafCount[R], tb = leafStart[T], tc = leafCount[T];
+  const float sx = (float)(leafCtr[3 * R] - leafCtr[3 * T]);
+  const float sy = (float)(leafCtr[3 * R + 1] - leafCtr[3 * T + 1]);
+  const float sz = (float)(leafCtr[3 * R + 2] - leafCtr[3 * T + 2]);
+  float4(*Q)[32] = sQ[warp];
+  for (int g0 = 0; g0 < rc; g0 += 32) {
+    const int t = g0 + lane;
+    const bool valid = t < rc;
+    // a lane past the group's end: far away, zero weights (its terms vanish, its sums are dropped)
+    const float4 a = valid ? recA[rb + t] : make_float4(1e4f, 1e4f, 1e4f, 0.f);
+    const float4 b = valid ? recB[rb + t] : make_float4(0.f, 0.f, 1.f, 0.f);
+    const float2 tx = f2(a.x + sx), ty = f2(a.y + sy), tz = f2(a.z + sz);
+    const float2 tnx = f2(b.x), tny = f2(b.y), tnz = f2(b.z);
+    const float2 wat = f2(a.w), wbt = f2(b.w), watn = f2(-a.w), wbtn = f2(-b.w);
+    float2 acc0 = f2(0.f), acc1 = f2(0.f);
+    for (int j0 = 0; j0 < tc; j0 += 32) {
+      const int m = min(32, tc - j0);
+      // stage the tile: source j0+lane, or a padding source far away with zero weights
+      float4 sa = make_float4(-1e4f, -1e4f, -1e4f, 0.f), sb = make_float4(0.f, 0.f, 1.f, 0.f);
+      if (lane < m) {
+        sa = recA[tb + j0 + lane];
+        sb = recB[tb + j0 + lane];
+      }
+      __syncwarp();   // the previous tile's reads are done
+      {
+        const int o = (lane + 16) & 31;   // the slot that holds this source second
+        Q[0][lane].x = -sa.x; Q[0][lane].z = -sa.y; Q[0][o].y = -sa.x; Q[0][o].w = -sa.y;
+        Q[1][lane].x = -sa.z; Q[1][lane].z = sa.w;  Q[1][o].y = -sa.z; Q[1][o].w = sa.w;
+        Q[2][lane].x = sb.x;  Q[2][lane].z = sb.y;  Q[2][o].y = sb.x;  Q[2][o].w = sb.y;
+        Q[3][lane].x = sb.z;  Q[3][lane].z = sb.w;  Q[3][o].y = sb.z;  Q[3][o].w = sb.w;
+      }
+      __syncwarp();
+      float2 own = f2(0.f);   // this lane's source j0+lane: (pot, dpdn) from the group's 32 targets
+#pragma unroll 4
+      for (int st = 0; st < 16; st++) {
+        const int slot = (lane + st) & 31;
+        float2 s0, s1;
+        near_sym_pair2(Q[0][slot], Q[1][slot], Q[2][slot], Q[3][slot], tx, ty, tz, tnx, tny, tnz, wat, wbt, watn,
+                       wbtn, kappa, kexp, eps, ieps, kap2, acc0, acc1, s0, s1);
+        // this lane's source was the first source of lane (lane - st) and the second of lane (lane - st - 16)
+        const int l1 = (lane - st) & 31, l2 = (lane - st - 16) & 31;
+        const float a0 = __shfl_sync(0xffffffffu, s0.x, l1), a1 = __shfl_sync(0xffffffffu, s1.x, l1);
+        const float b0 = __shfl_sync(0xffffffffu, s0.y, l2), b1 = __shfl_sync(0xffffffffu, s1.y, l2);
+        own = __fadd2_rn(own, __fadd2_rn(make_float2(a0, a1), make_float2(b0, b1)));
+      }
+      if (lane < m) {   // the tile side's slot: written by the first group, added to by the next
+        float2 *q = scr + tk.w + j0 + lane;
+        const float2 prev = g0 == 0 ? f2(0.f) : *q;
+        *q = __fadd2_rn(prev, own);
+      }
+    }
+    if (valid) scr[tk.z + t] = make_float2(acc0.x + acc0.y, acc1.x + acc1.y);
+  }
 }
 
 // FP64 correction for every special pair: exact panelIA0 minus the
@@ -815,6 +966,58 @@ static bool special_pairs_host(Context &c, const std::vector<int> &nearSortedFla
   return true;
 }
 
+// The symmetric kernel's leaf pairs (mixed contexts, FMM operator): every
+// unordered pair of distinct near leaves whose smaller leaf has at least
+// FB_NEAR_SYM_MIN_LEAF panels, the larger leaf on the register side; a scratch
+// slot of 2 floats per (ordered pair, target panel); costliest pairs first.
+// FABIPB_B200_NEAR_SYM=0 turns it off (every pair in the ordered kernel).
+static bool setup_near_sym(Context &c) {
+  c.nSymTasks = 0;
+  const char *env = getenv("FABIPB_B200_NEAR_SYM");
+  if (!c.mixed || c.dense || (env && atoi(env) == 0)) return true;
+  const PanelTree &pt = c.pt;
+  const size_t nEnt = pt.nearSrc.size();
+  std::vector<int> symOff(nEnt, -1);
+  std::vector<int4> tasks;
+  std::vector<long long> cost;
+  long long tot = 0, pairs = 0;
+  for (int L = 0; L < pt.nLeaves; L++)
+    for (int p = pt.nearOff[L]; p < pt.nearOff[L + 1]; p++) {
+      const int S = pt.nearSrc[p];
+      if (S <= L) continue;
+      const int cl = pt.leafCount[L], cs = pt.leafCount[S];
+      if (std::min(cl, cs) < FB_NEAR_SYM_MIN_LEAF) continue;
+      int q = -1;   // the mirror entry (S <- L)
+      for (int k = pt.nearOff[S]; k < pt.nearOff[S + 1]; k++)
+        if (pt.nearSrc[k] == L) { q = k; break; }
+      if (q < 0) continue;   // not mirrored: both directions stay ordered
+      const bool lReg = cl >= cs;
+      const int R = lReg ? L : S, T = lReg ? S : L, pR = lReg ? p : q, pT = lReg ? q : p;
+      FB_CHECK(tot + cl + cs < 2147483647LL, "symmetric near-field scratch above 2^31 slots");
+      symOff[pR] = (int)tot;
+      tot += pt.leafCount[R];
+      symOff[pT] = (int)tot;
+      tot += pt.leafCount[T];
+      tasks.push_back(make_int4(R, T, symOff[pR], symOff[pT]));
+      cost.push_back((long long)cl * cs);
+      pairs += (long long)cl * cs;
+    }
+  if (tasks.empty()) return true;
+  std::vector<int> ord(tasks.size());
+  for (size_t i = 0; i < ord.size(); i++) ord[i] = (int)i;
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+  std::vector<int4> sorted(tasks.size());
+  for (size_t i = 0; i < ord.size(); i++) sorted[i] = tasks[ord[i]];
+  cudaStream_t s = c.stream;
+  if (!c.arena.upload(&c.d_symTask, sorted, s) || !c.arena.upload(&c.d_symOff, symOff, s) ||
+      !c.arena.alloc_n(&c.d_symScr, (size_t)tot) || !c.arena.alloc_n(&c.d_symA, (size_t)c.n) ||
+      !c.arena.alloc_n(&c.d_symB, (size_t)c.n))
+    return false;
+  c.nSymTasks = (int)sorted.size();
+  c.symPanelPairs = pairs;
+  return true;
+}
+
 // static target geometry relative to the leaf centres
 static bool setup_near_targets(Context &c) {
   const int n = c.n;
@@ -831,7 +1034,7 @@ static bool setup_near_targets(Context &c) {
         n, c.d_vtx, c.d_nrm, c.d_area, c.d_leafOfPanel, c.d_leafCtr, (double4 *)c.d_tgtP, (double4 *)c.d_tgtN);
   }
   FB_CUDA(cudaGetLastError());
-  return true;
+  return setup_near_sym(c);
 }
 
 template <typename T, bool ADJ>
@@ -846,11 +1049,20 @@ static void launch_near_t(Context &c, const void *tgtP, const void *tgtN, void *
   near_pack_kernel<T><<<ceil_div(n, 256), 256, 0, s>>>(n, (const V *)tgtP, (const V *)tgtN, c.d_area, sgm, (V *)srcA,
                                                        (V *)srcB, packed ? (ADJ ? 2 : 1) : 0);
   if (packed) {
+    const bool sym = !ADJ && c.nSymTasks > 0 && tgtP == c.d_tgtP;
+    if (sym) {   // unordered leaf pairs of the symmetric kernel first, into the scratch
+      near_pack_kernel<float><<<ceil_div(n, 256), 256, 0, s>>>(n, (const float4 *)tgtP, (const float4 *)tgtN,
+                                                               c.d_area, sgm, c.d_symA, c.d_symB, 0);
+      near_sym_f2_kernel<<<ceil_div(c.nSymTasks, kSymWarps), kSymWarps * 32, 0, s>>>(
+          c.nSymTasks, c.d_symTask, c.d_leafStart, c.d_leafCount, c.d_leafCtr, c.d_symA, c.d_symB, (float)kap,
+          (float)kexp, (float)eps, (float)(1.0 / eps), (float)(kap * kap), c.d_symScr);
+      c.launches += 2;
+    }
     near_apply_f2_kernel<ADJ><<<grid, kNearWarps * 32, 0, s>>>(
         c.nWork, c.d_work, c.d_leafStart, c.d_leafCount, c.d_nearOff, c.d_nearSrc, c.d_leafCtr,
         (const float4 *)tgtP, (const float4 *)tgtN, (const float4 *)srcA, (const float4 *)srcB, c.d_spOff, c.d_spSrc,
         ADJ ? c.d_spKT : c.d_spK, sgm, c.d_area, n, (float)kap, (float)kexp, (float)eps, (float)(1.0 / eps),
-        (float)(kap * kap), coef, accumulate ? 1 : 0, out);
+        (float)(kap * kap), coef, accumulate ? 1 : 0, out, sym ? c.d_symOff : nullptr, c.d_symScr);
     return;
   }
   near_apply_kernel<T, ADJ><<<grid, kNearWarps * 32, 0, s>>>(

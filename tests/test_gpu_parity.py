@@ -109,6 +109,32 @@ def test_matvec(name, precision, tol, case_dir, golden_meta):
     assert rel_l2(got, g["matvec"]) < tol
 
 
+@pytest.mark.parametrize("name,depth", [("sphere1280", 1), ("star2048", 2), ("shell1152", 2)])
+def test_symmetric_near_field(name, depth, case_dir, golden_meta, monkeypatch):
+    """The symmetric FP32 near field (each unordered pair of distinct near
+    leaves evaluated once for both directions, sums through the scratch):
+    shallow trees, so that the leaves are large enough for it; against the
+    FP64 near field and matvec (5e-6) and against the ordered FP32 kernel
+    alone (FABIPB_B200_NEAR_SYM=0; only the summation order differs)."""
+    opts = dict(golden_meta[name]["opts"], t=depth)
+    pan, _ = meshio.load_case(os.path.join(case_dir, name))
+    sg = make_golden.seeded_sigma(pan.n, 6)
+    s64 = lib.Surface(pan, lib.params(precision=lib.FP64, **case_params(opts)))
+    ref_near, ref_mv = s64.apply(sg, part=lib.NEAR), s64.matvec(sg)
+    out = {}
+    for sym in (True, False):
+        if not sym:
+            monkeypatch.setenv("FABIPB_B200_NEAR_SYM", "0")
+        s = lib.Surface(pan, lib.params(precision=lib.MIXED, **case_params(opts)))
+        n0 = s.launch_count()
+        near = s.apply(sg, part=lib.NEAR)
+        out[sym] = (near, s.launch_count() - n0, s.matvec(sg))
+    assert out[True][1] == out[False][1] + 2   # the symmetric pack and kernel ran
+    assert rel_l2(out[True][0], ref_near) < 5e-6
+    assert rel_l2(out[True][2], ref_mv) < 5e-6
+    assert rel_l2(out[True][0], out[False][0]) < 2e-6
+
+
 def test_apply_alpha_beta_semantics(case_dir, golden_meta, oracles):
     name = "star2048"
     s, _, _ = surface(case_dir, golden_meta, name, lib.FP64)
