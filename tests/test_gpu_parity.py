@@ -109,7 +109,7 @@ def test_matvec(name, precision, tol, case_dir, golden_meta):
     assert rel_l2(got, g["matvec"]) < tol
 
 
-@pytest.mark.parametrize("name,depth", [("sphere1280", 1), ("star2048", 2), ("shell1152", 2)])
+@pytest.mark.parametrize("name,depth", [("sphere1280", 2), ("star2048", 2), ("shell1152", 2)])
 def test_symmetric_near_field(name, depth, case_dir, golden_meta, monkeypatch):
     """The symmetric FP32 near field (each unordered pair of distinct near
     leaves evaluated once for both directions, sums through the scratch):
