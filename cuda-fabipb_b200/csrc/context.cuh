@@ -46,14 +46,15 @@ struct Context {
   double4 *d_spK = nullptr;                    // exact minus one-point coefficient
   double4 *d_spKT = nullptr;                   // the same for the transposed operator
   void *d_tgtP64 = nullptr, *d_tgtN64 = nullptr;   // FP64 records of a mixed context (refinement residuals)
-  // the symmetric FP32 near field (mixed contexts): unordered leaf pairs (register leaf, tile leaf,
-  // scratch offsets), per near-list entry its scratch offset (-1: the ordered kernel computes it)
+  // the symmetric near field: unordered leaf pairs (register leaf, tile leaf, scratch offsets),
+  // per near-list entry its scratch offset (-1: the ordered kernel computes it); scratch and
+  // records in the context's near-field precision (2 and 4 floats or doubles per entry)
   int nSymTasks = 0;
   long long symPanelPairs = 0;                 // unordered panel pairs of those leaf pairs
   int4 *d_symTask = nullptr;
   int *d_symOff = nullptr;
-  float2 *d_symScr = nullptr;
-  float4 *d_symA = nullptr, *d_symB = nullptr; // records {position, A*sigma_dpdn}, {normal, A*sigma_pot}
+  void *d_symScr = nullptr;
+  void *d_symA = nullptr, *d_symB = nullptr;   // records {position, A*sigma_dpdn}, {normal, A*sigma_pot}
   void *d_srcA64 = nullptr, *d_srcB64 = nullptr;
 
   // ---- FMM ----------------------------------------------------------

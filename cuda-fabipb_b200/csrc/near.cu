@@ -173,7 +173,8 @@ near_apply_kernel(int nWork, const int2 *__restrict__ work, const int *__restric
                   const int *__restrict__ spOff, const int *__restrict__ spSrc,
                   const double4 *__restrict__ spK, const double *__restrict__ sgm,
                   const double *__restrict__ area, int n, T kappa, T kexp, T eps, T ieps, T kap2,
-                  double coef, int accumulate, double *out) {
+                  double coef, int accumulate, double *out, const int *__restrict__ symOff,
+                  const T *__restrict__ symScr) {
   typedef typename Vec4<T>::t V;
   __shared__ V sA[kNearWarps][32];
   __shared__ V sB[kNearWarps][32];
@@ -195,6 +196,16 @@ near_apply_kernel(int nWork, const int2 *__restrict__ work, const int *__restric
   T acc0 = (T)0, acc1 = (T)0;
   const int p1 = nearOff[L + 1];
   for (int p = nearOff[L]; p < p1; p++) {
+    if (symOff) {   // a leaf pair of the symmetric kernel: its sums for this target are in the scratch
+      const int o = symOff[p];
+      if (o >= 0) {   // warp-uniform
+        if (valid && sub == 0) {
+          acc0 += symScr[2 * (size_t)(o + (X - base))];
+          acc1 += symScr[2 * (size_t)(o + (X - base)) + 1];
+        }
+        continue;
+      }
+    }
     const int S = nearSrc[p];
     const int sb = leafStart[S], sc = leafCount[S];
     const T tx = tp.x + (T)(cx - leafCtr[3 * S]);
@@ -567,6 +578,102 @@ near_sym_f2_kernel(int nTasks, const int4 *__restrict__ tasks, const int *__rest
       }
     }
     if (valid) scr[tk.z + t] = make_float2(acc0.x + acc0.y, acc1.x + acc1.y);
+  }
+}
+
+// The same symmetric scheme in scalar arithmetic (FP64 contexts): lane t
+// takes source (t + s) mod 32 in step s of 32; the source's term from the
+// lane's target goes to the owning lane by shuffle.
+template <typename T>
+__device__ __forceinline__ void near_sym_pair(const typename Vec4<T>::t a, const typename Vec4<T>::t b, T tx, T ty,
+                                              T tz, T tnx, T tny, T tnz, T wat, T wbt, T kappa, T kexp, T eps,
+                                              T ieps, T kap2, T &acc0, T &acc1, T &s0, T &s1) {
+  const T dx = tx - a.x, dy = ty - a.y, dz = tz - a.z;
+  const T r2 = dx * dx + dy * dy + dz * dz;
+  const T g = rsqrt_t(r2);   // distinct leaves: r > 0
+  const T r = r2 * g;
+  const T e = expneg_t(kexp, r);
+  const T c = (kappa * r + (T)1) * e;
+  const T g2 = g * g, h = g2 * g;
+  const T ipX = tnx * dx + tny * dy + tnz * dz;
+  const T ipY = b.x * dx + b.y * dy + b.z * dz;
+  const T ip0 = tnx * b.x + tny * b.y + tnz * b.z;
+  const T t1 = ipY * h, t2 = ipX * h, u = ipX * t1;
+  const T y0 = g - g * e;
+  const T dd = (ip0 * g - (T)3 * u) * g2;
+  const T y3 = dd * (c - (T)1) - kap2 * e * u;
+  const T fe = eps * c - (T)1, fi = c * ieps - (T)1;
+  acc0 += y0 * a.w + t1 * fe * b.w;
+  acc1 += t2 * fi * a.w + y3 * b.w;
+  s0 = y0 * wat - t2 * fe * wbt;
+  s1 = y3 * wbt - t1 * fi * wat;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSymWarps * 32, sizeof(T) == 8 ? 2 : FB_NEAR_SYM_MIN_BLOCKS)
+near_sym_kernel(int nTasks, const int4 *__restrict__ tasks, const int *__restrict__ leafStart,
+                const int *__restrict__ leafCount, const double *__restrict__ leafCtr,
+                const typename Vec4<T>::t *__restrict__ recA, const typename Vec4<T>::t *__restrict__ recB, T kappa,
+                T kexp, T eps, T ieps, T kap2, T *scr) {
+  typedef typename Vec4<T>::t V;
+  __shared__ V sA[kSymWarps][32], sB[kSymWarps][32];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int task = blockIdx.x * kSymWarps + warp;
+  if (task >= nTasks) return;  // warp-uniform
+  const int4 tk = tasks[task];
+  const int R = tk.x, Tl = tk.y;
+  const int rb = leafStart[R], rc = leafCount[R], tb = leafStart[Tl], tc = leafCount[Tl];
+  const T sx = (T)(leafCtr[3 * R] - leafCtr[3 * Tl]);
+  const T sy = (T)(leafCtr[3 * R + 1] - leafCtr[3 * Tl + 1]);
+  const T sz = (T)(leafCtr[3 * R + 2] - leafCtr[3 * Tl + 2]);
+  for (int g0 = 0; g0 < rc; g0 += 32) {
+    const int t = g0 + lane;
+    const bool valid = t < rc;
+    V a, b;
+    if (valid) {
+      a = recA[rb + t];
+      b = recB[rb + t];
+    } else {   // far away, zero weights
+      a.x = a.y = a.z = (T)1e4; a.w = (T)0;
+      b.x = b.y = (T)0; b.z = (T)1; b.w = (T)0;
+    }
+    const T tx = a.x + sx, ty = a.y + sy, tz = a.z + sz;
+    T acc0 = (T)0, acc1 = (T)0;
+    for (int j0 = 0; j0 < tc; j0 += 32) {
+      const int m = min(32, tc - j0);
+      V pa, pb;
+      if (lane < m) {
+        pa = recA[tb + j0 + lane];
+        pb = recB[tb + j0 + lane];
+      } else {
+        pa.x = pa.y = pa.z = (T)-1e4; pa.w = (T)0;
+        pb.x = pb.y = (T)0; pb.z = (T)1; pb.w = (T)0;
+      }
+      __syncwarp();
+      sA[warp][lane] = pa;
+      sB[warp][lane] = pb;
+      __syncwarp();
+      T own0 = (T)0, own1 = (T)0;
+#pragma unroll 2
+      for (int st = 0; st < 32; st++) {
+        const int j = (lane + st) & 31;
+        T s0, s1;
+        near_sym_pair<T>(sA[warp][j], sB[warp][j], tx, ty, tz, b.x, b.y, b.z, a.w, b.w, kappa, kexp, eps, ieps, kap2,
+                         acc0, acc1, s0, s1);
+        const int from = (lane - st) & 31;   // the lane whose source this step is this lane's
+        own0 += __shfl_sync(0xffffffffu, s0, from);
+        own1 += __shfl_sync(0xffffffffu, s1, from);
+      }
+      if (lane < m) {
+        T *q = scr + 2 * (size_t)(tk.w + j0 + lane);
+        q[0] = (g0 == 0 ? (T)0 : q[0]) + own0;
+        q[1] = (g0 == 0 ? (T)0 : q[1]) + own1;
+      }
+    }
+    if (valid) {
+      scr[2 * (size_t)(tk.z + t)] = acc0;
+      scr[2 * (size_t)(tk.z + t) + 1] = acc1;
+    }
   }
 }
 
@@ -966,7 +1073,7 @@ static bool special_pairs_host(Context &c, const std::vector<int> &nearSortedFla
   return true;
 }
 
-// The symmetric kernel's leaf pairs (mixed contexts, FMM operator): every
+// The symmetric kernels' leaf pairs (FMM operator, both precisions): every
 // unordered pair of distinct near leaves whose smaller leaf has at least
 // FB_NEAR_SYM_MIN_LEAF panels, the larger leaf on the register side; a scratch
 // slot of 2 floats per (ordered pair, target panel); costliest pairs first.
@@ -974,7 +1081,7 @@ static bool special_pairs_host(Context &c, const std::vector<int> &nearSortedFla
 static bool setup_near_sym(Context &c) {
   c.nSymTasks = 0;
   const char *env = getenv("FABIPB_B200_NEAR_SYM");
-  if (!c.mixed || c.dense || (env && atoi(env) == 0)) return true;
+  if (c.dense || (env && atoi(env) == 0)) return true;
   const PanelTree &pt = c.pt;
   const size_t nEnt = pt.nearSrc.size();
   std::vector<int> symOff(nEnt, -1);
@@ -1009,9 +1116,10 @@ static bool setup_near_sym(Context &c) {
   std::vector<int4> sorted(tasks.size());
   for (size_t i = 0; i < ord.size(); i++) sorted[i] = tasks[ord[i]];
   cudaStream_t s = c.stream;
+  const size_t esz = c.mixed ? sizeof(float) : sizeof(double);   // scratch element; records are 4 of them
   if (!c.arena.upload(&c.d_symTask, sorted, s) || !c.arena.upload(&c.d_symOff, symOff, s) ||
-      !c.arena.alloc_n(&c.d_symScr, (size_t)tot) || !c.arena.alloc_n(&c.d_symA, (size_t)c.n) ||
-      !c.arena.alloc_n(&c.d_symB, (size_t)c.n))
+      !c.arena.alloc(&c.d_symScr, 2 * esz * (size_t)tot) || !c.arena.alloc(&c.d_symA, 4 * esz * (size_t)c.n) ||
+      !c.arena.alloc(&c.d_symB, 4 * esz * (size_t)c.n))
     return false;
   c.nSymTasks = (int)sorted.size();
   c.symPanelPairs = pairs;
@@ -1052,23 +1160,36 @@ static void launch_near_t(Context &c, const void *tgtP, const void *tgtN, void *
     const bool sym = !ADJ && c.nSymTasks > 0 && tgtP == c.d_tgtP;
     if (sym) {   // unordered leaf pairs of the symmetric kernel first, into the scratch
       near_pack_kernel<float><<<ceil_div(n, 256), 256, 0, s>>>(n, (const float4 *)tgtP, (const float4 *)tgtN,
-                                                               c.d_area, sgm, c.d_symA, c.d_symB, 0);
+                                                               c.d_area, sgm, (float4 *)c.d_symA, (float4 *)c.d_symB, 0);
       near_sym_f2_kernel<<<ceil_div(c.nSymTasks, kSymWarps), kSymWarps * 32, 0, s>>>(
-          c.nSymTasks, c.d_symTask, c.d_leafStart, c.d_leafCount, c.d_leafCtr, c.d_symA, c.d_symB, (float)kap,
-          (float)kexp, (float)eps, (float)(1.0 / eps), (float)(kap * kap), c.d_symScr);
+          c.nSymTasks, c.d_symTask, c.d_leafStart, c.d_leafCount, c.d_leafCtr, (const float4 *)c.d_symA,
+          (const float4 *)c.d_symB, (float)kap, (float)kexp, (float)eps, (float)(1.0 / eps), (float)(kap * kap),
+          (float2 *)c.d_symScr);
       c.launches += 2;
     }
     near_apply_f2_kernel<ADJ><<<grid, kNearWarps * 32, 0, s>>>(
         c.nWork, c.d_work, c.d_leafStart, c.d_leafCount, c.d_nearOff, c.d_nearSrc, c.d_leafCtr,
         (const float4 *)tgtP, (const float4 *)tgtN, (const float4 *)srcA, (const float4 *)srcB, c.d_spOff, c.d_spSrc,
         ADJ ? c.d_spKT : c.d_spK, sgm, c.d_area, n, (float)kap, (float)kexp, (float)eps, (float)(1.0 / eps),
-        (float)(kap * kap), coef, accumulate ? 1 : 0, out, sym ? c.d_symOff : nullptr, c.d_symScr);
+        (float)(kap * kap), coef, accumulate ? 1 : 0, out, sym ? c.d_symOff : nullptr,
+        (const float2 *)c.d_symScr);
     return;
+  }
+  // the symmetric kernel for the context's own records (not the FP64 residual records of a mixed context)
+  const bool sym = !ADJ && c.nSymTasks > 0 && tgtP == c.d_tgtP && (sizeof(T) == 8) == !c.mixed;
+  if (sym) {
+    near_pack_kernel<T><<<ceil_div(n, 256), 256, 0, s>>>(n, (const V *)tgtP, (const V *)tgtN, c.d_area, sgm,
+                                                         (V *)c.d_symA, (V *)c.d_symB, 0);
+    near_sym_kernel<T><<<ceil_div(c.nSymTasks, kSymWarps), kSymWarps * 32, 0, s>>>(
+        c.nSymTasks, c.d_symTask, c.d_leafStart, c.d_leafCount, c.d_leafCtr, (const V *)c.d_symA,
+        (const V *)c.d_symB, (T)kap, (T)kexp, (T)eps, (T)(1.0 / eps), (T)(kap * kap), (T *)c.d_symScr);
+    c.launches += 2;
   }
   near_apply_kernel<T, ADJ><<<grid, kNearWarps * 32, 0, s>>>(
       c.nWork, c.d_work, c.d_leafStart, c.d_leafCount, c.d_nearOff, c.d_nearSrc, c.d_leafCtr, (const V *)tgtP,
       (const V *)tgtN, (const V *)srcA, (const V *)srcB, c.d_spOff, c.d_spSrc, ADJ ? c.d_spKT : c.d_spK, sgm,
-      c.d_area, n, (T)kap, (T)kexp, (T)eps, (T)(1.0 / eps), (T)(kap * kap), coef, accumulate ? 1 : 0, out);
+      c.d_area, n, (T)kap, (T)kexp, (T)eps, (T)(1.0 / eps), (T)(kap * kap), coef, accumulate ? 1 : 0, out,
+      sym ? c.d_symOff : nullptr, (const T *)c.d_symScr);
 }
 
 // FP64 records in a mixed context, for the FP64 residuals of iterative

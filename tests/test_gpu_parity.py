@@ -111,28 +111,31 @@ def test_matvec(name, precision, tol, case_dir, golden_meta):
 
 @pytest.mark.parametrize("name,depth", [("sphere1280", 2), ("star2048", 2), ("shell1152", 2)])
 def test_symmetric_near_field(name, depth, case_dir, golden_meta, monkeypatch):
-    """The symmetric FP32 near field (each unordered pair of distinct near
-    leaves evaluated once for both directions, sums through the scratch):
-    shallow trees, so that the leaves are large enough for it; against the
-    FP64 near field and matvec (5e-6) and against the ordered FP32 kernel
-    alone (FABIPB_B200_NEAR_SYM=0; only the summation order differs)."""
+    """The symmetric near field (each unordered pair of distinct near leaves
+    evaluated once for both directions, sums through the scratch), FP32 packed
+    and FP64: shallow trees, so that the leaves are large enough for it;
+    against the ordered kernels alone (FABIPB_B200_NEAR_SYM=0): FP64 to 1e-13
+    (only the summation order differs), FP32 to 2e-6 of the ordered FP32 and
+    5e-6 of the FP64 near field and matvec."""
     opts = dict(golden_meta[name]["opts"], t=depth)
     pan, _ = meshio.load_case(os.path.join(case_dir, name))
     sg = make_golden.seeded_sigma(pan.n, 6)
-    s64 = lib.Surface(pan, lib.params(precision=lib.FP64, **case_params(opts)))
-    ref_near, ref_mv = s64.apply(sg, part=lib.NEAR), s64.matvec(sg)
     out = {}
     for sym in (True, False):
-        if not sym:
-            monkeypatch.setenv("FABIPB_B200_NEAR_SYM", "0")
-        s = lib.Surface(pan, lib.params(precision=lib.MIXED, **case_params(opts)))
-        n0 = s.launch_count()
-        near = s.apply(sg, part=lib.NEAR)
-        out[sym] = (near, s.launch_count() - n0, s.matvec(sg))
-    assert out[True][1] == out[False][1] + 2   # the symmetric pack and kernel ran
-    assert rel_l2(out[True][0], ref_near) < 5e-6
-    assert rel_l2(out[True][2], ref_mv) < 5e-6
-    assert rel_l2(out[True][0], out[False][0]) < 2e-6
+        monkeypatch.setenv("FABIPB_B200_NEAR_SYM", "1" if sym else "0")
+        for prec in (lib.FP64, lib.MIXED):
+            s = lib.Surface(pan, lib.params(precision=prec, **case_params(opts)))
+            n0 = s.launch_count()
+            near = s.apply(sg, part=lib.NEAR)
+            out[sym, prec] = (near, s.launch_count() - n0, s.matvec(sg))
+    for prec in (lib.FP64, lib.MIXED):
+        assert out[True, prec][1] == out[False, prec][1] + 2   # the symmetric pack and kernel ran
+    ref_near, ref_mv = out[False, lib.FP64][0], out[False, lib.FP64][2]
+    assert rel_l2(out[True, lib.FP64][0], ref_near) < 1e-13
+    assert rel_l2(out[True, lib.FP64][2], ref_mv) < 1e-13
+    assert rel_l2(out[True, lib.MIXED][0], ref_near) < 5e-6
+    assert rel_l2(out[True, lib.MIXED][2], ref_mv) < 5e-6
+    assert rel_l2(out[True, lib.MIXED][0], out[False, lib.MIXED][0]) < 2e-6
 
 
 def test_apply_alpha_beta_semantics(case_dir, golden_meta, oracles):
