@@ -128,7 +128,7 @@ def main_large():
 
 # Central finite differences of the reference CLI's own energy on star2048:
 # every charge-tree cluster opened (FABIPB_ENERGY_TREE_THETA=1e-9, so the
-# panel-tree energy is the direct panel-charge sum), GMRES to 1e-12, the
+# panel-tree energy is the direct panel-charge sum), GMRES to 1e-14, the
 # charges written with ten decimals, the raw energy read at full precision
 # from the CLI's energy-compare line (FABIPB_ENERGY_MODE=compare,
 # src/fabipb.c:1172-1181).  Step 1e-5 e for a charge, 1e-4 A for a position
@@ -154,7 +154,7 @@ def main_fd():
     """fd_star2048.json: the reference's central differences of its energy."""
     from fabipb_b200 import meshio
     from oracle import oracle as O
-    opts = dict(CASES[FD_CASE][2], o=1e-12)
+    opts = dict(CASES[FD_CASE][2], o=1e-14)
     env = {"FABIPB_ENERGY_TREE_THETA": "1e-9", "FABIPB_ENERGY_MODE": "compare"}
     out = {"case": FD_CASE, "hq": FD_HQ, "hx": FD_HX, "units": "raw energy", "charges": {}}
     with tempfile.TemporaryDirectory() as tmp:
@@ -164,7 +164,9 @@ def main_fd():
 
         def energy(c):
             write_pqr(base + ".pqr", c)
-            _, _, _, out = O.run_ref_solve(base, ref_opts(opts, True), threads=os.cpu_count(), extra_env=env)
+            _, it, res, out = O.run_ref_solve(base, ref_opts(opts, True) + ["-i=1000"], threads=os.cpu_count(),
+                                              extra_env=env)
+            assert res <= opts["o"], (it, res)   # converged: the differences see no solver noise above 1e-14
             line = [l for l in out.splitlines() if l.startswith("Energy compare:")][0]
             return float(line.split("panel-tree raw=")[1].split()[0])
 

@@ -13,7 +13,7 @@ reference's own finite differences.
   truncation only (p=4, MAC 0.7: energy 1.7e-4, dE/dq 1.7e-3 relative).
 * On star2048, the library's gradients against central differences of the
   reference CLI's own energy (tests/golden/fd_star2048.json, written by
-  make_golden.py --fd: direct energy, GMRES to 1e-12, raw energies at full
+  make_golden.py --fd: direct energy, GMRES to 1e-14, raw energies at full
   precision).
 
 The energy differentiated is the direct panel-charge sum E = e(q, r) . sigma
@@ -145,8 +145,10 @@ def test_gradients_match_reference_finite_differences(case_dir, golden_meta):
     for k, rec in fd["charges"].items():
         k = int(k)
         # E is quadratic in q: the charge differences are exact up to the solves'
-        # residuals over h; positions: also the O(h^2) truncation
-        assert abs(dq[k] - rec["dq"]) <= 1e-5 * abs(rec["dq"]), (k, dq[k], rec["dq"])
+        # residuals over h; positions: also the O(h^2) truncation (the reference
+        # solves to 1e-14 for them: at 1e-12 its differences carried noise of
+        # 5e-6 in these units)
+        assert abs(dq[k] - rec["dq"]) <= 1e-6 * abs(rec["dq"]), (k, dq[k], rec["dq"])
         scale = max(abs(v) for v in rec["dx"])
         for a in range(3):
-            assert abs(dx[k, a] - rec["dx"][a]) <= 1e-3 * scale, (k, a, dx[k, a], rec["dx"][a])
+            assert abs(dx[k, a] - rec["dx"][a]) <= 1e-4 * scale, (k, a, dx[k, a], rec["dx"][a])
