@@ -144,12 +144,10 @@ def test_gradients_match_reference_finite_differences(case_dir, golden_meta):
     assert info2 == 0
     for k, rec in fd["charges"].items():
         k = int(k)
-        # E is quadratic in q: the charge differences are exact up to the solves'
-        # residuals over h; positions: also the O(h^2) truncation.  The
-        # reference's differences keep ~3e-8 of solver noise (raw units) even
-        # at its GMRES tolerance 1e-14 (5e-6 at 1e-12), a few 1e-4 of the
-        # largest component of a charge's force
-        assert abs(dq[k] - rec["dq"]) <= 1e-6 * abs(rec["dq"]), (k, dq[k], rec["dq"])
+        # the reference's energies carry ~1e-9 of solver noise: over the steps
+        # (1e-2 e, 1e-2 A) 5e-8 in the differences; positions also the O(h^2)
+        # truncation (a few 1e-4 of the force)
+        assert abs(dq[k] - rec["dq"]) <= 1e-5 * abs(rec["dq"]), (k, dq[k], rec["dq"])
         scale = max(abs(v) for v in rec["dx"])
         for a in range(3):
-            assert abs(dx[k, a] - rec["dx"][a]) <= 1e-3 * scale, (k, a, dx[k, a], rec["dx"][a])
+            assert abs(dx[k, a] - rec["dx"][a]) <= 1e-3 * scale + 2e-7, (k, a, dx[k, a], rec["dx"][a])
