@@ -443,7 +443,7 @@ near_apply_f2_kernel(int nWork, const int2 *__restrict__ work, const int *__rest
 }
 
 // ---------------------------------------------------------------------------
-// Symmetric near field (FP32, packed f32x2; mixed contexts, forward operator).
+// Symmetric near field (FP32, packed f32x2; mixed contexts; forward and transposed operator).
 // The one-point pair term of K(X, Y) and that of K(Y, X) share r, 1/r,
 // e^{-kappa r}, (kappa r + 1) e^{-kappa r}, n_X.n_Y and the double-layer
 // factors; with d = x_X - x_Y, swapping the panels negates d, so
@@ -460,17 +460,19 @@ near_apply_f2_kernel(int nWork, const int2 *__restrict__ work, const int *__rest
 // The sums go to a scratch slot per (ordered leaf pair, panel); the ordered
 // near-field kernel adds them, in its near-list order, to its own FP32 sums
 // (deterministic: no atomics).  Self pairs and pairs with a small leaf stay in
-// the ordered kernel.
+// the ordered kernel.  ADJ: the transposed operator, with the transposed
+// blocks of the two directions (near_pair's ADJ terms and their swap).
 // ---------------------------------------------------------------------------
 #ifndef FB_NEAR_SYM_MIN_BLOCKS
 #define FB_NEAR_SYM_MIN_BLOCKS 6
 #endif
 // leaf pairs whose smaller leaf has fewer panels stay in the ordered kernel
 #ifndef FB_NEAR_SYM_MIN_LEAF
-#define FB_NEAR_SYM_MIN_LEAF 24
+#define FB_NEAR_SYM_MIN_LEAF 48
 #endif
 constexpr int kSymWarps = 4;
 
+template <bool ADJ>
 __device__ __forceinline__ void near_sym_pair2(const float4 A, const float4 B, const float4 C, const float4 D,
                                                float2 tx, float2 ty, float2 tz, float2 tnx, float2 tny, float2 tnz,
                                                float2 wat, float2 wbt, float2 watn, float2 wbtn, float kappa,
@@ -503,16 +505,27 @@ __device__ __forceinline__ void near_sym_pair2(const float4 A, const float4 B, c
   const float2 fe = __ffma2_rn(f2(eps), c, m1), fi = __ffma2_rn(f2(ieps), c, m1);    // eps c - 1, c/eps - 1
   const float2 t1fe = __fmul2_rn(t1, fe), t2fi = __fmul2_rn(t2, fi);
   const float2 t2fe = __fmul2_rn(t2, fe), t1fi = __fmul2_rn(t1, fi);
-  // K(X, Y): the target X of this lane, sources Y
-  acc0 = __ffma2_rn(y0, wa, acc0);
-  acc0 = __ffma2_rn(t1fe, wb, acc0);
-  acc1 = __ffma2_rn(t2fi, wa, acc1);
-  acc1 = __ffma2_rn(y3, wb, acc1);
-  // K(Y, X): the two sources as targets of this lane's panel
-  s0 = __ffma2_rn(t2fe, wbtn, __fmul2_rn(y0, wat));
-  s1 = __ffma2_rn(t1fi, watn, __fmul2_rn(y3, wbt));
+  if (ADJ) {
+    // the transposed blocks (near_pair's ADJ terms): K(Y,X)^T to the target X, K(X,Y)^T to the sources
+    acc0 = __ffma2_rn(y3, wa, acc0);
+    acc0 = __ffma2_rn(make_float2(-t2fe.x, -t2fe.y), wb, acc0);
+    acc1 = __ffma2_rn(y0, wb, acc1);
+    acc1 = __ffma2_rn(make_float2(-t1fi.x, -t1fi.y), wa, acc1);
+    s0 = __ffma2_rn(t1fe, wbt, __fmul2_rn(y3, wat));
+    s1 = __ffma2_rn(t2fi, wat, __fmul2_rn(y0, wbt));
+  } else {
+    // K(X, Y): the target X of this lane, sources Y
+    acc0 = __ffma2_rn(y0, wa, acc0);
+    acc0 = __ffma2_rn(t1fe, wb, acc0);
+    acc1 = __ffma2_rn(t2fi, wa, acc1);
+    acc1 = __ffma2_rn(y3, wb, acc1);
+    // K(Y, X): the two sources as targets of this lane's panel
+    s0 = __ffma2_rn(t2fe, wbtn, __fmul2_rn(y0, wat));
+    s1 = __ffma2_rn(t1fi, watn, __fmul2_rn(y3, wbt));
+  }
 }
 
+template <bool ADJ>
 __global__ void __launch_bounds__(kSymWarps * 32, FB_NEAR_SYM_MIN_BLOCKS)
 near_sym_f2_kernel(int nTasks, const int4 *__restrict__ tasks, const int *__restrict__ leafStart,
                    const int *__restrict__ leafCount, const double *__restrict__ leafCtr,
@@ -563,8 +576,8 @@ near_sym_f2_kernel(int nTasks, const int4 *__restrict__ tasks, const int *__rest
       for (int st = 0; st < 16; st++) {
         const int slot = (lane + st) & 31;
         float2 s0, s1;
-        near_sym_pair2(Q[0][slot], Q[1][slot], Q[2][slot], Q[3][slot], tx, ty, tz, tnx, tny, tnz, wat, wbt, watn,
-                       wbtn, kappa, kexp, eps, ieps, kap2, acc0, acc1, s0, s1);
+        near_sym_pair2<ADJ>(Q[0][slot], Q[1][slot], Q[2][slot], Q[3][slot], tx, ty, tz, tnx, tny, tnz, wat, wbt,
+                            watn, wbtn, kappa, kexp, eps, ieps, kap2, acc0, acc1, s0, s1);
         // this lane's source was the first source of lane (lane - st) and the second of lane (lane - st - 16)
         const int l1 = (lane - st) & 31, l2 = (lane - st - 16) & 31;
         const float a0 = __shfl_sync(0xffffffffu, s0.x, l1), a1 = __shfl_sync(0xffffffffu, s1.x, l1);
@@ -584,7 +597,7 @@ near_sym_f2_kernel(int nTasks, const int4 *__restrict__ tasks, const int *__rest
 // The same symmetric scheme in scalar arithmetic (FP64 contexts): lane t
 // takes source (t + s) mod 32 in step s of 32; the source's term from the
 // lane's target goes to the owning lane by shuffle.
-template <typename T>
+template <typename T, bool ADJ>
 __device__ __forceinline__ void near_sym_pair(const typename Vec4<T>::t a, const typename Vec4<T>::t b, T tx, T ty,
                                               T tz, T tnx, T tny, T tnz, T wat, T wbt, T kappa, T kexp, T eps,
                                               T ieps, T kap2, T &acc0, T &acc1, T &s0, T &s1) {
@@ -603,13 +616,20 @@ __device__ __forceinline__ void near_sym_pair(const typename Vec4<T>::t a, const
   const T dd = (ip0 * g - (T)3 * u) * g2;
   const T y3 = dd * (c - (T)1) - kap2 * e * u;
   const T fe = eps * c - (T)1, fi = c * ieps - (T)1;
-  acc0 += y0 * a.w + t1 * fe * b.w;
-  acc1 += t2 * fi * a.w + y3 * b.w;
-  s0 = y0 * wat - t2 * fe * wbt;
-  s1 = y3 * wbt - t1 * fi * wat;
+  if (ADJ) {   // the transposed blocks, as near_pair's ADJ terms
+    acc0 += y3 * a.w - t2 * fe * b.w;
+    acc1 += y0 * b.w - t1 * fi * a.w;
+    s0 = y3 * wat + t1 * fe * wbt;
+    s1 = y0 * wbt + t2 * fi * wat;
+  } else {
+    acc0 += y0 * a.w + t1 * fe * b.w;
+    acc1 += t2 * fi * a.w + y3 * b.w;
+    s0 = y0 * wat - t2 * fe * wbt;
+    s1 = y3 * wbt - t1 * fi * wat;
+  }
 }
 
-template <typename T>
+template <typename T, bool ADJ>
 __global__ void __launch_bounds__(kSymWarps * 32, sizeof(T) == 8 ? 2 : FB_NEAR_SYM_MIN_BLOCKS)
 near_sym_kernel(int nTasks, const int4 *__restrict__ tasks, const int *__restrict__ leafStart,
                 const int *__restrict__ leafCount, const double *__restrict__ leafCtr,
@@ -658,8 +678,8 @@ near_sym_kernel(int nTasks, const int4 *__restrict__ tasks, const int *__restric
       for (int st = 0; st < 32; st++) {
         const int j = (lane + st) & 31;
         T s0, s1;
-        near_sym_pair<T>(sA[warp][j], sB[warp][j], tx, ty, tz, b.x, b.y, b.z, a.w, b.w, kappa, kexp, eps, ieps, kap2,
-                         acc0, acc1, s0, s1);
+        near_sym_pair<T, ADJ>(sA[warp][j], sB[warp][j], tx, ty, tz, b.x, b.y, b.z, a.w, b.w, kappa, kexp, eps, ieps,
+                              kap2, acc0, acc1, s0, s1);
         const int from = (lane - st) & 31;   // the lane whose source this step is this lane's
         own0 += __shfl_sync(0xffffffffu, s0, from);
         own1 += __shfl_sync(0xffffffffu, s1, from);
@@ -1157,11 +1177,11 @@ static void launch_near_t(Context &c, const void *tgtP, const void *tgtN, void *
   near_pack_kernel<T><<<ceil_div(n, 256), 256, 0, s>>>(n, (const V *)tgtP, (const V *)tgtN, c.d_area, sgm, (V *)srcA,
                                                        (V *)srcB, packed ? (ADJ ? 2 : 1) : 0);
   if (packed) {
-    const bool sym = !ADJ && c.nSymTasks > 0 && tgtP == c.d_tgtP;
+    const bool sym = c.nSymTasks > 0 && tgtP == c.d_tgtP;
     if (sym) {   // unordered leaf pairs of the symmetric kernel first, into the scratch
       near_pack_kernel<float><<<ceil_div(n, 256), 256, 0, s>>>(n, (const float4 *)tgtP, (const float4 *)tgtN,
                                                                c.d_area, sgm, (float4 *)c.d_symA, (float4 *)c.d_symB, 0);
-      near_sym_f2_kernel<<<ceil_div(c.nSymTasks, kSymWarps), kSymWarps * 32, 0, s>>>(
+      near_sym_f2_kernel<ADJ><<<ceil_div(c.nSymTasks, kSymWarps), kSymWarps * 32, 0, s>>>(
           c.nSymTasks, c.d_symTask, c.d_leafStart, c.d_leafCount, c.d_leafCtr, (const float4 *)c.d_symA,
           (const float4 *)c.d_symB, (float)kap, (float)kexp, (float)eps, (float)(1.0 / eps), (float)(kap * kap),
           (float2 *)c.d_symScr);
@@ -1176,11 +1196,11 @@ static void launch_near_t(Context &c, const void *tgtP, const void *tgtN, void *
     return;
   }
   // the symmetric kernel for the context's own records (not the FP64 residual records of a mixed context)
-  const bool sym = !ADJ && c.nSymTasks > 0 && tgtP == c.d_tgtP && (sizeof(T) == 8) == !c.mixed;
+  const bool sym = c.nSymTasks > 0 && tgtP == c.d_tgtP && (sizeof(T) == 8) == !c.mixed;
   if (sym) {
     near_pack_kernel<T><<<ceil_div(n, 256), 256, 0, s>>>(n, (const V *)tgtP, (const V *)tgtN, c.d_area, sgm,
                                                          (V *)c.d_symA, (V *)c.d_symB, 0);
-    near_sym_kernel<T><<<ceil_div(c.nSymTasks, kSymWarps), kSymWarps * 32, 0, s>>>(
+    near_sym_kernel<T, ADJ><<<ceil_div(c.nSymTasks, kSymWarps), kSymWarps * 32, 0, s>>>(
         c.nSymTasks, c.d_symTask, c.d_leafStart, c.d_leafCount, c.d_leafCtr, (const V *)c.d_symA,
         (const V *)c.d_symB, (T)kap, (T)kexp, (T)eps, (T)(1.0 / eps), (T)(kap * kap), (T *)c.d_symScr);
     c.launches += 2;

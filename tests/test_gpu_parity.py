@@ -109,33 +109,41 @@ def test_matvec(name, precision, tol, case_dir, golden_meta):
     assert rel_l2(got, g["matvec"]) < tol
 
 
-@pytest.mark.parametrize("name,depth", [("sphere1280", 2), ("star2048", 2), ("shell1152", 2)])
-def test_symmetric_near_field(name, depth, case_dir, golden_meta, monkeypatch):
+@pytest.mark.parametrize("name,depth,height", [("sphere1280", 1, 1), ("star2048", 2, 2), ("shell1152", 2, 2)])
+def test_symmetric_near_field(name, depth, height, case_dir, golden_meta, monkeypatch):
     """The symmetric near field (each unordered pair of distinct near leaves
     evaluated once for both directions, sums through the scratch), FP32 packed
-    and FP64: shallow trees, so that the leaves are large enough for it;
-    against the ordered kernels alone (FABIPB_B200_NEAR_SYM=0): FP64 to 1e-13
-    (only the summation order differs), FP32 to 2e-6 of the ordered FP32 and
-    5e-6 of the FP64 near field and matvec."""
+    and FP64, forward and transposed: shallow trees, so that the leaves are
+    large enough for it; against the ordered kernels alone
+    (FABIPB_B200_NEAR_SYM=0): FP64 to 1e-13 (only the summation order
+    differs), FP32 to 2e-6 of the ordered FP32 and 5e-6 of the FP64 near
+    field, matvec and transposed near field; the duality of the symmetric
+    FP64 near field."""
     opts = dict(golden_meta[name]["opts"], t=depth)
     pan, _ = meshio.load_case(os.path.join(case_dir, name))
     sg = make_golden.seeded_sigma(pan.n, 6)
+    lam = make_golden.seeded_sigma(pan.n, 7)
     out = {}
     for sym in (True, False):
         monkeypatch.setenv("FABIPB_B200_NEAR_SYM", "1" if sym else "0")
         for prec in (lib.FP64, lib.MIXED):
-            s = lib.Surface(pan, lib.params(precision=prec, **case_params(opts)))
+            s = lib.Surface(pan, lib.params(precision=prec, height=height, **case_params(opts)))
             n0 = s.launch_count()
             near = s.apply(sg, part=lib.NEAR)
-            out[sym, prec] = (near, s.launch_count() - n0, s.matvec(sg))
+            out[sym, prec] = (near, s.launch_count() - n0, s.matvec(sg), s.apply_adjoint(lam, part=lib.NEAR))
     for prec in (lib.FP64, lib.MIXED):
         assert out[True, prec][1] == out[False, prec][1] + 2   # the symmetric pack and kernel ran
-    ref_near, ref_mv = out[False, lib.FP64][0], out[False, lib.FP64][2]
+    ref_near, ref_mv, ref_adj = out[False, lib.FP64][0], out[False, lib.FP64][2], out[False, lib.FP64][3]
     assert rel_l2(out[True, lib.FP64][0], ref_near) < 1e-13
     assert rel_l2(out[True, lib.FP64][2], ref_mv) < 1e-13
+    assert rel_l2(out[True, lib.FP64][3], ref_adj) < 1e-13      # the transposed operator
     assert rel_l2(out[True, lib.MIXED][0], ref_near) < 5e-6
     assert rel_l2(out[True, lib.MIXED][2], ref_mv) < 5e-6
+    assert rel_l2(out[True, lib.MIXED][3], ref_adj) < 5e-6
     assert rel_l2(out[True, lib.MIXED][0], out[False, lib.MIXED][0]) < 2e-6
+    # duality of the symmetric near field: <lam, K sg> = <K^T lam, sg>
+    lhs, rhs = float(lam @ out[True, lib.FP64][0]), float(out[True, lib.FP64][3] @ sg)
+    assert abs(lhs - rhs) <= 1e-12 * np.linalg.norm(lam) * np.linalg.norm(out[True, lib.FP64][0])
 
 
 def test_apply_alpha_beta_semantics(case_dir, golden_meta, oracles):
