@@ -646,19 +646,23 @@ def run_ours(args):
         peak_src = "measured FP64 FMA rate of this GPU (DFMA chains, fabipb_b200_simt_peak)"
     # DRAM bytes per launch from the committed ncu summary of this kernel and
     # workload, or of the smaller capture that stands in for it, scaled by panels
-    kname = "near_apply_f2_kernel<0>" if prec == lib.MIXED else "near_apply_kernel<double,0>"
-    kfile = "near_apply_f2_kernel" if prec == lib.MIXED else "near_apply_kernel_double"
+    # the near-field pass: the symmetric kernel (unordered leaf pairs) and the ordered kernel (self
+    # pairs, scratch sums, FP64 special pairs), timed together as one apply
+    kname = ("near_sym_f2_kernel<0> + near_apply_f2_kernel<0>" if prec == lib.MIXED
+             else "near_sym_kernel<double,0> + near_apply_kernel<double,0>")
+    kfiles = (("near_sym_f2_kernel", "near_apply_f2_kernel") if prec == lib.MIXED
+              else ("near_sym_kernel_double", "near_apply_kernel_double"))
     traffic, traffic_src = None, None
-    for case, scale in ((args.case, 1.0),) + tuple(PROFILE_PROXY.get(args.case, ())):
-        prof = os.path.join(ROOT, "profiles", "%s_%s.md" % (kfile, case))
-        if os.path.exists(prof):
-            with open(prof) as fp:
-                m = re.search(r"dram_bytes_per_launch \| (\d+)", fp.read())
-            if m:
-                traffic = int(int(m.group(1)) * scale)
-                traffic_src = "ncu capture of %s%s" % (case, "" if scale == 1.0 else
-                                                       ", scaled by panels (x%.2f)" % scale)
-                break
+    for kfile in kfiles:
+        for case, scale in ((args.case, 1.0),) + tuple(PROFILE_PROXY.get(args.case, ())):
+            prof = os.path.join(ROOT, "profiles", "%s_%s.md" % (kfile, case))
+            if traffic is None and os.path.exists(prof):
+                with open(prof) as fp:
+                    m = re.search(r"dram_bytes_per_launch[^|]*\| (\d+)", fp.read())
+                if m:
+                    traffic = int(int(m.group(1)) * scale)
+                    traffic_src = "ncu capture %s of %s%s" % (os.path.basename(prof), case, "" if scale == 1.0 else
+                                                              ", scaled by panels (x%.2f)" % scale)
     passes = pass_report(surf, info, x.data_ptr(), flush, args.steps, prec == lib.MIXED, fp32_peak, fp64_peak)
     free, total = torch.cuda.mem_get_info()
     mem_ctx = (total - free) / 2**30
