@@ -562,14 +562,16 @@ near_sym_f2_kernel(int nTasks, const int4 *__restrict__ tasks, const int *__rest
         sa = recA[tb + j0 + lane];
         sb = recB[tb + j0 + lane];
       }
+      // slot m holds source m first and source m + 16 (mod 32, the lane m ^ 16) second
+      const float ox = __shfl_xor_sync(0xffffffffu, sa.x, 16), oy = __shfl_xor_sync(0xffffffffu, sa.y, 16);
+      const float oz = __shfl_xor_sync(0xffffffffu, sa.z, 16), ow = __shfl_xor_sync(0xffffffffu, sa.w, 16);
+      const float px = __shfl_xor_sync(0xffffffffu, sb.x, 16), py = __shfl_xor_sync(0xffffffffu, sb.y, 16);
+      const float pz = __shfl_xor_sync(0xffffffffu, sb.z, 16), pw = __shfl_xor_sync(0xffffffffu, sb.w, 16);
       __syncwarp();   // the previous tile's reads are done
-      {
-        const int o = (lane + 16) & 31;   // the slot that holds this source second
-        Q[0][lane].x = -sa.x; Q[0][lane].z = -sa.y; Q[0][o].y = -sa.x; Q[0][o].w = -sa.y;
-        Q[1][lane].x = -sa.z; Q[1][lane].z = sa.w;  Q[1][o].y = -sa.z; Q[1][o].w = sa.w;
-        Q[2][lane].x = sb.x;  Q[2][lane].z = sb.y;  Q[2][o].y = sb.x;  Q[2][o].w = sb.y;
-        Q[3][lane].x = sb.z;  Q[3][lane].z = sb.w;  Q[3][o].y = sb.z;  Q[3][o].w = sb.w;
-      }
+      Q[0][lane] = make_float4(-sa.x, -ox, -sa.y, -oy);
+      Q[1][lane] = make_float4(-sa.z, -oz, sa.w, ow);
+      Q[2][lane] = make_float4(sb.x, px, sb.y, py);
+      Q[3][lane] = make_float4(sb.z, pz, sb.w, pw);
       __syncwarp();
       float2 own = f2(0.f);   // this lane's source j0+lane: (pot, dpdn) from the group's 32 targets
 #pragma unroll 4
