@@ -482,8 +482,8 @@ static void launch_walk(Context &c, int mode, const double *sgm, double *rhs, do
   ChargeTreeDev &d = *c.ct;
   // the screened-only walk uses the RHS acceptance ratio (treecode.c:731)
   const double theta = (mode == 1) ? c.prm.energy_theta : c.prm.rhs_theta;
-  // the energy walks of a mixed context in FP32 (the RHS walk stays FP64)
-  auto kern = (c.mixed && mode != 0) ? tree_walk_kernel<PM, float> : tree_walk_kernel<PM, double>;
+  // the walks of a mixed context (RHS and energy) with FP32 cluster and direct terms, FP64 sums
+  auto kern = c.mixed ? tree_walk_kernel<PM, float> : tree_walk_kernel<PM, double>;
   kern<<<ceil_div(c.n, 256), 256, 0, c.stream>>>(
       mode, c.n, c.prm.quad_order, c.d_vtx, c.d_nrm, c.d_area, theta, d.height, d.depth, c.prm.kappa, c.epsilon,
       c.NM, d.d_ctr, d.d_rad, d.d_level, d.d_kidStart, d.d_kidCount, d.d_itemStart, d.d_itemCount, d.d_order,
