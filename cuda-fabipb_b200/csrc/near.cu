@@ -470,6 +470,10 @@ near_apply_f2_kernel(int nWork, const int2 *__restrict__ work, const int *__rest
 #ifndef FB_NEAR_SYM_MIN_LEAF
 #define FB_NEAR_SYM_MIN_LEAF 48
 #endif
+#ifndef FB_NEAR_SYM_UNROLL
+#define FB_NEAR_SYM_UNROLL 4
+#endif
+constexpr int kSymUnroll = FB_NEAR_SYM_UNROLL;
 constexpr int kSymWarps = 4;
 
 template <bool ADJ>
@@ -574,7 +578,7 @@ near_sym_f2_kernel(int nTasks, const int4 *__restrict__ tasks, const int *__rest
       Q[3][lane] = make_float4(sb.z, pz, sb.w, pw);
       __syncwarp();
       float2 own = f2(0.f);   // this lane's source j0+lane: (pot, dpdn) from the group's 32 targets
-#pragma unroll 4
+#pragma unroll kSymUnroll
       for (int st = 0; st < 16; st++) {
         const int slot = (lane + st) & 31;
         float2 s0, s1;
