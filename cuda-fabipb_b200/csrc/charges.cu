@@ -11,14 +11,17 @@
 //   energy walk     energyTreeWalk/panelEnergyTree, src/treecode.c:581-695,
 //                   summed as in panelEnergyWorker, src/treecode.c:869-887
 //
-// Each walk is one thread per panel with an explicit stack that pops the
-// children in index order, i.e. the reference's depth-first recursion and
-// its summation order.  Accepted clusters evaluate the Cartesian derivative
-// tensor (fmm.cu derivs<>) to order p+1 and contract it with the cluster
-// moments; leaves sum their charges directly.  All in FP64; the energy is
-// reduced per block and then in block order, so it is deterministic.
+// Each walk gives every panel point the reference's depth-first recursion
+// and its summation order (children in index order); a warp walks its 32
+// points together with one stack of (cube, lane mask) entries.  Accepted
+// clusters evaluate the Cartesian derivative tensor to order p+1 (unrolled
+// into registers) and contract it with the cluster moments; leaves sum their
+// charges directly.  FP64, or FP32 terms with FP64 sums in mixed contexts;
+// the energy is reduced per block and then in block order, so it is
+// deterministic.
 #include <algorithm>
 #include <cstring>
+#include <utility>
 
 #include "context.cuh"
 #include "quad.cuh"
@@ -33,7 +36,7 @@ struct ChargeTreeDev {
   double *d_ctr = nullptr, *d_rad = nullptr;
   int *d_level = nullptr, *d_kidStart = nullptr, *d_kidCount = nullptr;
   int *d_itemStart = nullptr, *d_itemCount = nullptr, *d_order = nullptr;
-  double *d_mom = nullptr;                     // nCubes x NM
+  void *d_smom = nullptr;   // nCubes x NM signed moments (-1)^|i| M_i, FP32 in mixed contexts
   double *d_partial = nullptr;                 // energy partial sums
   int partialCap = 0;
   double *d_posOrig = nullptr, *d_chrOrig = nullptr;  // input order (direct RHS)
@@ -171,9 +174,24 @@ static bool build_charge_tree(Context &c) {
       !d.arena.upload(&d.d_ctr, t.x, s) || !d.arena.upload(&d.d_rad, t.rad, s) ||
       !d.arena.upload(&d.d_level, t.level, s) || !d.arena.upload(&d.d_kidStart, t.kidStart, s) ||
       !d.arena.upload(&d.d_kidCount, t.kidCount, s) || !d.arena.upload(&d.d_itemStart, t.itemStart, s) ||
-      !d.arena.upload(&d.d_itemCount, t.itemCount, s) || !d.arena.upload(&d.d_order, order, s) ||
-      !d.arena.upload(&d.d_mom, mom, s))
+      !d.arena.upload(&d.d_itemCount, t.itemCount, s) || !d.arena.upload(&d.d_order, order, s))
     return false;
+  // the walks contract (-1)^|i| M_i (the sign of D^i taken at the point rather
+  // than at the cube); a mixed context's walks read them in FP32
+  for (size_t cc = 0; cc < (size_t)t.nCubes; cc++)
+    for (int i = 0; i < NM; i++)
+      if ((mi[3 * i] + mi[3 * i + 1] + mi[3 * i + 2]) & 1) mom[cc * NM + i] = -mom[cc * NM + i];
+  if (c.mixed) {
+    std::vector<float> smf(mom.begin(), mom.end());
+    float *p = nullptr;
+    if (!d.arena.upload(&p, smf, s)) return false;
+    d.d_smom = p;
+    FB_CUDA(cudaStreamSynchronize(s));
+  } else {
+    double *p = nullptr;
+    if (!d.arena.upload(&p, mom, s)) return false;
+    d.d_smom = p;
+  }
   FB_CUDA(cudaStreamSynchronize(s));  // host vectors above are about to go out of scope
   d.built = true;
   return true;
@@ -318,138 +336,344 @@ rhs_direct_f2_kernel(int n, int m, const double *__restrict__ vtx, const double 
 }
 
 // ---------------------------------------------------------------------------
-// charge-tree walks: mode 0 = RHS (Coulomb), mode 1 = energy (G0 - Gk)
+// charge-tree walks: mode 0 = RHS (Coulomb), 1 = energy (G0 - Gk), 2 = the
+// screened term alone (the plugin ABI's energy of a reused RHS)
 // ---------------------------------------------------------------------------
-// T = float (the energy walks of a mixed context): derivative tables, their
-// contraction and the direct leaf terms in FP32 (the point-to-cluster
-// offsets in FP64, then rounded); the per-panel sums stay FP64.
-template <int PM, typename T = double>
-__device__ void walk_point(int mode, const double *qp, const double *nxd, double theta, int height, int depth,
-                           double kappad, double epsd, int NM, const double *__restrict__ ctr,
-                           const double *__restrict__ rad, const int *__restrict__ level,
-                           const int *__restrict__ kidStart, const int *__restrict__ kidCount,
-                           const int *__restrict__ itemStart, const int *__restrict__ itemCount,
-                           const int *__restrict__ order, const double *__restrict__ mom,
-                           const double *__restrict__ pos, const double *__restrict__ chr, double *y) {
+// A warp walks the charge tree for its 32 points (consecutive panels in tree
+// order, so neighbours in space) together.  Its stack, in shared memory,
+// holds (cube, lane mask) entries.  At a cube every lane of the mask makes its
+// own acceptance test; the accepting lanes evaluate the cube's expansion
+// together, the lanes at a leaf sum its charges, and the children are pushed
+// (last child first) with the mask of the lanes that go on into them.  Each
+// lane therefore visits exactly the cubes of its own depth-first walk, in the
+// reference's order, while the cube records and the moments are read once per
+// warp and every expansion runs at a warp-uniform order.
+//
+// The expansion: the derivative tensor of the radial kernel by the level
+// recursion of derivs_inplace, unrolled at compile time for each order so
+// that the tensor lives in registers, contracted with the signed moments
+// (-1)^|i| M_i.  By linearity of the recursion in its radial sequence, the
+// energy's  sum M_i D^i (G0 - Gk)  and  sum M_i n.grad D^i (eps Gk - G0)  are
+// two tensors of the combined sequences (the first only to order p).  T = float
+// (mixed contexts): tensors, contraction and the leaves' pair terms in FP32,
+// point-to-cube offsets in FP64 and then rounded; the per-panel sums in FP64.
+constexpr int kWalkThreads = 256;
+constexpr int kWalkStack = 8 * 20 + 4;   // depth <= 20: at most 7 per level + 2 entries wait
+
+struct WalkTree {
+  const double *ctr, *rad, *pos, *chr;
+  const int *level, *kidStart, *kidCount, *itemStart, *itemCount, *order;
+  const void *smom;   // nCubes x NM signed moments, T
+  double theta;
+  int height, depth, NM;
+};
+
+// the multi-index at graded position i (the inverse of fmm.cu's gidx)
+struct Tri { int a, b, c; };
+__host__ __device__ constexpr Tri gmi(int i) {
+  for (int n = 0; n < 64; n++)
+    for (int a = 0; a <= n; a++)
+      for (int b = 0; b <= n - a; b++)
+        if (i-- == 0) return Tri{a, b, n - a - b};
+  return Tri{0, 0, 0};
+}
+
+// One step of the level recursion of derivs_inplace: kind 0 sets entry 0 to
+// the radial term G[p]; kind 1 sets d[e] = d[a] x[axis] + fb d[b] (b < 0: no
+// second term).
+struct DerivOp { int kind, e, a, b, axis, fb, p; };
+__host__ __device__ constexpr int deriv_ops(int order) {
+  int s = 1;
+  for (int p = order - 1; p >= 0; p--) s += nmom_c(order - p);
+  return s;
+}
+__host__ __device__ constexpr DerivOp deriv_op(int order, int s) {
+  if (s == 0) return DerivOp{0, 0, 0, -1, 0, 0, order};
+  s--;
+  for (int p = order - 1; p >= 0; p--) {
+    for (int e = nmom_c(order - p) - 1; e >= 1; e--, s--) {
+      if (s != 0) continue;
+      const Tri m = gmi(e);
+      if (m.a >= 1)
+        return DerivOp{1, e, gidx(m.a - 1, m.b, m.c), m.a >= 2 ? gidx(m.a - 2, m.b, m.c) : -1, 0, m.a - 1, 0};
+      if (m.b >= 1)
+        return DerivOp{1, e, gidx(0, m.b - 1, m.c), m.b >= 2 ? gidx(0, m.b - 2, m.c) : -1, 1, m.b - 1, 0};
+      return DerivOp{1, e, gidx(0, 0, m.c - 1), m.c >= 2 ? gidx(0, 0, m.c - 2) : -1, 2, m.c - 1, 0};
+    }
+    if (s == 0) return DerivOp{0, 0, 0, -1, 0, 0, p};
+    s--;
+  }
+  return DerivOp{0, 0, 0, -1, 0, 0, 0};
+}
+
+template <int ORDER, int S, typename T>
+__device__ __forceinline__ void deriv_step(T *d, const T *x, const T *G) {
+  constexpr DerivOp op = deriv_op(ORDER, S);
+  if constexpr (op.kind == 0) d[0] = G[op.p];
+  else if constexpr (op.b < 0) d[op.e] = d[op.a] * x[op.axis];
+  else d[op.e] = d[op.a] * x[op.axis] + d[op.b] * (T)op.fb;
+}
+template <int ORDER, typename T, int... S>
+__device__ __forceinline__ void deriv_steps(T *d, const T *x, const T *G, std::integer_sequence<int, S...>) {
+  (deriv_step<ORDER, S>(d, x, G), ...);
+}
+// D^e G for |e| <= ORDER from the radial sequence G[0..ORDER], into registers
+template <int ORDER, typename T>
+__device__ __forceinline__ void deriv_table(T *d, const T *x, const T *G) {
+  deriv_steps<ORDER>(d, x, G, std::make_integer_sequence<int, deriv_ops(ORDER)>{});
+}
+
+// y0 += sum_I sm_I d_I;  g_k += sum_I sm_I d_{I + e_k}
+template <bool Y0, bool Y1, int I, typename T>
+__device__ __forceinline__ void contract_step(const T *__restrict__ sm, const T *d, T &y0, T &g0, T &g1, T &g2) {
+  constexpr Tri m = gmi(I);
+  constexpr int e1 = gidx(m.a + 1, m.b, m.c), e2 = gidx(m.a, m.b + 1, m.c), e3 = gidx(m.a, m.b, m.c + 1);
+  const T s = sm[I];
+  if constexpr (Y0) y0 += s * d[I];
+  if constexpr (Y1) {
+    g0 += s * d[e1];
+    g1 += s * d[e2];
+    g2 += s * d[e3];
+  }
+}
+template <bool Y0, bool Y1, typename T, int... I>
+__device__ __forceinline__ void contract(const T *__restrict__ sm, const T *d, T &y0, T &g0, T &g1, T &g2,
+                                         std::integer_sequence<int, I...>) {
+  (contract_step<Y0, Y1, I>(sm, d, y0, g0, g1, g2), ...);
+}
+
+// Radial sequences of derivs_inplace: G0[k] = (1/r d/dr)^k (1/(4 pi r)), and
+// the screened Gk (src/kernel.c:84-104), for k <= K.
+template <int K, typename T>
+__device__ __forceinline__ void radial_coulomb(T r, T *G0) {
+  const T r2 = (T)-1 / (r * r);
+  G0[0] = (T)kFourPiI / r;
+#pragma unroll
+  for (int k = 0; k < K; k++) G0[k + 1] = (T)(2 * k + 1) * r2 * G0[k];
+}
+template <int K, typename T>
+__device__ __forceinline__ void radial_screened(T r, T kappa, T *G0, T *Gk) {
+  const T rexp = exp(-kappa * r), r1 = (T)1 / r, rr2 = r1 * r1, nr2 = -rr2, k2 = kappa * kappa;
+  G0[0] = r1 * (T)kFourPiI;
+  Gk[0] = rexp * G0[0];
+  if constexpr (K >= 1) {
+    G0[1] = nr2 * G0[0];
+    Gk[1] = -Gk[0] * (rr2 + kappa * r1);
+  }
+#pragma unroll
+  for (int k = 1; k < K; k++) {
+    G0[k + 1] = (T)(2 * k + 1) * nr2 * G0[k];
+    Gk[k + 1] = rr2 * (k2 * Gk[k - 1] - (T)(2 * k + 1) * Gk[k]);
+  }
+}
+
+// The terms of one accepted cube of expansion order ORD at offset x from the
+// point: y0 (potential) and y1 (normal derivative) of the walk's mode.
+template <int ORD, typename T, int MODE>
+__device__ __forceinline__ void cube_terms(const T *__restrict__ sm, const T *x, const T *nx, T kappa, T eps, T &y0,
+                                           T &y1) {
+  using Moments = std::make_integer_sequence<int, nmom_c(ORD)>;
+  const T r = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+  T a0 = (T)0, g0 = (T)0, g1 = (T)0, g2 = (T)0;
+  if constexpr (MODE == 0) {
+    T G[ORD + 2], d[nmom_c(ORD + 1)];
+    radial_coulomb<ORD + 1>(r, G);
+    deriv_table<ORD + 1>(d, x, G);
+    contract<true, true>(sm, d, a0, g0, g1, g2, Moments{});
+    y0 = a0;
+    y1 = nx[0] * g0 + nx[1] * g1 + nx[2] * g2;
+  } else if constexpr (MODE == 1) {
+    T G0[ORD + 2], Gk[ORD + 2], H[ORD + 2];
+    radial_screened<ORD + 1>(r, kappa, G0, Gk);
+    {
+      T d[nmom_c(ORD)];
+#pragma unroll
+      for (int k = 0; k <= ORD; k++) H[k] = G0[k] - Gk[k];
+      deriv_table<ORD>(d, x, H);
+      contract<true, false>(sm, d, a0, g0, g1, g2, Moments{});
+    }
+    {
+      T d[nmom_c(ORD + 1)];
+#pragma unroll
+      for (int k = 0; k <= ORD + 1; k++) H[k] = eps * Gk[k] - G0[k];
+      deriv_table<ORD + 1>(d, x, H);
+      contract<false, true>(sm, d, a0, g0, g1, g2, Moments{});
+    }
+    y0 = a0;
+    y1 = nx[0] * g0 + nx[1] * g1 + nx[2] * g2;
+  } else {
+    T G0[ORD + 2], Gk[ORD + 2], d[nmom_c(ORD + 1)];
+    radial_screened<ORD + 1>(r, kappa, G0, Gk);
+    deriv_table<ORD + 1>(d, x, Gk);
+    contract<true, true>(sm, d, a0, g0, g1, g2, Moments{});
+    y0 = a0;
+    y1 = eps * (nx[0] * g0 + nx[1] * g1 + nx[2] * g2);
+  }
+}
+
+// Orders above the unrolled ones: the runtime recursion with the tensors in
+// local memory.
+template <int PM, typename T, int MODE>
+__device__ __noinline__ void cube_terms_generic(int ord, const T *__restrict__ sm, const T *x, const T *nx, T kappa,
+                                                T eps, T &y0, T &y1) {
   constexpr int ND = nmom_c(PM);
-  int stack[8 * 20 + 4];
-  int sp = 0;
-  stack[sp++] = 0;
   T d0[ND], dk[ND];
-  const T nx[3] = {(T)nxd[0], (T)nxd[1], (T)nxd[2]};
-  const T kappa = (T)kappad, eps = (T)epsd;
+  derivs_inplace<PM, T>(ord + 1, x, kappa, MODE == 0, d0, dk, 1);
+  T a0 = (T)0, a1 = (T)0;
+  for (int i = 0, nmo = nmom(ord); i < nmo; i++) {
+    const char4 a = c_mi[i];
+    const int e1 = IDX(a.x + 1, a.y, a.z), e2 = IDX(a.x, a.y + 1, a.z), e3 = IDX(a.x, a.y, a.z + 1);
+    const T s = sm[i];
+    if (MODE == 0) {
+      a0 += s * d0[i];
+      a1 += s * (nx[0] * d0[e1] + nx[1] * d0[e2] + nx[2] * d0[e3]);
+    } else if (MODE == 2) {
+      a0 += s * dk[i];
+      a1 += s * eps * (nx[0] * dk[e1] + nx[1] * dk[e2] + nx[2] * dk[e3]);
+    } else {
+      a0 += s * (d0[i] - dk[i]);
+      a1 += s * (eps * (nx[0] * dk[e1] + nx[1] * dk[e2] + nx[2] * dk[e3]) -
+                 (nx[0] * d0[e1] + nx[1] * d0[e2] + nx[2] * d0[e3]));
+    }
+  }
+  y0 = a0;
+  y1 = a1;
+}
+
+// unrolled up to order 6 (FP32) or 5 (FP64, whose tensors take twice the registers)
+template <typename T>
+__host__ __device__ constexpr int walk_unroll_max() { return sizeof(T) == 4 ? 6 : 5; }
+
+template <int ORD, int PM, typename T, int MODE>
+__device__ __forceinline__ void cube_dispatch(int ord, const T *__restrict__ sm, const T *x, const T *nx, T kappa,
+                                              T eps, T &y0, T &y1) {
+  if constexpr (ORD < PM && ORD <= walk_unroll_max<T>()) {
+    if (ord == ORD) {
+      cube_terms<ORD, T, MODE>(sm, x, nx, kappa, eps, y0, y1);
+      return;
+    }
+    cube_dispatch<ORD + 1, PM, T, MODE>(ord, sm, x, nx, kappa, eps, y0, y1);
+  } else if constexpr (ORD < PM) {
+    cube_terms_generic<PM, T, MODE>(ord, sm, x, nx, kappa, eps, y0, y1);
+  }
+}
+
+// The walk of one point per lane; lanes with active == false only take part in
+// the warp's collective steps.  y[] accumulates in the lane's visiting order.
+template <int PM, typename T, int MODE>
+__device__ __forceinline__ void walk_warp(const WalkTree &t, bool active, const double *qp, const T *nx, T kappa,
+                                          T eps, double *y, int2 *stk) {
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned all = __ballot_sync(0xffffffffu, active);
+  if (all == 0u) return;
+  if (lane == 0) stk[0] = make_int2(0, (int)all);
+  __syncwarp();
+  int sp = 1;
   while (sp > 0) {
-    const int c = stack[--sp];
-    double r[3] = {qp[0] - ctr[3 * c], qp[1] - ctr[3 * c + 1], qp[2] - ctr[3 * c + 2]};
-    const double dist = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-    if (rad[c] < theta * dist && level[c] >= height) {
-      const int ord = order[c], nmo = nmom(ord);
-      const T rt[3] = {(T)r[0], (T)r[1], (T)r[2]};
-      derivs_inplace<PM, T>(ord + 1, rt, kappa, mode == 0, d0, dk, 1);
-      const double *mc = mom + (size_t)c * NM;
+    const int2 top = stk[--sp];
+    __syncwarp();   // every lane has read the entry before lane 0 may reuse its slot
+    const int c = top.x;
+    const unsigned mask = (unsigned)top.y;
+    const bool in = (mask >> lane) & 1u;
+    const double r0 = qp[0] - t.ctr[3 * (size_t)c], r1 = qp[1] - t.ctr[3 * (size_t)c + 1],
+                 r2 = qp[2] - t.ctr[3 * (size_t)c + 2];
+    const int lev = t.level[c];
+    const bool acc = in && t.rad[c] < t.theta * sqrt(r0 * r0 + r1 * r1 + r2 * r2) && lev >= t.height;
+    const unsigned accMask = __ballot_sync(0xffffffffu, acc);
+    if (acc) {
+      const T x[3] = {(T)r0, (T)r1, (T)r2};
       T y0 = (T)0, y1 = (T)0;
-      for (int i = 0; i < nmo; i++) {
-        const char4 a = c_mi[i];
-        const int e1 = IDX(a.x + 1, a.y, a.z), e2 = IDX(a.x, a.y + 1, a.z), e3 = IDX(a.x, a.y, a.z + 1);
-        const T sm = (T)(c_sgn3[i] * mc[i]);
-        if (mode == 0) {
-          y0 += sm * d0[i];
-          y1 += sm * (nx[0] * d0[e1] + nx[1] * d0[e2] + nx[2] * d0[e3]);
-        } else if (mode == 2) {
-          y0 += sm * dk[i];
-          y1 += sm * eps * (nx[0] * dk[e1] + nx[1] * dk[e2] + nx[2] * dk[e3]);
-        } else {
-          y0 += sm * (d0[i] - dk[i]);
-          const T dn0 = nx[0] * d0[e1] + nx[1] * d0[e2] + nx[2] * d0[e3];
-          const T dnk = nx[0] * dk[e1] + nx[1] * dk[e2] + nx[2] * dk[e3];
-          y1 += sm * (eps * dnk - dn0);
-        }
-      }
-      if (mode == 0) {
+      cube_dispatch<0, PM, T, MODE>(t.order[c], static_cast<const T *>(t.smom) + (size_t)c * t.NM, x, nx, kappa,
+                                    eps, y0, y1);
+      if (MODE == 0) {
         y[0] += (double)y0 / kFourPiI;
         y[1] += (double)y1 / kFourPiI;
       } else {
         y[0] += (double)y0;
         y[1] += (double)y1;
       }
-      continue;
     }
-    if (level[c] == depth) {
-      const int s0 = itemStart[c], s1 = s0 + itemCount[c];
-      for (int j = s0; j < s1; j++) {
-        const T x[3] = {(T)(qp[0] - pos[3 * (size_t)j]), (T)(qp[1] - pos[3 * (size_t)j + 1]),
-                        (T)(qp[2] - pos[3 * (size_t)j + 2])};
-        const T r2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
-        const T ip = nx[0] * x[0] + nx[1] * x[1] + nx[2] * x[2];
-        const T q = (T)chr[j];
-        if (mode == 0) {
-          const T ri = (T)1 / sqrt(r2), r3i = ri / r2;
-          y[0] += (double)(q * ri);
-          y[1] += (double)(q * (-ip * r3i));
-        } else {
-          const T rn = sqrt(r2), G0 = (T)kFourPiI / rn, ek = exp(-kappa * rn);
-          const T Gk = ek * G0, coef = (kappa * rn + (T)1) * ek;
-          const T dG0dn = -ip * G0 / r2, dGkdn = coef * dG0dn;
-          if (mode == 2) {
-            y[0] += (double)(q * Gk);
-            y[1] += (double)(q * eps * dGkdn);
+    const unsigned rest = mask & ~accMask;
+    if (rest == 0u) continue;
+    if (lev == t.depth) {
+      if (in && !acc) {
+        for (int j = t.itemStart[c], j1 = j + t.itemCount[c]; j < j1; j++) {
+          const T x[3] = {(T)(qp[0] - t.pos[3 * (size_t)j]), (T)(qp[1] - t.pos[3 * (size_t)j + 1]),
+                          (T)(qp[2] - t.pos[3 * (size_t)j + 2])};
+          const T rr2 = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+          const T ip = nx[0] * x[0] + nx[1] * x[1] + nx[2] * x[2];
+          const T q = (T)t.chr[j];
+          if (MODE == 0) {
+            const T ri = (T)1 / sqrt(rr2), r3i = ri / rr2;
+            y[0] += (double)(q * ri);
+            y[1] += (double)(q * (-ip * r3i));
           } else {
-            y[0] += (double)(q * (G0 - Gk));
-            y[1] += (double)(q * (eps * dGkdn - dG0dn));
+            const T rn = sqrt(rr2), G0 = (T)kFourPiI / rn, ek = exp(-kappa * rn);
+            const T Gk = ek * G0, coef = (kappa * rn + (T)1) * ek;
+            const T dG0dn = -ip * G0 / rr2, dGkdn = coef * dG0dn;
+            if (MODE == 2) {
+              y[0] += (double)(q * Gk);
+              y[1] += (double)(q * eps * dGkdn);
+            } else {
+              y[0] += (double)(q * (G0 - Gk));
+              y[1] += (double)(q * (eps * dGkdn - dG0dn));
+            }
           }
         }
       }
       continue;
     }
-    // children pop in index order
-    for (int k = kidCount[c] - 1; k >= 0; k--) stack[sp++] = kidStart[c] + k;
+    const int k0 = t.kidStart[c], nk = t.kidCount[c];
+    if (sp + nk > kWalkStack) break;   // unreachable: the host caps the depth at 20
+    if (lane == 0)
+      for (int k = 0; k < nk; k++) stk[sp + k] = make_int2(k0 + nk - 1 - k, (int)rest);   // first child on top
+    sp += nk;
+    __syncwarp();
   }
 }
 
-template <int PM, typename T>
-__global__ void tree_walk_kernel(int mode, int n, int q, const double *__restrict__ vtx, const double *__restrict__ nrm,
-                                 const double *__restrict__ area, double theta, int height, int depth, double kappa,
-                                 double eps, int NM, const double *__restrict__ ctr, const double *__restrict__ rad,
-                                 const int *__restrict__ level, const int *__restrict__ kidStart,
-                                 const int *__restrict__ kidCount, const int *__restrict__ itemStart,
-                                 const int *__restrict__ itemCount, const int *__restrict__ order,
-                                 const double *__restrict__ mom, const double *__restrict__ pos,
-                                 const double *__restrict__ chr, double fac, const double *__restrict__ sgm,
-                                 double *rhs, double *partial) {
-  __shared__ double red[256];
+template <int PM, typename T, int MODE>
+__global__ void __launch_bounds__(kWalkThreads)
+tree_walk_kernel(int n, int q, const double *__restrict__ vtx, const double *__restrict__ nrm,
+                 const double *__restrict__ area, WalkTree t, double kappa, double eps, double fac,
+                 const double *__restrict__ sgm, double *rhs, double *partial) {
+  __shared__ int2 stk[kWalkThreads / 32][kWalkStack];
+  __shared__ double red[kWalkThreads];
   const int X = blockIdx.x * blockDim.x + threadIdx.x;
-  double e = 0.0;
-  if (X < n) {
-    const double *v0 = vtx + 9 * (size_t)X;
-    double ax2[3], ax0[3], nx[3];
-    for (int k = 0; k < 3; k++) {
-      ax2[k] = v0[3 + k] - v0[k];
-      ax0[k] = v0[6 + k] - v0[3 + k];
-      nx[k] = nrm[3 * (size_t)X + k];
+  const bool valid = X < n;
+  const int Xs = valid ? X : 0;
+  const double *v0 = vtx + 9 * (size_t)Xs;
+  double ax2[3], ax0[3];
+  T nx[3];
+  for (int k = 0; k < 3; k++) {
+    ax2[k] = v0[3 + k] - v0[k];
+    ax0[k] = v0[6 + k] - v0[3 + k];
+    nx[k] = (T)nrm[3 * (size_t)Xs + k];
+  }
+  const double *tq = c_tLeg[q], *w = c_wLeg[q];
+  double o0 = 0.0, o1 = 0.0;
+  for (int ix = 0; ix < q; ix++)
+    for (int jx = 0; jx < q; jx++) {
+      double qp[3], y[2] = {0.0, 0.0};
+      for (int k = 0; k < 3; k++) qp[k] = v0[k] + tq[ix] * (ax2[k] + tq[jx] * ax0[k]);
+      walk_warp<PM, T, MODE>(t, valid, qp, nx, (T)kappa, (T)eps, y, stk[threadIdx.x >> 5]);
+      o0 += y[0] * tq[ix] * w[ix] * w[jx];
+      o1 += y[1] * tq[ix] * w[ix] * w[jx];
     }
-    const double *t = c_tLeg[q], *w = c_wLeg[q];
-    double o0 = 0.0, o1 = 0.0;
-    for (int ix = 0; ix < q; ix++)
-      for (int jx = 0; jx < q; jx++) {
-        double qp[3], y[2] = {0.0, 0.0};
-        for (int k = 0; k < 3; k++) qp[k] = v0[k] + t[ix] * (ax2[k] + t[jx] * ax0[k]);
-        walk_point<PM, T>(mode, qp, nx, theta, height, depth, kappa, eps, NM, ctr, rad, level, kidStart, kidCount,
-                       itemStart, itemCount, order, mom, pos, chr, y);
-        o0 += y[0] * t[ix] * w[ix] * w[jx];
-        o1 += y[1] * t[ix] * w[ix] * w[jx];
-      }
+  double e = 0.0;
+  if (valid) {
     o0 *= 2.0 * area[X];
     o1 *= 2.0 * area[X];
-    if (mode == 0) {
+    if (MODE == 0) {
       rhs[X] = fac * o0;
       rhs[n + X] = fac * o1;
-    } else if (mode == 2) {
+    } else if (MODE == 2) {
       e = -o0 * sgm[X + n] + o1 * sgm[X];   // rhsReuseEnergyWorker, treecode.c:889-910
     } else {
       e = o0 * sgm[X + n] + o1 * sgm[X];
     }
   }
-  if (mode != 0) {
+  if (MODE != 0) {
     red[threadIdx.x] = e;
     __syncthreads();
     for (int s = blockDim.x / 2; s > 0; s >>= 1) {
@@ -482,12 +706,16 @@ static void launch_walk(Context &c, int mode, const double *sgm, double *rhs, do
   ChargeTreeDev &d = *c.ct;
   // the screened-only walk uses the RHS acceptance ratio (treecode.c:731)
   const double theta = (mode == 1) ? c.prm.energy_theta : c.prm.rhs_theta;
-  // the walks of a mixed context (RHS and energy) with FP32 cluster and direct terms, FP64 sums
-  auto kern = c.mixed ? tree_walk_kernel<PM, float> : tree_walk_kernel<PM, double>;
-  kern<<<ceil_div(c.n, 256), 256, 0, c.stream>>>(
-      mode, c.n, c.prm.quad_order, c.d_vtx, c.d_nrm, c.d_area, theta, d.height, d.depth, c.prm.kappa, c.epsilon,
-      c.NM, d.d_ctr, d.d_rad, d.d_level, d.d_kidStart, d.d_kidCount, d.d_itemStart, d.d_itemCount, d.d_order,
-      d.d_mom, d.d_pos, d.d_chr, c.rhsFac != 0.0 ? c.rhsFac : kFourPiI / c.prm.eps1, sgm, rhs, partial);
+  const WalkTree t{d.d_ctr, d.d_rad, d.d_pos, d.d_chr, d.d_level, d.d_kidStart, d.d_kidCount, d.d_itemStart,
+                   d.d_itemCount, d.d_order, d.d_smom, theta, d.height, d.depth, c.NM};
+  // the walks of a mixed context (RHS and energy) with FP32 cube and pair terms, FP64 sums
+  auto kern = c.mixed ? (mode == 0 ? tree_walk_kernel<PM, float, 0>
+                                   : mode == 1 ? tree_walk_kernel<PM, float, 1> : tree_walk_kernel<PM, float, 2>)
+                      : (mode == 0 ? tree_walk_kernel<PM, double, 0>
+                                   : mode == 1 ? tree_walk_kernel<PM, double, 1> : tree_walk_kernel<PM, double, 2>);
+  kern<<<ceil_div(c.n, kWalkThreads), kWalkThreads, 0, c.stream>>>(
+      c.n, c.prm.quad_order, c.d_vtx, c.d_nrm, c.d_area, t, c.prm.kappa, c.epsilon,
+      c.rhsFac != 0.0 ? c.rhsFac : kFourPiI / c.prm.eps1, sgm, rhs, partial);
 }
 
 #define FB_DISPATCH_WALK(P, ...)                      \
