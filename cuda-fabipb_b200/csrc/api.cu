@@ -314,8 +314,12 @@ int create_context(const fabipb_b200_params *p, int n, const double *vtx, const 
   // pairs and M2L lists) and, in a mixed context, the FP64 near-field records
   // of the refinement residuals: built here, once, so that no solve, backward
   // pass or refinement pays for them on its first call
-  ok = ok && setup_near_adjoint(*c) && setup_m2l_adjoint(*c) && (!c->mixed || setup_near_fp64(*c));
-  tm.mark("adjoint_and_refinement_tables");
+  ok = ok && setup_near_adjoint(*c);
+  tm.mark("near_adjoint");
+  ok = ok && setup_m2l_adjoint(*c);
+  tm.mark("m2l_adjoint");
+  ok = ok && (!c->mixed || setup_near_fp64(*c));
+  tm.mark("near_fp64");
   if (ok && cudaStreamSynchronize(c->stream) != cudaSuccess) {
     set_error("setup kernels failed: %s", cudaGetErrorString(cudaGetLastError()));
     ok = false;

@@ -75,6 +75,7 @@ static int charge_order(const Context &c, int level) {
 static bool build_charge_tree(Context &c) {
   ChargeTreeDev &d = *c.ct;
   if (d.built) return true;
+  StageTimer tm("charges", c.stream);
   const int m = c.nChar;
   const double *pos = c.h_pos.data();
   double cminx = pos[0], cmaxx = pos[0], cminy = pos[1], cmaxy = pos[1], cminz = pos[2], cmaxz = pos[2];
@@ -193,6 +194,7 @@ static bool build_charge_tree(Context &c) {
     d.d_smom = p;
   }
   FB_CUDA(cudaStreamSynchronize(s));  // host vectors above are about to go out of scope
+  tm.mark("charge_tree");
   d.built = true;
   return true;
 }
