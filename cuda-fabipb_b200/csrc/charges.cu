@@ -21,6 +21,8 @@
 // deterministic.
 #include <algorithm>
 #include <cstring>
+#include <functional>
+#include <thread>
 #include <utility>
 
 #include "context.cuh"
@@ -131,25 +133,45 @@ static bool build_charge_tree(Context &c) {
       cv[i] *= ifact3[i];
     }
   };
-  std::vector<double> cv(NM);
-  for (int cc = t.levStart[t.depth]; cc < t.levStart[t.depth + 1]; cc++) {
-    int ord = order[cc], nmo = nmom(ord);
-    for (int k = 0; k < t.itemCount[cc]; k++) {
-      int j = sorted[t.itemStart[cc] + k];
-      double tr[3] = {pos[3 * (size_t)j] - t.x[3 * (size_t)cc], pos[3 * (size_t)j + 1] - t.x[3 * (size_t)cc + 1],
-                      pos[3 * (size_t)j + 2] - t.x[3 * (size_t)cc + 2]};
-      conv_vect(ord, tr, cv.data());
-      for (int i = 0; i < nmo; i++) mom[(size_t)cc * NM + i] += c.h_chr[j] * cv[i];
+  // a cube's moments depend only on its own charges or children: the cubes of a level on the
+  // host's cores, each summed in the same order whatever the split
+  auto per_cube = [NM](int c0, int c1, const std::function<void(int, int, double *)> &f) {
+    const int nth = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const int nc = c1 - c0;
+    if (nc < 64 || nth == 1) {
+      std::vector<double> cv(NM);
+      f(c0, c1, cv.data());
+      return;
     }
-  }
+    std::vector<std::thread> pool;
+    for (int th = 0; th < nth; th++)
+      pool.emplace_back([&, th] {
+        std::vector<double> cv(NM);
+        f(c0 + (int)((long long)nc * th / nth), c0 + (int)((long long)nc * (th + 1) / nth), cv.data());
+      });
+    for (auto &th : pool) th.join();
+  };
+  per_cube(t.levStart[t.depth], t.levStart[t.depth + 1], [&](int a, int b, double *cv) {
+    for (int cc = a; cc < b; cc++) {
+      int ord = order[cc], nmo = nmom(ord);
+      for (int k = 0; k < t.itemCount[cc]; k++) {
+        int j = sorted[t.itemStart[cc] + k];
+        double tr[3] = {pos[3 * (size_t)j] - t.x[3 * (size_t)cc], pos[3 * (size_t)j + 1] - t.x[3 * (size_t)cc + 1],
+                        pos[3 * (size_t)j + 2] - t.x[3 * (size_t)cc + 2]};
+        conv_vect(ord, tr, cv);
+        for (int i = 0; i < nmo; i++) mom[(size_t)cc * NM + i] += c.h_chr[j] * cv[i];
+      }
+    }
+  });
   for (int lev = t.depth - 1; lev >= t.height; lev--) {
-    for (int cc = t.levStart[lev]; cc < t.levStart[lev + 1]; cc++) {
+    per_cube(t.levStart[lev], t.levStart[lev + 1], [&](int a, int b, double *cv) {
+    for (int cc = a; cc < b; cc++) {
       int ordOut = order[cc];
       for (int k = 0; k < t.kidCount[cc]; k++) {
         int kid = t.kidStart[cc] + k, nIn = nmom(order[kid]);
         double tr[3] = {t.x[3 * (size_t)kid] - t.x[3 * (size_t)cc], t.x[3 * (size_t)kid + 1] - t.x[3 * (size_t)cc + 1],
                         t.x[3 * (size_t)kid + 2] - t.x[3 * (size_t)cc + 2]};
-        conv_vect(ordOut, tr, cv.data());
+        conv_vect(ordOut, tr, cv);
         int nOut = nmom(ordOut);
         for (int i = 0; i < nOut; i++) {
           int i1 = mi[3 * i], i2 = mi[3 * i + 1], i3 = mi[3 * i + 2];
@@ -164,6 +186,7 @@ static bool build_charge_tree(Context &c) {
         }
       }
     }
+    });
   }
   std::vector<double> spos(3 * (size_t)m), schr(m);
   for (int i = 0; i < m; i++) {

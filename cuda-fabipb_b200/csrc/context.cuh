@@ -50,6 +50,7 @@ struct Context {
   // per near-list entry its scratch offset (-1: the ordered kernel computes it); scratch and
   // records in the context's near-field precision (2 and 4 floats or doubles per entry)
   int nSymTasks = 0;
+  int nSym32 = 0;                              // the first nSym32 tasks are 32-wide, the rest half-warp
   long long symPanelPairs = 0;                 // unordered panel pairs of those leaf pairs
   int4 *d_symTask = nullptr;
   int *d_symOff = nullptr;

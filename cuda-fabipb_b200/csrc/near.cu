@@ -466,9 +466,17 @@ near_apply_f2_kernel(int nWork, const int2 *__restrict__ work, const int *__rest
 #ifndef FB_NEAR_SYM_MIN_BLOCKS
 #define FB_NEAR_SYM_MIN_BLOCKS 6
 #endif
-// leaf pairs whose smaller leaf has fewer panels stay in the ordered kernel
+// leaf pairs whose smaller leaf has fewer panels go to the half-warp kernel (mixed
+// contexts, down to FB_NEAR_SYM16_MIN_LEAF panels; larger pairs too where its
+// padding saves more than its overhead) or stay in the ordered kernel (FP64)
 #ifndef FB_NEAR_SYM_MIN_LEAF
 #define FB_NEAR_SYM_MIN_LEAF 48
+#endif
+#ifndef FB_NEAR_SYM16_MIN_LEAF
+#define FB_NEAR_SYM16_MIN_LEAF 4
+#endif
+#ifndef FB_NEAR_SYM16_COST
+#define FB_NEAR_SYM16_COST 125
 #endif
 #ifndef FB_NEAR_SYM_UNROLL
 #define FB_NEAR_SYM_UNROLL 4
@@ -595,6 +603,91 @@ near_sym_f2_kernel(int nTasks, const int4 *__restrict__ tasks, const int *__rest
         const float2 prev = g0 == 0 ? f2(0.f) : *q;
         *q = __fadd2_rn(prev, own);
       }
+    }
+    if (valid) scr[tk.z + t] = make_float2(acc0.x + acc0.y, acc1.x + acc1.y);
+  }
+}
+
+// The symmetric scheme for leaf pairs that pad badly into 32-panel groups
+// (mixed contexts; every pair whose smaller leaf has fewer than
+// FB_NEAR_SYM_MIN_LEAF panels, and larger ones where 16-panel padding saves
+// more than this kernel's per-tile overhead): each half-warp takes its own
+// leaf pair with 16-panel groups and 16-source tiles, so a pair of 46-panel
+// leaves fills 92% of the lanes instead of the 52% of 32-wide tiles.  In step
+// s of a tile, lane t of the half takes sources (t + s) and (t + s + 8)
+// (mod 16); after 8 steps every source has had all 16 targets.  Shuffles and
+// warp barriers take the half's lane mask, so the two halves may run
+// different trip counts.
+template <bool ADJ>
+__global__ void __launch_bounds__(kSymWarps * 32, FB_NEAR_SYM_MIN_BLOCKS)
+near_sym16_f2_kernel(int nTasks, const int4 *__restrict__ tasks, const int *__restrict__ leafStart,
+                     const int *__restrict__ leafCount, const double *__restrict__ leafCtr,
+                     const float4 *__restrict__ recA, const float4 *__restrict__ recB, float kappa, float kexp,
+                     float eps, float ieps, float kap2, float2 *scr) {
+  __shared__ float4 sQ[kSymWarps][2][4][16];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, half = lane >> 4, hl = lane & 15;
+  const unsigned hm = 0xffffu << (16 * half);
+  const int task = (blockIdx.x * kSymWarps + warp) * 2 + half;
+  if (task >= nTasks) return;  // uniform over the half
+  const int4 tk = tasks[task];
+  const int R = tk.x, T = tk.y;
+  const int rb = leafStart[R], rc = leafCount[R], tb = leafStart[T], tc = leafCount[T];
+  const float sx = (float)(leafCtr[3 * R] - leafCtr[3 * T]);
+  const float sy = (float)(leafCtr[3 * R + 1] - leafCtr[3 * T + 1]);
+  const float sz = (float)(leafCtr[3 * R + 2] - leafCtr[3 * T + 2]);
+  float4(*Q)[16] = sQ[warp][half];
+  for (int g0 = 0; g0 < rc; g0 += 16) {
+    const int t = g0 + hl;
+    const bool valid = t < rc;
+    // a lane past the group's end: far away, zero weights (its terms vanish, its sums are dropped)
+    const float4 a = valid ? recA[rb + t] : make_float4(1e4f, 1e4f, 1e4f, 0.f);
+    const float4 b = valid ? recB[rb + t] : make_float4(0.f, 0.f, 1.f, 0.f);
+    const float2 tx = f2(a.x + sx), ty = f2(a.y + sy), tz = f2(a.z + sz);
+    const float2 tnx = f2(b.x), tny = f2(b.y), tnz = f2(b.z);
+    const float2 wat = f2(a.w), wbt = f2(b.w), watn = f2(-a.w), wbtn = f2(-b.w);
+    float2 acc0 = f2(0.f), acc1 = f2(0.f);
+    // the tile's source j0+hl, or a padding source far away with zero weights; one tile ahead
+    float4 na = make_float4(-1e4f, -1e4f, -1e4f, 0.f), nb = make_float4(0.f, 0.f, 1.f, 0.f);
+    if (hl < tc) {
+      na = recA[tb + hl];
+      nb = recB[tb + hl];
+    }
+    for (int j0 = 0; j0 < tc; j0 += 16) {
+      const int m = min(16, tc - j0);
+      const float4 sa = na, sb = nb;
+      na = make_float4(-1e4f, -1e4f, -1e4f, 0.f);
+      nb = make_float4(0.f, 0.f, 1.f, 0.f);
+      if (j0 + 16 + hl < tc) {
+        na = recA[tb + j0 + 16 + hl];
+        nb = recB[tb + j0 + 16 + hl];
+      }
+      const int js = j0 + (hl < m ? hl : 0);
+      const float2 prev = hl < m && g0 > 0 ? scr[tk.w + js] : f2(0.f);
+      // slot m holds source m first and source m + 8 (mod 16, the lane m ^ 8) second
+      const float ox = __shfl_xor_sync(hm, sa.x, 8), oy = __shfl_xor_sync(hm, sa.y, 8);
+      const float oz = __shfl_xor_sync(hm, sa.z, 8), ow = __shfl_xor_sync(hm, sa.w, 8);
+      const float px = __shfl_xor_sync(hm, sb.x, 8), py = __shfl_xor_sync(hm, sb.y, 8);
+      const float pz = __shfl_xor_sync(hm, sb.z, 8), pw = __shfl_xor_sync(hm, sb.w, 8);
+      __syncwarp(hm);   // the previous tile's reads are done
+      Q[0][hl] = make_float4(-sa.x, -ox, -sa.y, -oy);
+      Q[1][hl] = make_float4(-sa.z, -oz, sa.w, ow);
+      Q[2][hl] = make_float4(sb.x, px, sb.y, py);
+      Q[3][hl] = make_float4(sb.z, pz, sb.w, pw);
+      __syncwarp(hm);
+      float2 own = f2(0.f);   // this lane's source j0+hl: (pot, dpdn) from the group's 16 targets
+#pragma unroll 4
+      for (int st = 0; st < 8; st++) {
+        const int slot = (hl + st) & 15;
+        float2 s0, s1;
+        near_sym_pair2<ADJ>(Q[0][slot], Q[1][slot], Q[2][slot], Q[3][slot], tx, ty, tz, tnx, tny, tnz, wat, wbt,
+                            watn, wbtn, kappa, kexp, eps, ieps, kap2, acc0, acc1, s0, s1);
+        // this lane's source was the first source of lane (hl - st) and the second of lane (hl - st - 8)
+        const int l1 = (hl - st) & 15, l2 = (hl - st - 8) & 15;
+        const float a0 = __shfl_sync(hm, s0.x, l1, 16), a1 = __shfl_sync(hm, s1.x, l1, 16);
+        const float b0 = __shfl_sync(hm, s0.y, l2, 16), b1 = __shfl_sync(hm, s1.y, l2, 16);
+        own = __fadd2_rn(own, __fadd2_rn(make_float2(a0, a1), make_float2(b0, b1)));
+      }
+      if (hl < m) scr[tk.w + js] = __fadd2_rn(prev, own);   // written by the first group, added to by the next
     }
     if (valid) scr[tk.z + t] = make_float2(acc0.x + acc0.y, acc1.x + acc1.y);
   }
@@ -1113,13 +1206,21 @@ static bool setup_near_sym(Context &c) {
   std::vector<int> symOff(nEnt, -1);
   std::vector<int4> tasks;
   std::vector<long long> cost;
+  std::vector<char> half;   // a pair with a small leaf: near_sym16_f2_kernel
   long long tot = 0, pairs = 0;
   for (int L = 0; L < pt.nLeaves; L++)
     for (int p = pt.nearOff[L]; p < pt.nearOff[L + 1]; p++) {
       const int S = pt.nearSrc[p];
       if (S <= L) continue;
       const int cl = pt.leafCount[L], cs = pt.leafCount[S];
-      if (std::min(cl, cs) < FB_NEAR_SYM_MIN_LEAF) continue;
+      const int mn = std::min(cl, cs);
+      if (mn < (c.mixed ? FB_NEAR_SYM16_MIN_LEAF : FB_NEAR_SYM_MIN_LEAF)) continue;
+      // mixed contexts: the half-warp kernel where its padding to 16-panel groups and tiles saves
+      // more than its larger per-tile overhead (FB_NEAR_SYM16_COST percent of the 32-wide cost
+      // per padded pair), which always holds below FB_NEAR_SYM_MIN_LEAF
+      const long long p32 = (long long)((cl + 31) / 32) * ((cs + 31) / 32) * 1024;
+      const long long p16 = (long long)((cl + 15) / 16) * ((cs + 15) / 16) * 256;
+      const bool small = c.mixed && (mn < FB_NEAR_SYM_MIN_LEAF || p16 * FB_NEAR_SYM16_COST < p32 * 100);
       int q = -1;   // the mirror entry (S <- L)
       for (int k = pt.nearOff[S]; k < pt.nearOff[S + 1]; k++)
         if (pt.nearSrc[k] == L) { q = k; break; }
@@ -1133,14 +1234,22 @@ static bool setup_near_sym(Context &c) {
       tot += pt.leafCount[T];
       tasks.push_back(make_int4(R, T, symOff[pR], symOff[pT]));
       cost.push_back((long long)cl * cs);
+      half.push_back(small);
       pairs += (long long)cl * cs;
     }
   if (tasks.empty()) return true;
+  // the 32-wide tasks first, then the half-warp ones, each by decreasing cost
   std::vector<int> ord(tasks.size());
   for (size_t i = 0; i < ord.size(); i++) ord[i] = (int)i;
-  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+  std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) {
+    return half[a] != half[b] ? half[b] != 0 : cost[a] > cost[b];
+  });
   std::vector<int4> sorted(tasks.size());
-  for (size_t i = 0; i < ord.size(); i++) sorted[i] = tasks[ord[i]];
+  int n32 = 0;
+  for (size_t i = 0; i < ord.size(); i++) {
+    sorted[i] = tasks[ord[i]];
+    n32 += half[ord[i]] ? 0 : 1;
+  }
   cudaStream_t s = c.stream;
   const size_t esz = c.mixed ? sizeof(float) : sizeof(double);   // scratch element; records are 4 of them
   if (!c.arena.upload(&c.d_symTask, sorted, s) || !c.arena.upload(&c.d_symOff, symOff, s) ||
@@ -1148,6 +1257,7 @@ static bool setup_near_sym(Context &c) {
       !c.arena.alloc(&c.d_symB, 4 * esz * (size_t)c.n))
     return false;
   c.nSymTasks = (int)sorted.size();
+  c.nSym32 = n32;
   c.symPanelPairs = pairs;
   return true;
 }
@@ -1187,11 +1297,21 @@ static void launch_near_t(Context &c, const void *tgtP, const void *tgtN, void *
     if (sym) {   // unordered leaf pairs of the symmetric kernel first, into the scratch
       near_pack_kernel<float><<<ceil_div(n, 256), 256, 0, s>>>(n, (const float4 *)tgtP, (const float4 *)tgtN,
                                                                c.d_area, sgm, (float4 *)c.d_symA, (float4 *)c.d_symB, 0);
-      near_sym_f2_kernel<ADJ><<<ceil_div(c.nSymTasks, kSymWarps), kSymWarps * 32, 0, s>>>(
-          c.nSymTasks, c.d_symTask, c.d_leafStart, c.d_leafCount, c.d_leafCtr, (const float4 *)c.d_symA,
-          (const float4 *)c.d_symB, (float)kap, (float)kexp, (float)eps, (float)(1.0 / eps), (float)(kap * kap),
-          (float2 *)c.d_symScr);
-      c.launches += 2;
+      if (c.nSym32 > 0) {
+        near_sym_f2_kernel<ADJ><<<ceil_div(c.nSym32, kSymWarps), kSymWarps * 32, 0, s>>>(
+            c.nSym32, c.d_symTask, c.d_leafStart, c.d_leafCount, c.d_leafCtr, (const float4 *)c.d_symA,
+            (const float4 *)c.d_symB, (float)kap, (float)kexp, (float)eps, (float)(1.0 / eps), (float)(kap * kap),
+            (float2 *)c.d_symScr);
+        c.launches += 1;
+      }
+      if (c.nSymTasks > c.nSym32) {
+        near_sym16_f2_kernel<ADJ><<<ceil_div(c.nSymTasks - c.nSym32, 2 * kSymWarps), kSymWarps * 32, 0, s>>>(
+            c.nSymTasks - c.nSym32, c.d_symTask + c.nSym32, c.d_leafStart, c.d_leafCount, c.d_leafCtr,
+            (const float4 *)c.d_symA, (const float4 *)c.d_symB, (float)kap, (float)kexp, (float)eps,
+            (float)(1.0 / eps), (float)(kap * kap), (float2 *)c.d_symScr);
+        c.launches += 1;
+      }
+      c.launches += 1;
     }
     near_apply_f2_kernel<ADJ><<<grid, kNearWarps * 32, 0, s>>>(
         c.nWork, c.d_work, c.d_leafStart, c.d_leafCount, c.d_nearOff, c.d_nearSrc, c.d_leafCtr,
