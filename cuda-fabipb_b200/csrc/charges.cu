@@ -393,61 +393,6 @@ struct WalkTree {
   int height, depth, NM;
 };
 
-// the multi-index at graded position i (the inverse of fmm.cu's gidx)
-struct Tri { int a, b, c; };
-__host__ __device__ constexpr Tri gmi(int i) {
-  for (int n = 0; n < 64; n++)
-    for (int a = 0; a <= n; a++)
-      for (int b = 0; b <= n - a; b++)
-        if (i-- == 0) return Tri{a, b, n - a - b};
-  return Tri{0, 0, 0};
-}
-
-// One step of the level recursion of derivs_inplace: kind 0 sets entry 0 to
-// the radial term G[p]; kind 1 sets d[e] = d[a] x[axis] + fb d[b] (b < 0: no
-// second term).
-struct DerivOp { int kind, e, a, b, axis, fb, p; };
-__host__ __device__ constexpr int deriv_ops(int order) {
-  int s = 1;
-  for (int p = order - 1; p >= 0; p--) s += nmom_c(order - p);
-  return s;
-}
-__host__ __device__ constexpr DerivOp deriv_op(int order, int s) {
-  if (s == 0) return DerivOp{0, 0, 0, -1, 0, 0, order};
-  s--;
-  for (int p = order - 1; p >= 0; p--) {
-    for (int e = nmom_c(order - p) - 1; e >= 1; e--, s--) {
-      if (s != 0) continue;
-      const Tri m = gmi(e);
-      if (m.a >= 1)
-        return DerivOp{1, e, gidx(m.a - 1, m.b, m.c), m.a >= 2 ? gidx(m.a - 2, m.b, m.c) : -1, 0, m.a - 1, 0};
-      if (m.b >= 1)
-        return DerivOp{1, e, gidx(0, m.b - 1, m.c), m.b >= 2 ? gidx(0, m.b - 2, m.c) : -1, 1, m.b - 1, 0};
-      return DerivOp{1, e, gidx(0, 0, m.c - 1), m.c >= 2 ? gidx(0, 0, m.c - 2) : -1, 2, m.c - 1, 0};
-    }
-    if (s == 0) return DerivOp{0, 0, 0, -1, 0, 0, p};
-    s--;
-  }
-  return DerivOp{0, 0, 0, -1, 0, 0, 0};
-}
-
-template <int ORDER, int S, typename T>
-__device__ __forceinline__ void deriv_step(T *d, const T *x, const T *G) {
-  constexpr DerivOp op = deriv_op(ORDER, S);
-  if constexpr (op.kind == 0) d[0] = G[op.p];
-  else if constexpr (op.b < 0) d[op.e] = d[op.a] * x[op.axis];
-  else d[op.e] = d[op.a] * x[op.axis] + d[op.b] * (T)op.fb;
-}
-template <int ORDER, typename T, int... S>
-__device__ __forceinline__ void deriv_steps(T *d, const T *x, const T *G, std::integer_sequence<int, S...>) {
-  (deriv_step<ORDER, S>(d, x, G), ...);
-}
-// D^e G for |e| <= ORDER from the radial sequence G[0..ORDER], into registers
-template <int ORDER, typename T>
-__device__ __forceinline__ void deriv_table(T *d, const T *x, const T *G) {
-  deriv_steps<ORDER>(d, x, G, std::make_integer_sequence<int, deriv_ops(ORDER)>{});
-}
-
 // y0 += sum_I sm_I d_I;  g_k += sum_I sm_I d_{I + e_k}
 template <bool Y0, bool Y1, int I, typename T>
 __device__ __forceinline__ void contract_step(const T *__restrict__ sm, const T *d, T &y0, T &g0, T &g1, T &g2) {

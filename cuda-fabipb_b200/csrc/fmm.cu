@@ -480,6 +480,76 @@ __host__ __device__ constexpr int gidx(int a, int b, int c) {
   return ((a + b + c) * (a + b + c + 1) * (a + b + c + 2)) / 6 + a * (a + b + c + 1) - (a * (a - 1)) / 2 + b;
 }
 
+// the multi-index at graded position i (the inverse of gidx)
+struct Tri { int a, b, c; };
+__host__ __device__ constexpr Tri gmi(int i) {
+  for (int n = 0; n < 64; n++)
+    for (int a = 0; a <= n; a++)
+      for (int b = 0; b <= n - a; b++)
+        if (i-- == 0) return Tri{a, b, n - a - b};
+  return Tri{0, 0, 0};
+}
+
+// One step of the level recursion of derivs_inplace: kind 0 sets entry 0 to
+// the radial term G[p]; kind 1 sets d[e] = d[a] x[axis] + fb d[b] (b < 0: no
+// second term).
+struct DerivOp { int kind, e, a, b, axis, fb, p; };
+__host__ __device__ constexpr int deriv_ops(int order) {
+  int s = 1;
+  for (int p = order - 1; p >= 0; p--) s += nmom_c(order - p);
+  return s;
+}
+__host__ __device__ constexpr DerivOp deriv_op(int order, int s) {
+  if (s == 0) return DerivOp{0, 0, 0, -1, 0, 0, order};
+  s--;
+  for (int p = order - 1; p >= 0; p--) {
+    for (int e = nmom_c(order - p) - 1; e >= 1; e--, s--) {
+      if (s != 0) continue;
+      const Tri m = gmi(e);
+      if (m.a >= 1)
+        return DerivOp{1, e, gidx(m.a - 1, m.b, m.c), m.a >= 2 ? gidx(m.a - 2, m.b, m.c) : -1, 0, m.a - 1, 0};
+      if (m.b >= 1)
+        return DerivOp{1, e, gidx(0, m.b - 1, m.c), m.b >= 2 ? gidx(0, m.b - 2, m.c) : -1, 1, m.b - 1, 0};
+      return DerivOp{1, e, gidx(0, 0, m.c - 1), m.c >= 2 ? gidx(0, 0, m.c - 2) : -1, 2, m.c - 1, 0};
+    }
+    if (s == 0) return DerivOp{0, 0, 0, -1, 0, 0, p};
+    s--;
+  }
+  return DerivOp{0, 0, 0, -1, 0, 0, 0};
+}
+
+template <int ORDER, int S, typename T>
+__device__ __forceinline__ void deriv_step(T *d, const T *x, const T *G) {
+  constexpr DerivOp op = deriv_op(ORDER, S);
+  if constexpr (op.kind == 0) d[0] = G[op.p];
+  else if constexpr (op.b < 0) d[op.e] = d[op.a] * x[op.axis];
+  else d[op.e] = d[op.a] * x[op.axis] + d[op.b] * (T)op.fb;
+}
+template <int ORDER, typename T, int... S>
+__device__ __forceinline__ void deriv_steps(T *d, const T *x, const T *G, std::integer_sequence<int, S...>) {
+  (deriv_step<ORDER, S>(d, x, G), ...);
+}
+// D^e G for |e| <= ORDER from the radial sequence G[0..ORDER], into registers
+template <int ORDER, typename T>
+__device__ __forceinline__ void deriv_table(T *d, const T *x, const T *G) {
+  deriv_steps<ORDER>(d, x, G, std::make_integer_sequence<int, deriv_ops(ORDER)>{});
+}
+
+// The same recursion on packed (D^e G0, D^e Gk) pairs in FP32 (the M2L
+// tensors of a mixed context, generated in the kernel from the pair offset)
+template <int ORDER, int S>
+__device__ __forceinline__ void deriv_step2(float2 *d, const float2 *x, const float2 *G) {
+  constexpr DerivOp op = deriv_op(ORDER, S);
+  if constexpr (op.kind == 0) d[0] = G[op.p];
+  else if constexpr (op.b < 0) d[op.e] = __fmul2_rn(d[op.a], x[op.axis]);
+  else d[op.e] = __ffma2_rn(d[op.b], f2((float)op.fb), __fmul2_rn(d[op.a], x[op.axis]));
+}
+template <int ORDER, int... S>
+__device__ __forceinline__ void deriv_steps2(float2 *d, const float2 *x, const float2 *G,
+                                             std::integer_sequence<int, S...>) {
+  (deriv_step2<ORDER, S>(d, x, G), ...);
+}
+
 // M2L conv for orders up to 4 as straight-line code: every (alpha, beta)
 // entry of the convolution is a compile-time step, so each lane holds its
 // pair's derivative tensors in registers (loaded once per batch, all loads in
@@ -560,11 +630,18 @@ struct Vec2<float> {
 #ifndef FB_M2L_TREG_F32
 #define FB_M2L_TREG_F32 1
 #endif
+// FP32 M2L tensors generated in the kernel from the cube offsets (1) or read from
+// the FP32 copy of the set-up tensors (0)
+#ifndef FB_M2L_GEN_F32
+#define FB_M2L_GEN_F32 1
+#endif
 template <int PM, typename TV = double>
 struct M2LUnrolledShape {
   typedef typename Vec2<TV>::t V2;
   static constexpr int NMP = nmom_c(PM);
   static constexpr bool TSMEM = PM >= 5 && !(FB_M2L_TREG_F32 && sizeof(TV) == 4);
+  // FP32 tensors in registers are generated in the kernel (no tensor stream)
+  static constexpr bool GEN = sizeof(TV) == 4 && !TSMEM && FB_M2L_GEN_F32;
   static constexpr int W = TSMEM ? (sizeof(TV) == 8 ? 1 : 2) : 4;   // warps per block
   static constexpr size_t colBytes = (size_t)NMP * 32 * sizeof(V2);   // moment columns (and tensor columns)
   static constexpr size_t warpBytes = (TSMEM ? 2 : 1) * colBytes + 4 * NMP * sizeof(double);   // + [4][NMP] sums
@@ -634,9 +711,9 @@ __global__ void __launch_bounds__(M2LUnrolledShape<PM, TV>::W * 32,
 m2l_unrolled_kernel(int nDst, const int *__restrict__ dstList, const int *__restrict__ m2lOff,
                     const int *__restrict__ m2lSrc, const int *__restrict__ pairIdx,
                     const int *__restrict__ ordOfCube, long long nPairs,
-                    const typename Vec2<TV>::t *__restrict__ tens, int NM, double eps,
-                    const double *__restrict__ momPot, const double *__restrict__ momDpdn, double *lec1,
-                    double *lec2, double *lec3, double *lec4) {
+                    const typename Vec2<TV>::t *__restrict__ tens, const double *__restrict__ ctr, float kappa,
+                    int NM, double eps, const double *__restrict__ momPot, const double *__restrict__ momDpdn,
+                    double *lec1, double *lec2, double *lec3, double *lec4) {
   typedef M2LUnrolledShape<PM, TV> Sh;
   typedef typename Vec2<TV>::t V2;
   constexpr int NMP = Sh::NMP;
@@ -683,12 +760,36 @@ m2l_unrolled_kernel(int nDst, const int *__restrict__ dstList, const int *__rest
     }
 #endif
     M2LTensors<PM, TV, Sh::TSMEM> T;
-    const V2 *tp = tens + (ADJ ? pairIdx[live ? k : o0] : (live ? k : o0));
-    if constexpr (Sh::TSMEM) {
+    if constexpr (Sh::GEN) {
+      // the lane's pair tensor from its offset r = x_dst - x_src (the forward pair's cubes), by the
+      // radial sequences of derivs_inplace and the unrolled level recursion, in FP32 registers
+      const int dc = ADJ ? mySrc : f, sc = ADJ ? f : mySrc;
+      float x[3] = {1.f, 0.f, 0.f};   // a lane past the batch: any offset (its moments are zero)
+      if (live)
+        for (int q = 0; q < 3; q++) x[q] = (float)(ctr[3 * dc + q] - ctr[3 * sc + q]);
+      const float r = sqrtf(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+      const float rexp = expf(-kappa * r), r1 = 1.f / r, rr2 = r1 * r1, k2 = kappa * kappa;
+      float2 G[PM + 1];
+      G[0].x = r1 * (float)kFourPiI;
+      G[0].y = rexp * G[0].x;
+      if constexpr (PM >= 1) {
+        G[1].x = -rr2 * G[0].x;
+        G[1].y = -G[0].y * (rr2 + kappa * r1);
+      }
+#pragma unroll
+      for (int q = 1; q < PM; q++) {
+        G[q + 1].x = (float)(2 * q + 1) * -rr2 * G[q].x;
+        G[q + 1].y = rr2 * (k2 * G[q - 1].y - (float)(2 * q + 1) * G[q].y);
+      }
+      const float2 x2[3] = {f2(x[0]), f2(x[1]), f2(x[2])};
+      deriv_steps2<PM>(T.v, x2, G, std::make_integer_sequence<int, deriv_ops(PM)>{});
+    } else if constexpr (Sh::TSMEM) {
+      const V2 *tp = tens + (ADJ ? pairIdx[live ? k : o0] : (live ? k : o0));
       V2 *sT = reinterpret_cast<V2 *>(wbase + Sh::colBytes + 4 * NMP * sizeof(double));
       for (int e = 0; e < NMP; e++) sT[e * 32 + lane] = tp[(size_t)e * nPairs];
       T.col = sT;
     } else {
+      const V2 *tp = tens + (ADJ ? pairIdx[live ? k : o0] : (live ? k : o0));
 #pragma unroll
       for (int e = 0; e < NMP; e++) T.v[e] = tp[(size_t)e * nPairs];
     }
@@ -842,8 +943,8 @@ static void launch_m2l_unrolled(Context &c, int nDst, const int *dst, const int 
   }
   const unsigned grid = ceil_div((long long)nDst, Sh::W);
   m2l_unrolled_kernel<PU, ADJ, TV><<<grid, Sh::W * 32, Sh::bytes, c.stream>>>(
-      nDst, dst, off, src, pairIdx, c.d_ordM2L, c.nM2LPairs, (const typename Vec2<TV>::t *)tens, c.NM, c.epsilon,
-      inPot, inDpdn, o1, o2, o3, o4);
+      nDst, dst, off, src, pairIdx, c.d_ordM2L, c.nM2LPairs, (const typename Vec2<TV>::t *)tens, c.d_cubeCtr,
+      (float)c.prm.kappa, c.NM, c.epsilon, inPot, inDpdn, o1, o2, o3, o4);
 }
 
 // Forward: moments (d_mom) -> local expansions (4 planes of d_lec).
@@ -861,7 +962,7 @@ static void launch_m2l_t(Context &c, bool adj, bool fp32) {
   double *o3 = c.d_lec + 2 * plane, *o4 = c.d_lec + 3 * plane;
   if (PM <= 5) {
     constexpr int PU = PM <= 5 ? PM : 5;
-    if (fp32 && c.d_m2lTensF) {
+    if (fp32 && (M2LUnrolledShape<PU, float>::GEN || c.d_m2lTensF)) {
       if (adj) launch_m2l_unrolled<PU, true, float>(c, nDst, dst, off, src, pairIdx, c.d_m2lTensF, inPot, inDpdn, o1, o2, o3, o4);
       else launch_m2l_unrolled<PU, false, float>(c, nDst, dst, off, src, pairIdx, c.d_m2lTensF, inPot, inDpdn, o1, o2, o3, o4);
     } else {
@@ -983,7 +1084,8 @@ bool setup_fmm(Context &c) {
     if (!c.arena.alloc_n(&c.d_m2lTens, (size_t)c.NM * c.nM2LPairs)) return false;
     FB_DISPATCH_ORDER(c.P, launch_m2l_tensors, c, d_pairDst);
     FB_CUDA(cudaGetLastError());
-    if (c.mixed && c.P <= 5) {   // the FP32 copy the mixed conv reads
+    const bool genF32 = c.P == 5 ? M2LUnrolledShape<5, float>::GEN : M2LUnrolledShape<4, float>::GEN;
+    if (c.mixed && c.P <= 5 && !genF32) {   // the FP32 copy the mixed conv reads
       if (!c.arena.alloc_n(&c.d_m2lTensF, (size_t)c.NM * c.nM2LPairs)) return false;
       tensors_to_float_kernel<<<1184, 256, 0, s>>>((long long)c.NM * c.nM2LPairs, c.d_m2lTens, c.d_m2lTensF);
       FB_CUDA(cudaGetLastError());
