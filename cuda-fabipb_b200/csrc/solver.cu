@@ -68,41 +68,76 @@ void free_precond(Context &c) {
 
 // ---------------------------------------------------------------------------
 // block assembly: A(j, i) = -K1(X=j,Y=i) etc. in column-major M x M
-// ---------------------------------------------------------------------------
+// (src/precond_fmm.c:147-263: panelIA0 over the cube's panel pairs).
+// From the near field's own coefficients: every pair's one-point
+// term A_X A_Y KER4(p_X - p_Y) at the one-point nodes p = v0/2 + v1/4 + v2/4 (0
+// for X = Y), then, in pc_special_kernel, the exact-minus-one-point correction
+// of the special pairs (shared vertex, edge, self) from the near field's table,
+// so a block equals panelIA0's at -q=1 without its singularity tests per pair.
 template <typename TO>
-__global__ void pc_assemble_kernel(int nBlocks, const int *__restrict__ bStart, const int *__restrict__ bSize,
+__global__ void pc_onepoint_kernel(int nBlocks, const int *__restrict__ bStart, const int *__restrict__ bSize,
                                    const long long *__restrict__ bOff, const double *__restrict__ vtx,
-                                   const double *__restrict__ nrm, const double *__restrict__ area, int q,
-                                   double kappa, double eps, double s1, double s2, TO *A) {
+                                   const double *__restrict__ nrm, const double *__restrict__ area, double kappa,
+                                   double eps, double s1, double s2, TO *A) {
   for (int b = blockIdx.y; b < nBlocks; b += gridDim.y) {   // (the grid's y extent is capped at 65535)
-  const int hm = bSize[b], st = bStart[b], M = 2 * hm;
-  const long long pairs = (long long)hm * hm;
-  TO *Ab = A + bOff[b];
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < pairs;
-       p += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(p / hm), j = (int)(p % hm);  // i: pnlY (column), j: pnlX (row)
-    const int Xi = st + j, Yi = st + i;
-    PanelD X, Y;
-    const double *vx = vtx + 9 * (size_t)Xi, *vy = vtx + 9 * (size_t)Yi;
-    for (int k = 0; k < 3; k++)
-      for (int c = 0; c < 3; c++) { X.v[k][c] = vx[3 * k + c]; Y.v[k][c] = vy[3 * k + c]; }
-    for (int c = 0; c < 3; c++) {
-      X.a[0][c] = X.v[2][c] - X.v[1][c]; X.a[1][c] = X.v[0][c] - X.v[2][c]; X.a[2][c] = X.v[1][c] - X.v[0][c];
-      Y.a[0][c] = Y.v[2][c] - Y.v[1][c]; Y.a[1][c] = Y.v[0][c] - Y.v[2][c]; Y.a[2][c] = Y.v[1][c] - Y.v[0][c];
-      X.n[c] = nrm[3 * (size_t)Xi + c];
-      Y.n[c] = nrm[3 * (size_t)Yi + c];
+    const int hm = bSize[b], st = bStart[b], M = 2 * hm;
+    const long long pairs = (long long)hm * hm;
+    TO *Ab = A + bOff[b];
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < pairs;
+         p += (long long)gridDim.x * blockDim.x) {
+      const int i = (int)(p / hm), j = (int)(p % hm);  // i: pnlY (column), j: pnlX (row)
+      const int Xi = st + j, Yi = st + i;
+      double K[4] = {0.0, 0.0, 0.0, 0.0};
+      if (Xi != Yi) {
+        const double *vx = vtx + 9 * (size_t)Xi, *vy = vtx + 9 * (size_t)Yi;
+        double r[3], nX[3], nY[3];
+        for (int c = 0; c < 3; c++) {
+          const double mx = vx[c] + 0.5 * ((vx[3 + c] - vx[c]) + 0.5 * (vx[6 + c] - vx[3 + c]));
+          const double my = vy[c] + 0.5 * ((vy[3 + c] - vy[c]) + 0.5 * (vy[6 + c] - vy[3 + c]));
+          r[c] = mx - my;
+          nX[c] = nrm[3 * (size_t)Xi + c];
+          nY[c] = nrm[3 * (size_t)Yi + c];
+        }
+        if (r[0] != 0.0 || r[1] != 0.0 || r[2] != 0.0) {
+          double y[4];
+          ker4_d(kappa, eps, r, nX, nY, y);
+          const double w = area[Xi] * area[Yi];
+          for (int k = 0; k < 4; k++) K[k] = w * y[k];
+        }
+      }
+      const double d0 = (i == j) ? s1 * area[Yi] : 0.0;
+      const double d1 = (i == j) ? s2 * area[Yi] : 0.0;
+      Ab[(size_t)i * M + j] = (TO)(-K[1] + d0);
+      Ab[(size_t)i * M + j + hm] = (TO)(-K[0]);
+      Ab[(size_t)(i + hm) * M + j] = (TO)(-K[3]);
+      Ab[(size_t)(i + hm) * M + j + hm] = (TO)(-K[2] + d1);
     }
-    X.area = area[Xi];
-    Y.area = area[Yi];
-    double K[4];
-    panel_ia0_d(q, kappa, eps, X, Y, Xi == Yi, K, nullptr);
-    double d0 = (i == j) ? s1 * area[Yi] : 0.0;
-    double d1 = (i == j) ? s2 * area[Yi] : 0.0;
-    Ab[(size_t)i * M + j] = (TO)(-K[1] + d0);
-    Ab[(size_t)i * M + j + hm] = (TO)(-K[0]);
-    Ab[(size_t)(i + hm) * M + j] = (TO)(-K[3]);
-    Ab[(size_t)(i + hm) * M + j + hm] = (TO)(-K[2] + d1);
   }
+}
+
+// the special pairs (X, Y) of a block: add their correction (each entry has one writer)
+template <typename TO>
+__global__ void pc_special_kernel(int nBlocks, const int *__restrict__ bStart, const int *__restrict__ bSize,
+                                  const long long *__restrict__ bOff, const int *__restrict__ spOff,
+                                  const int *__restrict__ spSrc, const double4 *__restrict__ spK, TO *A) {
+  for (int b = blockIdx.y; b < nBlocks; b += gridDim.y) {
+    const int hm = bSize[b], st = bStart[b], M = 2 * hm;
+    TO *Ab = A + bOff[b];
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < hm; j += gridDim.x * blockDim.x) {
+      const int Xi = st + j;
+      for (int e = spOff[Xi]; e < spOff[Xi + 1]; e++) {
+        const int Yi = spSrc[e];
+        if (Yi < st || Yi >= st + hm) continue;
+        const int i = Yi - st;
+        const double4 d = spK[e];   // (K0, K1, K2, K3) exact minus one-point
+        TO *a0 = Ab + (size_t)i * M + j, *a1 = Ab + (size_t)i * M + j + hm;
+        TO *a2 = Ab + (size_t)(i + hm) * M + j, *a3 = Ab + (size_t)(i + hm) * M + j + hm;
+        *a0 = (TO)((double)*a0 - d.y);
+        *a1 = (TO)((double)*a1 - d.x);
+        *a2 = (TO)((double)*a2 - d.w);
+        *a3 = (TO)((double)*a3 - d.z);
+      }
+    }
   }
 }
 
@@ -827,18 +862,21 @@ bool precond_setup(Context &c, int mode) {
     FB_CHECK(p.maxM <= gj_max_rows<float>(), "preconditioner block of %d rows above the FP32 limit %d", p.maxM,
              gj_max_rows<float>());
     if (!p.arena.alloc_n(&p.d_invF, (size_t)off)) return false;
-    pc_assemble_kernel<float><<<grid, 128, 0, s>>>(p.nBlocks, p.d_start, p.d_size, p.d_off, c.d_vtx, c.d_nrm, c.d_area,
-                                                   c.prm.quad_order, c.prm.kappa, c.epsilon, s1, s2, p.d_invF);
-    c.launches += 1;
+    pc_onepoint_kernel<float><<<grid, 128, 0, s>>>(p.nBlocks, p.d_start, p.d_size, p.d_off, c.d_vtx, c.d_nrm,
+                                                   c.d_area, c.prm.kappa, c.epsilon, s1, s2, p.d_invF);
+    pc_special_kernel<float><<<dim3(4, grid.y), 128, 0, s>>>(p.nBlocks, p.d_start, p.d_size, p.d_off, c.d_spOff,
+                                                             c.d_spSrc, c.d_spK, p.d_invF);
+    c.launches += 2;
     FB_CUDA(cudaGetLastError());
     tm.mark("assemble");
     ok = factor_gauss_jordan<float>(c, p, p.d_invF);
   } else {
     if (!p.arena.alloc_n(&p.d_inv, (size_t)off)) return false;
-    pc_assemble_kernel<double><<<grid, 128, 0, s>>>(p.nBlocks, p.d_start, p.d_size, p.d_off, c.d_vtx, c.d_nrm,
-                                                    c.d_area, c.prm.quad_order, c.prm.kappa, c.epsilon, s1, s2,
-                                                    p.d_inv);
-    c.launches += 1;
+    pc_onepoint_kernel<double><<<grid, 128, 0, s>>>(p.nBlocks, p.d_start, p.d_size, p.d_off, c.d_vtx, c.d_nrm,
+                                                    c.d_area, c.prm.kappa, c.epsilon, s1, s2, p.d_inv);
+    pc_special_kernel<double><<<dim3(4, grid.y), 128, 0, s>>>(p.nBlocks, p.d_start, p.d_size, p.d_off, c.d_spOff,
+                                                              c.d_spSrc, c.d_spK, p.d_inv);
+    c.launches += 2;
     FB_CUDA(cudaGetLastError());
     tm.mark("assemble");
     ok = factor_gauss_jordan<double>(c, p, p.d_inv);
