@@ -550,11 +550,11 @@ __device__ __forceinline__ void deriv_steps2(float2 *d, const float2 *x, const f
   (deriv_step2<ORDER, S>(d, x, G), ...);
 }
 
-// M2L conv for orders up to 4 as straight-line code: every (alpha, beta)
+// M2L conv for orders up to 5 as straight-line code: every (alpha, beta)
 // entry of the convolution is a compile-time step, so each lane holds its
-// pair's derivative tensors in registers (loaded once per batch, all loads in
-// flight together), reads its source's moments from a padded shared-memory
-// column, and keeps the four raw sums S1 = sum c2 G0, S2 = sum c2 Gk,
+// pair's derivative tensors in registers (FP32: generated in the kernel from
+// the pair's cube offset; FP64: loaded once per batch, all loads in flight
+// together), reads its source's moments from a padded shared-memory column, and keeps the four raw sums S1 = sum c2 G0, S2 = sum c2 Gk,
 // S3 = sum c1 G0, S4 = sum c1 Gk per output coefficient, with the sign
 // (-1)^|beta| folded in.  The convM2L combinations (src/expan.c:258-290) are
 // formed once at the end: l1 = S1 - S2, l2 = eps S4 - S3, l3 = S1 - S2/eps,
