@@ -384,8 +384,6 @@ def pass_report(surf, info, x_ptr, flush, reps, prec_is_mixed, fp32, fp64):
             ach = amount / t / 1e9
             out[k] = {"ms": ms[k], "bound": "hbm", "achieved": ach, "unit": "GB/s", "peak": peak,
                       "frac": ach / peak, "algorithmic": amount, "peak_source": hbm_src}
-    m2l_bytes = 16.0 * nmom(p) * info["m2l_pairs"]   # the (D G0, D Gk) tensors read per launch
-    out["m2l"]["tensor_gbs"] = m2l_bytes / (ms["m2l"] / 1000.0) / 1e9
     return out
 
 

@@ -80,6 +80,8 @@ struct Context {
   long long nM2LPairs = 0;
   double2 *d_m2lTens = nullptr;                // [nMom][pairs] (D G0, D Gk) per M2L pair
   float2 *d_m2lTensF = nullptr;                // the same in FP32 (mixed contexts, orders <= 5)
+  float2 *d_momF2 = nullptr;                   // FP32 (pot, dpdn) rows of the M2L input, bulk-copy staging
+  int momF2Stride = 0;                         // float2 entries per row (a 16-byte multiple)
   // transposed M2L lists (adjoint operator)
   bool m2lAdjReady = false;
   std::vector<int> h_m2lDstT;

@@ -675,13 +675,39 @@ struct M2LSumsT {
   TV s1, s2, s3, s4;
 };
 
-template <int PM, int Q, bool FULL, bool ADJ, typename TV, typename TT>
-__device__ __forceinline__ void m2l_step(M2LSumsT<TV> &S, const typename Vec2<TV>::t *sC, const TT &T, int lane,
-                                         int order, double *sAcc) {
+// Moment readers of the conv.  M2LColMoments: the XOR-swizzled columns staged
+// by plain loads.  M2LRowMoments: the lane's source row of (pot, dpdn) float2
+// entries staged by bulk copies, read as float4 (entries IB, IB+1) at even IB;
+// within one alpha the conv takes beta in graded order from 0, and an odd entry
+// is used only if its even neighbour was (|beta| never falls), so the odd
+// entry takes the upper half of the last load.
+template <typename V2>
+struct M2LColMoments {
+  const V2 *sC;
+  int lane;
+  template <int IB>
+  __device__ __forceinline__ V2 get() { return sC[m2l_slot(IB, lane)]; }
+};
+struct M2LRowMoments {
+  const float2 *row;
+  float4 q;
+  template <int IB>
+  __device__ __forceinline__ float2 get() {
+    if constexpr ((IB & 1) == 0) {
+      q = *reinterpret_cast<const float4 *>(row + IB);
+      return make_float2(q.x, q.y);
+    } else {
+      return make_float2(q.z, q.w);
+    }
+  }
+};
+
+template <int PM, int Q, bool FULL, bool ADJ, typename TV, typename TT, typename TM>
+__device__ __forceinline__ void m2l_step(M2LSumsT<TV> &S, TM &M, const TT &T, int lane, int order, double *sAcc) {
   constexpr M2LEntry E = m2l_entry<PM>(Q);
   if (E.first) S.s1 = S.s2 = S.s3 = S.s4 = (TV)0;
   if (FULL || E.dsum <= order) {
-    const typename Vec2<TV>::t mo = sC[m2l_slot(E.ib, lane)];
+    const typename Vec2<TV>::t mo = M.template get<E.ib>();
     const typename Vec2<TV>::t d = T.get(E.ig, lane);
     if ((ADJ ? E.dal : E.dsum - E.dal) & 1) {   // (-1)^|input|, or (-1)^|output| transposed
       S.s1 -= mo.y * d.x; S.s2 -= mo.y * d.y; S.s3 -= mo.x * d.x; S.s4 -= mo.x * d.y;
@@ -695,11 +721,34 @@ __device__ __forceinline__ void m2l_step(M2LSumsT<TV> &S, const typename Vec2<TV
   }
 }
 
-template <int PM, bool FULL, bool ADJ, typename TV, typename TT, int... Q>
-__device__ __forceinline__ void m2l_steps(std::integer_sequence<int, Q...>, M2LSumsT<TV> &S,
-                                          const typename Vec2<TV>::t *sC, const TT &T, int lane, int order,
-                                          double *sAcc) {
-  (m2l_step<PM, Q, FULL, ADJ, TV, TT>(S, sC, T, lane, order, sAcc), ...);
+template <int PM, bool FULL, bool ADJ, typename TV, typename TT, typename TM, int... Q>
+__device__ __forceinline__ void m2l_steps(std::integer_sequence<int, Q...>, M2LSumsT<TV> &S, TM &M, const TT &T,
+                                          int lane, int order, double *sAcc) {
+  (m2l_step<PM, Q, FULL, ADJ, TV, TT, TM>(S, M, T, lane, order, sAcc), ...);
+}
+
+// The lane's FP32 M2L tensor (packed D^e G0, D^e Gk) from its pair's offset x =
+// x_dst - x_src: the radial sequences of derivs_inplace, then the unrolled
+// level recursion, in registers.  A lane without a pair (live false) gets the
+// zero tensor.
+template <int PM>
+__device__ __forceinline__ void m2l_gen_tensor(const float x[3], bool live, float kappa, float2 *Tv) {
+  const float r = sqrtf(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+  const float rexp = expf(-kappa * r), r1 = 1.f / r, rr2 = r1 * r1, k2 = kappa * kappa;
+  float2 G[PM + 1];
+  G[0].x = live ? r1 * (float)kFourPiI : 0.f;
+  G[0].y = rexp * G[0].x;
+  if constexpr (PM >= 1) {
+    G[1].x = -rr2 * G[0].x;
+    G[1].y = -G[0].y * (rr2 + kappa * r1);
+  }
+#pragma unroll
+  for (int q = 1; q < PM; q++) {
+    G[q + 1].x = (float)(2 * q + 1) * -rr2 * G[q].x;
+    G[q + 1].y = rr2 * (k2 * G[q - 1].y - (float)(2 * q + 1) * G[q].y);
+  }
+  const float2 x2[3] = {f2(x[0]), f2(x[1]), f2(x[2])};
+  deriv_steps2<PM>(Tv, x2, G, std::make_integer_sequence<int, deriv_ops(PM)>{});
 }
 
 // ADJ: the transposed interaction, as for m2l_kernel.  TV = float: tensors
@@ -764,25 +813,10 @@ m2l_unrolled_kernel(int nDst, const int *__restrict__ dstList, const int *__rest
       // the lane's pair tensor from its offset r = x_dst - x_src (the forward pair's cubes), by the
       // radial sequences of derivs_inplace and the unrolled level recursion, in FP32 registers
       const int dc = ADJ ? mySrc : f, sc = ADJ ? f : mySrc;
-      float x[3] = {1.f, 0.f, 0.f};   // a lane past the batch: any offset (its moments are zero)
+      float x[3] = {1.f, 0.f, 0.f};   // a lane past the batch: any offset (its tensor is zero)
       if (live)
         for (int q = 0; q < 3; q++) x[q] = (float)(ctr[3 * dc + q] - ctr[3 * sc + q]);
-      const float r = sqrtf(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
-      const float rexp = expf(-kappa * r), r1 = 1.f / r, rr2 = r1 * r1, k2 = kappa * kappa;
-      float2 G[PM + 1];
-      G[0].x = r1 * (float)kFourPiI;
-      G[0].y = rexp * G[0].x;
-      if constexpr (PM >= 1) {
-        G[1].x = -rr2 * G[0].x;
-        G[1].y = -G[0].y * (rr2 + kappa * r1);
-      }
-#pragma unroll
-      for (int q = 1; q < PM; q++) {
-        G[q + 1].x = (float)(2 * q + 1) * -rr2 * G[q].x;
-        G[q + 1].y = rr2 * (k2 * G[q - 1].y - (float)(2 * q + 1) * G[q].y);
-      }
-      const float2 x2[3] = {f2(x[0]), f2(x[1]), f2(x[2])};
-      deriv_steps2<PM>(T.v, x2, G, std::make_integer_sequence<int, deriv_ops(PM)>{});
+      m2l_gen_tensor<PM>(x, live, kappa, T.v);
     } else if constexpr (Sh::TSMEM) {
       const V2 *tp = tens + (ADJ ? pairIdx[live ? k : o0] : (live ? k : o0));
       V2 *sT = reinterpret_cast<V2 *>(wbase + Sh::colBytes + 4 * NMP * sizeof(double));
@@ -795,15 +829,208 @@ m2l_unrolled_kernel(int nDst, const int *__restrict__ dstList, const int *__rest
     }
     __syncwarp();
     M2LSumsT<TV> S{(TV)0, (TV)0, (TV)0, (TV)0};
+    M2LColMoments<V2> M{sC, lane};
     if (order == PM)
-      m2l_steps<PM, true, ADJ, TV>(std::make_integer_sequence<int, m2l_entries<PM>()>{}, S, sC, T, lane, order,
+      m2l_steps<PM, true, ADJ, TV>(std::make_integer_sequence<int, m2l_entries<PM>()>{}, S, M, T, lane, order,
                                    sAcc);
     else
-      m2l_steps<PM, false, ADJ, TV>(std::make_integer_sequence<int, m2l_entries<PM>()>{}, S, sC, T, lane, order,
+      m2l_steps<PM, false, ADJ, TV>(std::make_integer_sequence<int, m2l_entries<PM>()>{}, S, M, T, lane, order,
                                     sAcc);
   }
   __syncwarp();
   const int nm = ((order + 1) * (order + 2) * (order + 3)) / 6;
+  const double ieps = 1.0 / eps;
+  for (int e = lane; e < nm; e += 32) {
+    const double S1 = sAcc[e], S2 = sAcc[NMP + e], S3 = sAcc[2 * NMP + e], S4 = sAcc[3 * NMP + e];
+    const size_t o = (size_t)f * NM + e;
+    if (ADJ) {   // sign already folded in
+      lec1[o] += eps * S2 - S1 - S3 + S4;
+      lec2[o] += S1 + S3 - S2 - S4 * ieps;
+    } else {
+      lec1[o] += S1 - S2;
+      lec2[o] += eps * S4 - S3;
+      lec3[o] += S1 - S2 * ieps;
+      lec4[o] += S4 - S3;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// M2L of mixed contexts with the moments staged by the bulk-copy (TMA) engine.
+// The conv is that of m2l_unrolled_kernel<PM, ADJ, float> (generated FP32
+// tensors, the same (alpha, beta) walk and sums); the staging differs:
+//  * m2l_pack_kernel writes the input moments as one FP32 (pot, dpdn) row per
+//    cube, NMS float2 entries (NMP rounded up to a 16-byte multiple);
+//  * one warp per destination cube and per block; each lane's source row is
+//    fetched with one cp.async.bulk (global -> shared, no multicast) into a
+//    row of the warp's buffer, completion counted on an mbarrier;
+//  * two buffers: the copies of batch b+1 are in flight while batch b's
+//    tensors are generated and its conv runs, so the warp waits on no moment
+//    load; the next batch's source indices and cube centres are loaded one
+//    batch ahead as well;
+//  * shared rows of RS float2 (an odd number of 16-byte units), read as float4:
+//    the 8 lanes of each quarter-warp hit distinct 16-byte bank groups.
+// Every wait is bounded; a warp that gives up counts the stall in
+// g_m2lStalls, waits (bounded) for its other copy in flight and writes NaN to
+// its cube's local expansions, so the failure shows in the result.
+// ---------------------------------------------------------------------------
+__device__ unsigned int g_m2lStalls = 0;
+
+template <int PM>
+struct M2LBulkShape {
+  static constexpr int NMP = nmom_c(PM);
+  static constexpr int NMS = (NMP + 1) & ~1;                      // packed row: 16-byte multiple
+  static constexpr int RS = ((NMS / 2) & 1) ? NMS : NMS + 2;      // shared row stride, odd in 16-byte units
+  static constexpr size_t bufBytes = (size_t)32 * RS * sizeof(float2);
+  static constexpr size_t accOff = 2 * bufBytes;
+  static constexpr size_t barOff = accOff + 4 * NMP * sizeof(double);
+  static constexpr size_t bytes = barOff + 2 * sizeof(unsigned long long);
+  // resident warps per SM allowed by shared memory (1 KB reserved per block)
+  static constexpr int FIT = (int)((228 * 1024) / (bytes + 1024));
+  static constexpr int MINB = FIT < 1 ? 1 : (FIT > 32 ? 32 : FIT);
+};
+
+__global__ void m2l_pack_kernel(long long total, int NM, int NMS, const double *__restrict__ pot,
+                                const double *__restrict__ dpdn, float2 *out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const long long f = i / NMS;
+  const int e = (int)(i - f * NMS);
+  out[i] = e < NM ? make_float2((float)pot[f * NM + e], (float)dpdn[f * NM + e]) : make_float2(0.f, 0.f);
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+// bounded wait for the phase of the given parity; false if it never completed
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity) {
+  const unsigned a = smem_u32(bar);
+  for (int i = 0; i < (1 << 22); i++) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+// one bulk copy global -> this CTA's shared memory, counted on bar
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// the copies of the batch starting at b (nb sources, lane j's source sj) into buf
+template <int PM>
+__device__ __forceinline__ void m2l_bulk_issue(int nb, int sj, int lane, const float2 *__restrict__ momF, float2 *buf,
+                                               unsigned long long *bar) {
+  typedef M2LBulkShape<PM> Sh;
+  __syncwarp();
+  // the generic-proxy reads of this buffer (the conv two batches back) are
+  // ordered before the async-proxy writes that follow
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (lane == 0) mbar_expect_tx(bar, (unsigned)(nb * Sh::NMS * sizeof(float2)));
+  __syncwarp();
+  if (lane < nb) bulk_g2s(buf + lane * Sh::RS, momF + (size_t)sj * Sh::NMS, Sh::NMS * sizeof(float2), bar);
+}
+
+template <int PM, bool ADJ>
+__global__ void __launch_bounds__(32, M2LBulkShape<PM>::MINB)
+m2l_bulk_kernel(const int *__restrict__ dstList, const int *__restrict__ m2lOff, const int *__restrict__ m2lSrc,
+                const int *__restrict__ ordOfCube, const double *__restrict__ ctr, float kappa, int NM, double eps,
+                const float2 *__restrict__ momF, double *lec1, double *lec2, double *lec3, double *lec4) {
+  typedef M2LBulkShape<PM> Sh;
+  constexpr int NMP = Sh::NMP;
+  extern __shared__ __align__(16) unsigned char m2lbSmem[];
+  float2 *buf = reinterpret_cast<float2 *>(m2lbSmem);   // [2][32][RS]
+  double *sAcc = reinterpret_cast<double *>(m2lbSmem + Sh::accOff);   // [4][NMP]
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(m2lbSmem + Sh::barOff);
+  const int lane = threadIdx.x;
+  const int f = dstList[blockIdx.x];
+  const int order = ordOfCube[f];
+  const int o0 = m2lOff[f], o1 = m2lOff[f + 1];
+  for (int e = lane; e < 4 * NMP; e += 32) sAcc[e] = 0.0;
+  if (lane == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  const double cf0 = ctr[3 * f], cf1 = ctr[3 * f + 1], cf2 = ctr[3 * f + 2];
+  // batch 0 in flight; batch 1's sources and batch 0's centres loaded
+  int srcCur = o0 + lane < o1 ? m2lSrc[o0 + lane] : 0;
+  m2l_bulk_issue<PM>(min(32, o1 - o0), srcCur, lane, momF, buf, &bar[0]);
+  int srcNext = o0 + 32 + lane < o1 ? m2lSrc[o0 + 32 + lane] : 0;
+  double cs0 = ctr[3 * srcCur], cs1 = ctr[3 * srcCur + 1], cs2 = ctr[3 * srcCur + 2];
+  unsigned phase = 0;   // bit s: the parity to wait for on bar[s]
+  bool bad = false;
+  int it = 0;
+  for (int b0 = o0; b0 < o1; b0 += 32, it++) {
+    const int s = it & 1;
+    const bool live = b0 + lane < o1;
+    const bool more = b0 + 32 < o1;
+    if (more) m2l_bulk_issue<PM>(min(32, o1 - b0 - 32), srcNext, lane, momF, buf + (s ^ 1) * 32 * Sh::RS, &bar[s ^ 1]);
+    const int srcNext2 = b0 + 64 + lane < o1 ? m2lSrc[b0 + 64 + lane] : 0;
+    const double cn0 = ctr[3 * srcNext], cn1 = ctr[3 * srcNext + 1], cn2 = ctr[3 * srcNext + 2];
+    // the lane's tensor from the pair's offset (forward: x_dst - x_src; transposed: the
+    // forward pair's cubes, x_src - x_dst here)
+    M2LTensors<PM, float, false> T;
+    {
+      float x[3] = {1.f, 0.f, 0.f};
+      if (live) {
+        if (ADJ) {
+          x[0] = (float)(cs0 - cf0); x[1] = (float)(cs1 - cf1); x[2] = (float)(cs2 - cf2);
+        } else {
+          x[0] = (float)(cf0 - cs0); x[1] = (float)(cf1 - cs1); x[2] = (float)(cf2 - cs2);
+        }
+      }
+      m2l_gen_tensor<PM>(x, live, kappa, T.v);
+    }
+    const bool ok = mbar_wait(&bar[s], (phase >> s) & 1);
+    phase ^= 1u << s;
+    if (!__all_sync(0xffffffffu, ok)) {
+      bad = true;
+      if (more) mbar_wait(&bar[s ^ 1], (phase >> (s ^ 1)) & 1);
+      break;
+    }
+    // a lane past the batch reads row 0 (finite moments) with its zero tensor
+    M2LRowMoments M{buf + s * 32 * Sh::RS + (live ? lane : 0) * Sh::RS, make_float4(0.f, 0.f, 0.f, 0.f)};
+    M2LSumsT<float> S{0.f, 0.f, 0.f, 0.f};
+    if (order == PM)
+      m2l_steps<PM, true, ADJ, float>(std::make_integer_sequence<int, m2l_entries<PM>()>{}, S, M, T, lane, order,
+                                      sAcc);
+    else
+      m2l_steps<PM, false, ADJ, float>(std::make_integer_sequence<int, m2l_entries<PM>()>{}, S, M, T, lane, order,
+                                       sAcc);
+    srcNext = srcNext2;
+    cs0 = cn0; cs1 = cn1; cs2 = cn2;
+  }
+  __syncwarp();
+  const int nm = ((order + 1) * (order + 2) * (order + 3)) / 6;
+  if (bad) {
+    if (lane == 0) atomicAdd(&g_m2lStalls, 1u);
+    const double nan = __longlong_as_double(0x7ff8000000000000ll);
+    for (int e = lane; e < nm; e += 32) {
+      const size_t o = (size_t)f * NM + e;
+      lec1[o] = nan;
+      lec2[o] = nan;
+      if (!ADJ) {
+        lec3[o] = nan;
+        lec4[o] = nan;
+      }
+    }
+    return;
+  }
   const double ieps = 1.0 / eps;
   for (int e = lane; e < nm; e += 32) {
     const double S1 = sAcc[e], S2 = sAcc[NMP + e], S3 = sAcc[2 * NMP + e], S4 = sAcc[3 * NMP + e];
@@ -947,10 +1174,30 @@ static void launch_m2l_unrolled(Context &c, int nDst, const int *dst, const int 
       (float)c.prm.kappa, c.NM, c.epsilon, inPot, inDpdn, o1, o2, o3, o4);
 }
 
+// The bulk-copy staged M2L of a mixed context: the input rows packed to FP32,
+// then one warp per destination cube.
+template <int PU, bool ADJ>
+static void launch_m2l_bulk(Context &c, int nDst, const int *dst, const int *off, const int *src,
+                            const double *inPot, const double *inDpdn, double *o1, double *o2, double *o3,
+                            double *o4) {
+  typedef M2LBulkShape<PU> Sh;
+  static bool attrDone = false;
+  if (!attrDone) {
+    cudaFuncSetAttribute(m2l_bulk_kernel<PU, ADJ>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::bytes);
+    attrDone = true;
+  }
+  const long long total = (long long)c.pt.nFmm * Sh::NMS;
+  m2l_pack_kernel<<<ceil_div(total, 256), 256, 0, c.stream>>>(total, c.NM, Sh::NMS, inPot, inDpdn, c.d_momF2);
+  m2l_bulk_kernel<PU, ADJ><<<nDst, 32, Sh::bytes, c.stream>>>(dst, off, src, c.d_ordM2L, c.d_cubeCtr,
+                                                              (float)c.prm.kappa, c.NM, c.epsilon, c.d_momF2, o1,
+                                                              o2, o3, o4);
+  c.launches += 1;   // the pack
+}
+
 // Forward: moments (d_mom) -> local expansions (4 planes of d_lec).
 // Adjoint: adjoint locals g12, g34 (planes 0, 1 of d_lec) -> adjoint moments
 // (pot, dpdn: planes 0, 1 of d_mom) over the transposed pair lists.
-// fp32: the FP32 conv of a mixed context (orders up to 4).
+// fp32: the FP32 conv of a mixed context (orders up to 5).
 template <int PM>
 static void launch_m2l_t(Context &c, bool adj, bool fp32) {
   const size_t plane = (size_t)c.pt.nFmm * c.NM;
@@ -962,7 +1209,10 @@ static void launch_m2l_t(Context &c, bool adj, bool fp32) {
   double *o3 = c.d_lec + 2 * plane, *o4 = c.d_lec + 3 * plane;
   if (PM <= 5) {
     constexpr int PU = PM <= 5 ? PM : 5;
-    if (fp32 && (M2LUnrolledShape<PU, float>::GEN || c.d_m2lTensF)) {
+    if (fp32 && c.d_momF2) {
+      if (adj) launch_m2l_bulk<PU, true>(c, nDst, dst, off, src, inPot, inDpdn, o1, o2, o3, o4);
+      else launch_m2l_bulk<PU, false>(c, nDst, dst, off, src, inPot, inDpdn, o1, o2, o3, o4);
+    } else if (fp32 && (M2LUnrolledShape<PU, float>::GEN || c.d_m2lTensF)) {
       if (adj) launch_m2l_unrolled<PU, true, float>(c, nDst, dst, off, src, pairIdx, c.d_m2lTensF, inPot, inDpdn, o1, o2, o3, o4);
       else launch_m2l_unrolled<PU, false, float>(c, nDst, dst, off, src, pairIdx, c.d_m2lTensF, inPot, inDpdn, o1, o2, o3, o4);
     } else {
@@ -1089,6 +1339,13 @@ bool setup_fmm(Context &c) {
       if (!c.arena.alloc_n(&c.d_m2lTensF, (size_t)c.NM * c.nM2LPairs)) return false;
       tensors_to_float_kernel<<<1184, 256, 0, s>>>((long long)c.NM * c.nM2LPairs, c.d_m2lTens, c.d_m2lTensF);
       FB_CUDA(cudaGetLastError());
+    }
+    // the FP32 rows the bulk-copy staged M2L reads; FABIPB_B200_M2L_BULK=0 at
+    // context creation keeps the plain-load staging (m2l_unrolled_kernel)
+    const char *bulkEnv = getenv("FABIPB_B200_M2L_BULK");
+    if (c.mixed && c.P <= 5 && genF32 && !(bulkEnv && atoi(bulkEnv) == 0)) {
+      c.momF2Stride = (c.NM + 1) & ~1;
+      if (!c.arena.alloc_n(&c.d_momF2, (size_t)pt.nFmm * c.momF2Stride)) return false;
     }
   }
   // leaf matrices

@@ -43,6 +43,92 @@ template <>
 struct Vec4<double> {
   typedef double4 t;
 };
+template <typename T>
+struct Pair2;
+template <>
+struct Pair2<float> {
+  typedef float2 t;
+};
+template <>
+struct Pair2<double> {
+  typedef double2 t;
+};
+
+// The ordered kernels' gathers, written so that their loads overlap instead of
+// forming one dependent chain per near leaf or special pair.
+//
+// sym_scratch_sums: the symmetric kernels' sums of this target (offset xo in its
+// leaf) over the near-list entries [p0, p1) that they took, in list order:
+// the warp reads 32 entries' slots at once and keeps up to 8 scratch loads in
+// flight.  take: the lane adds (one lane per target).
+template <typename T>
+__device__ __forceinline__ void sym_scratch_sums(int p0, int p1, int lane, bool take, int xo,
+                                                 const int *__restrict__ symOff, const T *__restrict__ symScr,
+                                                 T &a0, T &a1) {
+  typedef typename Pair2<T>::t P;
+  const P *scr = reinterpret_cast<const P *>(symScr);
+  for (int q0 = p0; q0 < p1; q0 += 32) {
+    const int o = q0 + lane < p1 ? symOff[q0 + lane] : -1;
+    unsigned m = __ballot_sync(0xffffffffu, o >= 0);
+    while (m) {   // warp-uniform
+      T v0[8], v1[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        v0[u] = v1[u] = (T)0;
+        if (m) {   // warp-uniform
+          const int oj = __shfl_sync(0xffffffffu, o, __ffs(m) - 1);
+          m &= m - 1;
+          if (take) {
+            const P v = scr[(size_t)oj + xo];
+            v0[u] = v.x;
+            v1[u] = v.y;
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 8; u++) {
+        a0 += v0[u];
+        a1 += v1[u];
+      }
+    }
+  }
+}
+
+// special_sums: the FP64 special-pair corrections of target X in table order,
+// four entries' loads (index, coefficients, then the two densities) at a time.
+__device__ __forceinline__ void special_sums(int X, int n, const int *__restrict__ spOff,
+                                             const int *__restrict__ spSrc, const double4 *__restrict__ spK,
+                                             const double *__restrict__ sgm, double &e0, double &e1) {
+  int e = spOff[X];
+  const int e1End = spOff[X + 1];
+  for (; e + 4 <= e1End; e += 4) {
+    int Y[4];
+    double4 d[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      Y[u] = spSrc[e + u];
+      d[u] = spK[e + u];
+    }
+    double sp[4], sd[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      sp[u] = sgm[Y[u]];
+      sd[u] = sgm[n + Y[u]];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      e0 += d[u].x * sd[u] + d[u].y * sp[u];
+      e1 += d[u].z * sd[u] + d[u].w * sp[u];
+    }
+  }
+  for (; e < e1End; e++) {
+    const int Y = spSrc[e];
+    const double4 d = spK[e];
+    const double sp = sgm[Y], sd = sgm[n + Y];
+    e0 += d.x * sd + d.y * sp;
+    e1 += d.z * sd + d.w * sp;
+  }
+}
 
 // FP32: the single MUFU instructions (PTX rsqrt.approx / ex2.approx, flush
 // to zero; relative error ~2^-22, far below the FP32 P2P tolerance).  FP64:
@@ -194,18 +280,12 @@ near_apply_kernel(int nWork, const int2 *__restrict__ work, const int *__restric
   const V tp = tgtP[X], tn = tgtN[X];
   const double cx = leafCtr[3 * L], cy = leafCtr[3 * L + 1], cz = leafCtr[3 * L + 2];
   T acc0 = (T)0, acc1 = (T)0;
-  const int p1 = nearOff[L + 1];
-  for (int p = nearOff[L]; p < p1; p++) {
-    if (symOff) {   // a leaf pair of the symmetric kernel: its sums for this target are in the scratch
-      const int o = symOff[p];
-      if (o >= 0) {   // warp-uniform
-        if (valid && sub == 0) {
-          acc0 += symScr[2 * (size_t)(o + (X - base))];
-          acc1 += symScr[2 * (size_t)(o + (X - base)) + 1];
-        }
-        continue;
-      }
-    }
+  const int pBeg = nearOff[L], p1 = nearOff[L + 1];
+  // the leaf pairs of the symmetric kernel: their sums for this target are in the scratch
+  if (symOff) sym_scratch_sums<T>(pBeg, p1, lane, valid && sub == 0, X - base, symOff, symScr, acc0, acc1);
+  // the other near leaves
+  for (int p = pBeg; p < p1; p++) {
+    if (symOff && symOff[p] >= 0) continue;   // warp-uniform: summed above
     const int S = nearSrc[p];
     const int sb = leafStart[S], sc = leafCount[S];
     const T tx = tp.x + (T)(cx - leafCtr[3 * S]);
@@ -242,14 +322,7 @@ near_apply_kernel(int nWork, const int2 *__restrict__ work, const int *__restric
   }
   if (!valid || sub != 0) return;
   double e0 = 0.0, e1 = 0.0;
-  const int s1 = spOff[X + 1];
-  for (int e = spOff[X]; e < s1; e++) {
-    const int Y = spSrc[e];
-    const double4 d = spK[e];
-    const double sp = sgm[Y], sd = sgm[n + Y];
-    e0 += d.x * sd + d.y * sp;
-    e1 += d.z * sd + d.w * sp;
-  }
+  special_sums(X, n, spOff, spSrc, spK, sgm, e0, e1);
   const double AX = area[X] * kFourPiI;
   const double v0 = coef * (AX * (double)acc0 + e0), v1 = coef * (AX * (double)acc1 + e1);
   out[X] = accumulate ? out[X] + v0 : v0;   // each output has exactly one writer
@@ -377,19 +450,14 @@ near_apply_f2_kernel(int nWork, const int2 *__restrict__ work, const int *__rest
   const double cx = leafCtr[3 * L], cy = leafCtr[3 * L + 1], cz = leafCtr[3 * L + 2];
   float2 acc0 = f2(0.f), acc1 = f2(0.f);
   float *pf = reinterpret_cast<float *>(&sP[warp][lane >> 1][0]) + (lane & 1);
-  const int p1 = nearOff[L + 1];
-  for (int p = nearOff[L]; p < p1; p++) {
-    if (symOff) {   // a leaf pair of the symmetric kernel: its sums for this target are in the scratch
-      const int o = symOff[p];
-      if (o >= 0) {   // warp-uniform
-        if (valid && sub == 0) {
-          const float2 v = symScr[o + (X - base)];
-          acc0.x += v.x;
-          acc1.x += v.y;
-        }
-        continue;
-      }
-    }
+  const int pBeg = nearOff[L], p1 = nearOff[L + 1];
+  // the leaf pairs of the symmetric kernel: their sums for this target are in the scratch
+  if (symOff)
+    sym_scratch_sums<float>(pBeg, p1, lane, valid && sub == 0, X - base, symOff,
+                            reinterpret_cast<const float *>(symScr), acc0.x, acc1.x);
+  // the other near leaves
+  for (int p = pBeg; p < p1; p++) {
+    if (symOff && symOff[p] >= 0) continue;   // warp-uniform: summed above
     const int S = nearSrc[p];
     const int sb = leafStart[S], sc = leafCount[S];
     const float2 tx = f2(tp.x + (float)(cx - leafCtr[3 * S]));
@@ -428,14 +496,7 @@ near_apply_f2_kernel(int nWork, const int2 *__restrict__ work, const int *__rest
   }
   if (!valid || sub != 0) return;
   double e0 = 0.0, e1 = 0.0;
-  const int sp1 = spOff[X + 1];
-  for (int e = spOff[X]; e < sp1; e++) {
-    const int Y = spSrc[e];
-    const double4 d = spK[e];
-    const double sp = sgm[Y], sd = sgm[n + Y];
-    e0 += d.x * sd + d.y * sp;
-    e1 += d.z * sd + d.w * sp;
-  }
+  special_sums(X, n, spOff, spSrc, spK, sgm, e0, e1);
   const double AX = area[X] * kFourPiI;
   const double v0 = coef * (AX * (double)s0 + e0), v1 = coef * (AX * (double)s1 + e1);
   out[X] = accumulate ? out[X] + v0 : v0;   // each output has exactly one writer

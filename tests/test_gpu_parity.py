@@ -150,6 +150,41 @@ def test_symmetric_near_field(name, depth, height, case_dir, golden_meta, monkey
     assert abs(lhs - rhs) <= 1e-12 * np.linalg.norm(lam) * np.linalg.norm(out[True, lib.FP64][0])
 
 
+@pytest.mark.parametrize("name,order,depth", [("sphere1280", 3, 3), ("star2048", 4, 3), ("shell1152", 5, 3),
+                                               ("star2048", 5, 4), ("sphere1280", 4, 4)])
+def test_m2l_bulk_staging(name, order, depth, case_dir, golden_meta, monkeypatch):
+    """The M2L of mixed contexts with its moments staged by bulk copies into
+    shared memory (the default) against the plain-load staging
+    (FABIPB_B200_M2L_BULK=0): the same FP32 tensors, moments and conv order, so
+    the far fields agree to 1e-6 relative (FP32 rounding: the compiler pairs and
+    contracts the FP32 operations of the two kernels differently), forward and
+    transposed; both within
+    2e-5 of the FP64 far field (FP32 tensors, moments and leaf matrices); the bulk path launches one kernel more (the FP32
+    row pack).  The depth-4 trees give destinations with more than 64 pairs, so
+    the copies of the next batch are in flight while a batch is summed."""
+    opts = dict(golden_meta[name]["opts"], p=order, t=depth)
+    pan, _ = meshio.load_case(os.path.join(case_dir, name))
+    sg = make_golden.seeded_sigma(pan.n, 8)
+    lam = make_golden.seeded_sigma(pan.n, 9)
+    out = {}
+    for mode, prec, env in (("bulk", lib.MIXED, "1"), ("plain", lib.MIXED, "0"), ("fp64", lib.FP64, "1")):
+        monkeypatch.setenv("FABIPB_B200_M2L_BULK", env)
+        s = lib.Surface(pan, lib.params(precision=prec, **case_params(opts)))
+        n0 = s.launch_count()
+        far = s.apply(sg, part=lib.FAR)
+        out[mode] = (far, s.launch_count() - n0, s.apply_adjoint(lam, part=lib.FAR))
+        if mode == "bulk":
+            _, dst = s.m2l_pairs()
+            most = int(np.bincount(dst).max()) if dst.size else 0
+    if depth == 4:
+        assert most > 64
+    assert out["bulk"][1] == out["plain"][1] + 1
+    assert rel_l2(out["bulk"][0], out["plain"][0]) < 1e-6
+    assert rel_l2(out["bulk"][2], out["plain"][2]) < 1e-6
+    assert rel_l2(out["bulk"][0], out["fp64"][0]) < 2e-5
+    assert rel_l2(out["bulk"][2], out["fp64"][2]) < 2e-5
+
+
 def test_apply_alpha_beta_semantics(case_dir, golden_meta, oracles):
     name = "star2048"
     s, _, _ = surface(case_dir, golden_meta, name, lib.FP64)
