@@ -96,6 +96,7 @@ FLOP_PER_PAIR = 60.0   # algorithmic count per near panel pair (KER4 + apply)
 PROFILE_PROXY = {"shell2097152": (("shell524176", 2096704 / 524176),)}
 DIRECT_ORACLE_MAX = 300000   # panels up to which the FP64 direct-summation oracle is solved
 SAMPLE_ABOVE = 500000        # panels above which the CPU reference matvec is sampled
+REF_GPU_DEFAULT_MAX = 2200000  # panels up to which the reference's CUDA backend is timed by default
 
 
 def case_base(name):
@@ -174,7 +175,7 @@ def cpu_reference_rate(base, name, opts, reps, warmup=1, budget=60.0):
     return reps / dt, "port", cores, "%d timed matvecs of the full mesh (FP64 restatement)" % reps, reps
 
 
-def ref_gpu_rate(base, name, opts, reps=10, timeout=900):
+def ref_gpu_rate(base, name, opts, reps=10, timeout=900, budget=60.0):
     """matvec/s of the reference's own CUDA backend (src/gpu_backend_cuda.cu,
     compiled from its sources into oracle/_ref by `make -C oracle refgpu`):
     MtVmain with -g=1 on this GPU, host wall time of `reps` calls after two
@@ -185,7 +186,7 @@ def ref_gpu_rate(base, name, opts, reps=10, timeout=900):
     try:
         pre = os.path.join(tempfile.gettempdir(), "fabipb_refgpu_time")
         out = O.run_ref_harness("time", base, pre, ref_opts(opts), threads=os.cpu_count() or 1, reps=reps,
-                                warmup=2, gpu=True, timeout=timeout, budget=60.0)
+                                warmup=2, gpu=True, timeout=timeout, budget=budget)
         r = json.loads(out.strip().splitlines()[-1])
     except Exception as e:   # a baseline, not the product: report the failure, keep the line
         return {"value": None, "error": str(e)[-300:]}
@@ -565,11 +566,14 @@ def run_ours(args):
     # process holds no device memory yet
     ref_gpu = None
     if rank == 0 and not args.no_ref_gpu:
-        if PANELS[name] <= DIRECT_ORACLE_MAX or args.ref_gpu:
+        if PANELS[name] <= DIRECT_ORACLE_MAX:
             ref_gpu = ref_gpu_rate(base, name, opts)
+        elif PANELS[name] <= REF_GPU_DEFAULT_MAX or args.ref_gpu:
+            # a few seconds per reference matvec here: 3 timed calls, about 30 s of timing
+            ref_gpu = ref_gpu_rate(base, name, opts, reps=3, budget=30.0)
         else:
             ref_gpu = {"value": None, "skipped": "not run by default above %d panels (--ref-gpu runs it)" %
-                       DIRECT_ORACLE_MAX}
+                       REF_GPU_DEFAULT_MAX}
     fp32_peak = lib.simt_peak_tflops(local, fp64=False)
     fp64_peak = lib.simt_peak_tflops(local, fp64=True)
     prec = lib.MIXED if args.precision == "mixed" else lib.FP64
@@ -745,7 +749,7 @@ def main():
                     help="seconds of timed reference work at most (--impl reference)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-gpu", action="store_true",
-                    help="time the reference's own CUDA backend also on meshes above %d panels" % DIRECT_ORACLE_MAX)
+                    help="time the reference's own CUDA backend also on meshes above %d panels" % REF_GPU_DEFAULT_MAX)
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip the reference's CUDA backend")
     ap.add_argument("--no-dropin", action="store_true", help="skip the plugin-ABI end-to-end timing")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 operator's matvec rate")
