@@ -899,6 +899,69 @@ __global__ void special_coeff_kernel(long long nSp, const int *__restrict__ spDs
   if (caseOut) caseOut[e] = cs;
 }
 
+// panel i (tree order) as the quadrature rules take it
+__device__ inline void load_panel_d(const double *__restrict__ vtx, const double *__restrict__ nrm,
+                                    const double *__restrict__ area, int i, PanelD &P) {
+  const double *v = vtx + 9 * (size_t)i;
+  for (int k = 0; k < 3; k++)
+    for (int c = 0; c < 3; c++) P.v[k][c] = v[3 * k + c];
+  for (int c = 0; c < 3; c++) {
+    P.a[0][c] = P.v[2][c] - P.v[1][c];
+    P.a[1][c] = P.v[0][c] - P.v[2][c];
+    P.a[2][c] = P.v[1][c] - P.v[0][c];
+    P.n[c] = nrm[3 * (size_t)i + c];
+  }
+  P.area = area[i];
+}
+
+// Near field at panel quadrature order q > 1: the reference's near-field loop
+// with panelIA0 at order q for every near pair (src/fmm.c:554-593,
+// src/numQuad.c:629-697) -- q^4 kernel evaluations for a disjoint pair
+// (pnlNil0), the Sauter rules for touching ones -- in FP64, one thread per
+// target panel, the near leaves in list order and their panels in order.
+// Forward (target X, K = panelIA0(X, Y)):
+//   out_pot[X] += K0 s_dpdn[Y] + K1 s_pot[Y],  out_dpdn[X] += K2 s_dpdn[Y] + K3 s_pot[Y].
+// ADJ, the transposed operator (target Y, K = panelIA0(X, Y) of the forward
+// pair; the near-leaf relation is symmetric):
+//   out_pot[Y] += K1 l_pot[X] + K3 l_dpdn[X],  out_dpdn[Y] += K0 l_pot[X] + K2 l_dpdn[X].
+template <bool ADJ>
+__global__ void __launch_bounds__(128)
+near_quad_kernel(int n, int q, const int *__restrict__ leafOfPanel, const int *__restrict__ leafStart,
+                 const int *__restrict__ leafCount, const int *__restrict__ nearOff, const int *__restrict__ nearSrc,
+                 const double *__restrict__ vtx, const double *__restrict__ nrm, const double *__restrict__ area,
+                 double kappa, double eps, const double *__restrict__ sgm, double coef, int accumulate,
+                 double *out) {
+  const int T = blockIdx.x * blockDim.x + threadIdx.x;
+  if (T >= n) return;
+  PanelD P;
+  load_panel_d(vtx, nrm, area, T, P);
+  const int L = leafOfPanel[T];
+  double e0 = 0.0, e1 = 0.0;
+  const int p1 = nearOff[L + 1];
+  for (int p = nearOff[L]; p < p1; p++) {
+    const int S = nearSrc[p];
+    const int y1 = leafStart[S] + leafCount[S];
+    for (int Y = leafStart[S]; Y < y1; Y++) {
+      PanelD Q;
+      load_panel_d(vtx, nrm, area, Y, Q);
+      double K[4];
+      const double sp = sgm[Y], sd = sgm[n + Y];
+      if (ADJ) {
+        panel_ia0_d(q, kappa, eps, Q, P, Y == T, K, nullptr);
+        e0 += K[1] * sp + K[3] * sd;
+        e1 += K[0] * sp + K[2] * sd;
+      } else {
+        panel_ia0_d(q, kappa, eps, P, Q, Y == T, K, nullptr);
+        e0 += K[0] * sd + K[1] * sp;
+        e1 += K[2] * sd + K[3] * sp;
+      }
+    }
+  }
+  const double v0 = coef * e0, v1 = coef * e1;
+  out[T] = accumulate ? out[T] + v0 : v0;   // each output has exactly one writer
+  out[T + n] = accumulate ? out[T + n] + v1 : v1;
+}
+
 namespace {
 
 struct VKey {
@@ -1089,9 +1152,12 @@ static bool setup_near_targets(Context &c);
 bool setup_near(Context &c) {
   const PanelTree &pt = c.pt;
   cudaStream_t s = c.stream;
-  if (c.prm.quad_order != 1) {
-    set_error("the device near field implements the one-point panel rule (-q=1); got -q=%d",
-              c.prm.quad_order);
+  // -q=1: the one-point P2P kernels plus the FP64 special-pair corrections;
+  // -q>1: near_quad_kernel (panelIA0 at order q for every near pair).  The
+  // special-pair table is built at order q either way (the preconditioners
+  // assemble their blocks from it).
+  if (c.prm.quad_order < 1 || c.prm.quad_order > 10) {
+    set_error("panel quadrature order -q=%d outside 1..10", c.prm.quad_order);
     return false;
   }
   // the direct operator: every leaf is near every leaf
@@ -1473,6 +1539,15 @@ bool launch_near(Context &c, const double *sgm, double coef, double *out, bool a
   if (adjoint && !setup_near_adjoint(c)) return false;
   cudaStream_t s = stream ? stream : c.stream;
   const bool acc = accumulate;
+  if (c.prm.quad_order > 1) {   // every near pair by panelIA0 at order q, in FP64 in every context
+    auto kern = adjoint ? near_quad_kernel<true> : near_quad_kernel<false>;
+    kern<<<ceil_div(c.n, 128), 128, 0, s>>>(c.n, c.prm.quad_order, c.d_leafOfPanel, c.d_leafStart, c.d_leafCount,
+                                            c.d_nearOff, c.d_nearSrc, c.d_vtx, c.d_nrm, c.d_area, c.prm.kappa,
+                                            c.epsilon, sgm, coef, acc ? 1 : 0, out);
+    c.launches += 1;
+    FB_CUDA(cudaGetLastError());
+    return true;
+  }
   if (c.mixed && fp64) {
     if (!setup_near_fp64(c)) return false;
     if (adjoint) launch_near_t<double, true>(c, c.d_tgtP64, c.d_tgtN64, c.d_srcA64, c.d_srcB64, sgm, coef, out, s, acc);

@@ -3,6 +3,7 @@
     python tests/golden/make_golden.py            # the small cases (cases.json, *.npz)
     python tests/golden/make_golden.py --large    # solve-only goldens (solve_cases.json)
     python tests/golden/make_golden.py --fd       # the reference's energy gradient by FD (fd_star2048.json)
+    python tests/golden/make_golden.py --quad     # panel quadrature order -q=2 (quad_cases.json, *_q2.npz)
 
 Needs the reference CPU solver compiled from its own sources
 (``make -C oracle ref``, which reads the read-only reference mount).  For each
@@ -126,6 +127,44 @@ def main_large():
         json.dump(out, fp, indent=1, sort_keys=True)
 
 
+# Golden cases recomputed at panel quadrature order -q=2 (panelIA0 with q^4
+# kernel evaluations for every disjoint near pair): one near-field apply and
+# one matvec of the seeded density, the direct right-hand side and the
+# panel-tree energy (q^2 points per panel), and the full CLI solve.
+QUAD_CASES = ("sphere320", "star2048")
+QUAD_ORDER = 2
+
+
+def main_quad():
+    from oracle import oracle as O
+    meta = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for name in QUAD_CASES:
+            opts = CASES[name][2]
+            base = generate_mesh(name, tmp)
+            pre = os.path.join(tmp, name + "_out")
+            o = ref_opts(opts) + ["-q=%d" % QUAD_ORDER]
+            O.run_ref_harness("tree", base, pre, o)
+            n = int(O.read_bin(pre, "hdr", np.int32)[0])
+            sg = seeded_sigma(n)
+            data = {}
+            O.run_ref_harness("near", base, pre, o, sigma=sg)
+            data["near"] = O.read_bin(pre, "pot", np.float64)
+            O.run_ref_harness("matvec", base, pre, o, sigma=sg)
+            data["matvec"] = O.read_bin(pre, "pot", np.float64)
+            O.run_ref_harness("rhs", base, pre, o)
+            data["rhs"] = O.read_bin(pre, "rhs", np.float64)
+            O.run_ref_harness("energy", base, pre, o, sigma=sg)
+            data["energy_raw"] = O.read_bin(pre, "energy", np.float64)
+            e, it, res, _ = O.run_ref_solve(base, ref_opts(opts, True) + ["-q=%d" % QUAD_ORDER], threads=4)
+            np.savez_compressed(os.path.join(HERE, "%s_q%d.npz" % (name, QUAD_ORDER)), **data)
+            meta[name] = {"panels": n, "opts": dict(opts, q=QUAD_ORDER), "digest": mesh_digest(base),
+                          "solve": {"energy": e, "iterations": it, "residual": res}}
+            print(name, "q=%d" % QUAD_ORDER, n, "energy", e, "its", it, "resid", res, flush=True)
+    with open(os.path.join(HERE, "quad_cases.json"), "w") as fp:
+        json.dump(meta, fp, indent=1, sort_keys=True)
+
+
 # Central finite differences of the reference CLI's own energy on star2048:
 # every charge-tree cluster opened (FABIPB_ENERGY_TREE_THETA=1e-9, so the
 # panel-tree energy is the direct panel-charge sum), GMRES to 1e-14, the
@@ -205,6 +244,8 @@ def main():
         return main_large()
     if "--fd" in sys.argv:
         return main_fd()
+    if "--quad" in sys.argv:
+        return main_quad()
     meta = {}
     with tempfile.TemporaryDirectory() as tmp:
         for name, (_, _, opts) in CASES.items():
