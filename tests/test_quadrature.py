@@ -86,3 +86,22 @@ def test_quad_dropin_solve_matches_cpu_reference(name, case_dir, quad_meta):
     e, it = D.parse(out)
     assert it == meta["solve"]["iterations"]
     assert abs(e - meta["solve"]["energy"]) <= 2e-6 + 1e-8 * abs(e)
+
+
+@pytest.mark.parametrize("name", make_golden.QUAD_CASES)
+def test_quad_library_solve(name, case_dir, quad_meta):
+    """The library's own device solve at -q=2 (FP64 operator; its block
+    preconditioner assembled from one-point terms plus the order-q special
+    pairs, where the reference's evaluates every block pair at order q):
+    converged, the reference's energy within ten times the GMRES tolerance,
+    its iteration count within two."""
+    meta = quad_meta[name]
+    opts = meta["opts"]
+    s = surface(case_dir, quad_meta, name, lib.FP64, charges=True)
+    b = s.rhs(use_tree=False)
+    s.precond_setup(2)
+    x, it, res, info = s.solve(b, b.copy(), restart=opts["a"], maxit=100, tol=opts["o"])
+    e = s.energy_raw(x) * 2 * np.pi * 332.0716
+    assert info == 0
+    assert abs(it - meta["solve"]["iterations"]) <= 2
+    assert abs(e - meta["solve"]["energy"]) <= 10 * opts["o"] * abs(meta["solve"]["energy"])
