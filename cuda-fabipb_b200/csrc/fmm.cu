@@ -727,6 +727,67 @@ __device__ __forceinline__ void m2l_steps(std::integer_sequence<int, Q...>, M2LS
   (m2l_step<PM, Q, FULL, ADJ, TV, TT, TM>(S, M, T, lane, order, sAcc), ...);
 }
 
+// Lane l ends with the warp total of v[(l >> 1) & 15]: one butterfly over
+// sixteen values (8 + 4 + 2 + 1 + 1 shuffles), whose first stages carry
+// several independent shuffles each.
+__device__ __forceinline__ float warp_sum16(const float (&v)[16], int lane) {
+  const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4, h2 = lane & 2;
+  float w[8], x[4], y[2];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+    w[i] = (h16 ? v[i + 8] : v[i]) + __shfl_xor_sync(0xffffffffu, h16 ? v[i] : v[i + 8], 16);
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+    x[i] = (h8 ? w[i + 4] : w[i]) + __shfl_xor_sync(0xffffffffu, h8 ? w[i] : w[i + 4], 8);
+#pragma unroll
+  for (int i = 0; i < 2; i++)
+    y[i] = (h4 ? x[i + 2] : x[i]) + __shfl_xor_sync(0xffffffffu, h4 ? x[i] : x[i + 2], 4);
+  float z = (h2 ? y[1] : y[0]) + __shfl_xor_sync(0xffffffffu, h2 ? y[0] : y[1], 2);
+  return z + __shfl_xor_sync(0xffffffffu, z, 1);
+}
+
+// The bulk-staged M2L's (alpha, beta) step: the conv of m2l_step (FP32), with
+// the four sums of four consecutive output coefficients reduced together by
+// warp_sum16 (16 shuffles for 16 sums instead of 24, and independent shuffle
+// chains), lane 2j (j = 4 slot + component) adding sum j to its coefficient.
+struct M2LSums16 {
+  float s1, s2, s3, s4;
+  float b[16];   // [slot of alpha mod 4][component]
+};
+template <int PM, int Q, bool FULL, bool ADJ, typename TT>
+__device__ __forceinline__ void m2l_step16(M2LSums16 &S, M2LRowMoments &M, const TT &T, int lane, int order,
+                                           double *sAcc) {
+  constexpr M2LEntry E = m2l_entry<PM>(Q);
+  if (E.first) S.s1 = S.s2 = S.s3 = S.s4 = 0.f;
+  if (FULL || E.dsum <= order) {
+    const float2 mo = M.template get<E.ib>();
+    const float2 d = T.get(E.ig, lane);
+    if ((ADJ ? E.dal : E.dsum - E.dal) & 1) {   // (-1)^|input|, or (-1)^|output| transposed
+      S.s1 -= mo.y * d.x; S.s2 -= mo.y * d.y; S.s3 -= mo.x * d.x; S.s4 -= mo.x * d.y;
+    } else {
+      S.s1 += mo.y * d.x; S.s2 += mo.y * d.y; S.s3 += mo.x * d.x; S.s4 += mo.x * d.y;
+    }
+  }
+  if constexpr (E.last) {
+    constexpr int slot = E.al & 3;
+    S.b[4 * slot] = S.s1;
+    S.b[4 * slot + 1] = S.s2;
+    S.b[4 * slot + 2] = S.s3;
+    S.b[4 * slot + 3] = S.s4;
+    if constexpr (slot == 3 || E.al == nmom_c(PM) - 1) {
+      // a last group of fewer than four: the slots past E.al are reduced, not written
+      const float t = warp_sum16(S.b, lane);
+      const int j = (lane >> 1) & 15, al = (E.al & ~3) + (j >> 2);
+      if (!(lane & 1) && al <= E.al && (FULL || c_mi[al].w <= order)) sAcc[(j & 3) * nmom_c(PM) + al] += (double)t;
+    }
+  }
+}
+template <int PM, bool FULL, bool ADJ, typename TT, int... Q>
+__device__ __forceinline__ void m2l_steps16(std::integer_sequence<int, Q...>, M2LSums16 &S, M2LRowMoments &M,
+                                            const TT &T, int lane, int order, double *sAcc) {
+  (m2l_step16<PM, Q, FULL, ADJ, TT>(S, M, T, lane, order, sAcc), ...);
+}
+
 // The lane's FP32 M2L tensor (packed D^e G0, D^e Gk) from its pair's offset x =
 // x_dst - x_src: the radial sequences of derivs_inplace, then the unrolled
 // level recursion, in registers.  A lane without a pair (live false) gets the
@@ -1005,13 +1066,11 @@ m2l_bulk_kernel(const int *__restrict__ dstList, const int *__restrict__ m2lOff,
     }
     // a lane past the batch reads row 0 (finite moments) with its zero tensor
     M2LRowMoments M{buf + s * 32 * Sh::RS + (live ? lane : 0) * Sh::RS, make_float4(0.f, 0.f, 0.f, 0.f)};
-    M2LSumsT<float> S{0.f, 0.f, 0.f, 0.f};
+    M2LSums16 S{};
     if (order == PM)
-      m2l_steps<PM, true, ADJ, float>(std::make_integer_sequence<int, m2l_entries<PM>()>{}, S, M, T, lane, order,
-                                      sAcc);
+      m2l_steps16<PM, true, ADJ>(std::make_integer_sequence<int, m2l_entries<PM>()>{}, S, M, T, lane, order, sAcc);
     else
-      m2l_steps<PM, false, ADJ, float>(std::make_integer_sequence<int, m2l_entries<PM>()>{}, S, M, T, lane, order,
-                                       sAcc);
+      m2l_steps16<PM, false, ADJ>(std::make_integer_sequence<int, m2l_entries<PM>()>{}, S, M, T, lane, order, sAcc);
     srcNext = srcNext2;
     cs0 = cn0; cs1 = cn1; cs2 = cn2;
   }
