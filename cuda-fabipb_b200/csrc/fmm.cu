@@ -923,7 +923,7 @@ m2l_unrolled_kernel(int nDst, const int *__restrict__ dstList, const int *__rest
 //  * m2l_pack_kernel writes the input moments as one FP32 (pot, dpdn) row per
 //    cube, NMS float2 entries (NMP rounded up to a 16-byte multiple);
 //  * one warp per destination cube and per block; each lane's source row is
-//    fetched with one cp.async.bulk (global -> shared, no multicast) into a
+//    fetched with one cp.async.bulk (global -> this CTA's shared memory only) into a
 //    row of the warp's buffer, completion counted on an mbarrier;
 //  * two buffers: the copies of batch b+1 are in flight while batch b's
 //    tensors are generated and its conv runs, so the warp waits on no moment
